@@ -1,0 +1,67 @@
+"""CPU checks of the drop-in boundary: the library loads and exports every symbol the header declares."""
+
+import ctypes
+import os
+import re
+
+import pytest
+
+from voxneus_b200 import _lib
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "voxneus_b200.h")
+
+
+def header_symbols():
+    src = open(HEADER).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    return sorted(set(re.findall(r"\b(vx_[a-z0-9_]+)\s*\(", src)))
+
+
+def test_header_declares_bound_symbols():
+    decl = set(header_symbols())
+    bound = set(_lib.exported_symbols())
+    assert decl == bound, (decl - bound, bound - decl)
+
+
+def test_library_exports_every_declared_symbol():
+    if not os.path.exists(_lib.library_path()):
+        pytest.skip("library not built")
+    lib = ctypes.CDLL(_lib.library_path())
+    for name in header_symbols():
+        assert hasattr(lib, name), name
+
+
+def test_size_queries_without_gpu():
+    if not os.path.exists(_lib.library_path()):
+        pytest.skip("library not built")
+    assert _lib.query("vx_vr_bitmap_words", _lib.i3([256, 256, 256])) == 256 ** 3 // 32
+    assert _lib.query("vx_reg_stencil_blocks", _lib.i3([256, 256, 256])) == (256 // 4) * (256 // 4) * (256 // 32)
+    assert _lib.query("vx_composite_workspace_blocks", 8192) >= 1
+    lib = _lib.load(require_cuda=False)
+    assert lib.vx_version().startswith(b"voxneus_b200")
+
+
+def test_invalid_arguments_are_rejected_before_launch():
+    """Validation errors come back as status codes with a message, no device touched."""
+    if not os.path.exists(_lib.library_path()):
+        pytest.skip("library not built")
+    lib = _lib.load(require_cuda=False)
+    st = lib.vx_grid_upsample(None, _lib.i3([0, 4, 4]), None, _lib.i3([8, 8, 8]), None)
+    assert st == 1 and b"positive" in lib.vx_last_error()
+    st = lib.vx_sample_multistep(None, _lib.i3([8, 8, 8]), _lib.f3([-1] * 3), _lib.f3([1] * 3), None, None, None,
+                                 None, 4, 16, 200, 4, 0, None, None, None, None, None, 0, None, None, None, None,
+                                 None, None)
+    assert st == 1 and b"<= 32" in lib.vx_last_error()
+
+
+def test_kernel_calls_fail_loudly_without_cuda(monkeypatch):
+    """No silent fallback: without a device the ops raise."""
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is present")
+    from voxneus_b200 import ops
+
+    with pytest.raises(RuntimeError):
+        ops.near_far_from_sphere(torch.zeros(2, 3), torch.ones(2, 3))

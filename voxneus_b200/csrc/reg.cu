@@ -1,0 +1,353 @@
+// Closed-form eikonal (Eq.10-11, regularization/eikonal.py:13-171) and Laplacian curvature
+// (Eq.12-14, regularization/curvature.py:13-165) gradients written straight into the grid
+// gradient.
+//
+// Two forms:
+//  * list form (the reference's kernel interface, eikonal_grad.cu / curvature_grad.cu):
+//    one thread per listed vertex, atomics into the gradient, scale 2/|list|;
+//  * fused gather form for the training step: one pass over 32x4x4 voxel tiles of the
+//    grid, skipping tiles with no active vertex. Each output voxel sums, in registers, the
+//    contributions of the <= 7 active interior vertices whose stencil touches it (itself
+//    and its 6 face neighbours), reading a halo-2 tile of the SDF from shared memory. No
+//    atomics: the result is deterministic. The active set is the V_R bitmap with the relax
+//    and narrow-band predicates, and |V_R| comes from the device-side counts.
+// Both forms also reduce the monitoring losses (mean over interior vertices) through
+// per-block partials and a last-block epilogue.
+#include "common.cuh"
+
+namespace vx {
+
+struct RegOut {
+  double* partials;       // 3 per block: eikonal sum, curvature sum, interior count
+  unsigned int* counter;  // zero before the first launch; reset by the last block
+  float* losses;          // [eikonal, curvature]
+};
+
+__device__ void reduce_losses(const RegOut& o, double e, double c, double n) {
+  __shared__ double s[3][32];
+  __shared__ bool is_last;
+  const int lane = threadIdx.x & 31;
+  const int warp = threadIdx.x >> 5;
+  const int nthreads = blockDim.x * blockDim.y * blockDim.z;
+  const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+  const int wl = tid & 31, ww = tid >> 5;
+  (void)lane;
+  (void)warp;
+  e = warp_sum_d(e);
+  c = warp_sum_d(c);
+  n = warp_sum_d(n);
+  if (wl == 0) {
+    s[0][ww] = e;
+    s[1][ww] = c;
+    s[2][ww] = n;
+  }
+  __syncthreads();
+  const unsigned nblocks = gridDim.x * gridDim.y * gridDim.z;
+  const unsigned bid = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
+  if (tid == 0) {
+    double a = 0, b = 0, k = 0;
+    for (int w = 0; w < (nthreads + 31) / 32; ++w) {
+      a += s[0][w];
+      b += s[1][w];
+      k += s[2][w];
+    }
+    o.partials[3 * bid] = a;
+    o.partials[3 * bid + 1] = b;
+    o.partials[3 * bid + 2] = k;
+    __threadfence();
+    is_last = (atomicAdd(o.counter, 1u) == nblocks - 1);
+  }
+  __syncthreads();
+  if (is_last && tid == 0) {
+    __threadfence();
+    const volatile double* p = o.partials;
+    double a = 0, b = 0, k = 0;
+    for (unsigned i = 0; i < nblocks; ++i) {
+      a += p[3 * i];
+      b += p[3 * i + 1];
+      k += p[3 * i + 2];
+    }
+    if (o.losses) {
+      o.losses[0] = k > 0 ? (float)(a / k) : 0.0f;
+      o.losses[1] = k > 0 ? (float)(b / k) : 0.0f;
+    }
+    *o.counter = 0u;
+  }
+}
+
+// ------------------------------------ list form --------------------------------------------
+
+__global__ void __launch_bounds__(256) k_eikonal_list(const float* __restrict__ f, Grid g,
+                                                      const int64_t* __restrict__ verts, int64_t nv,
+                                                      float* __restrict__ gg, float weight, RegOut o) {
+  double e = 0, n = 0;
+  const float dx = 2.0f * g.eps[0], dy = 2.0f * g.eps[1], dz = 2.0f * g.eps[2];
+  const int nblk = gridDim.x;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv; i += (int64_t)nblk * blockDim.x) {
+    const int64_t vx_ = verts[3 * i], vy_ = verts[3 * i + 1], vz_ = verts[3 * i + 2];
+    if (vx_ <= 0 || vx_ >= g.rx - 1 || vy_ <= 0 || vy_ >= g.ry - 1 || vz_ <= 0 || vz_ >= g.rz - 1) continue;
+    const int x = (int)vx_, y = (int)vy_, z = (int)vz_;
+    const float nx = (__ldg(f + lin3(g, x + 1, y, z)) - __ldg(f + lin3(g, x - 1, y, z))) / dx;
+    const float ny = (__ldg(f + lin3(g, x, y + 1, z)) - __ldg(f + lin3(g, x, y - 1, z))) / dy;
+    const float nz = (__ldg(f + lin3(g, x, y, z + 1)) - __ldg(f + lin3(g, x, y, z - 1))) / dz;
+    const float len = sqrtf(nx * nx + ny * ny + nz * nz);
+    const float scale = (2.0f / (float)nv) * (1.0f - 1.0f / (len + 1e-8f)) * weight;
+    const float ax = scale * nx, ay = scale * ny, az = scale * nz;
+    if (gg) {
+      atomicAdd(gg + lin3(g, x + 1, y, z), ax / dx);
+      atomicAdd(gg + lin3(g, x - 1, y, z), -ax / dx);
+      atomicAdd(gg + lin3(g, x, y + 1, z), ay / dy);
+      atomicAdd(gg + lin3(g, x, y - 1, z), -ay / dy);
+      atomicAdd(gg + lin3(g, x, y, z + 1), az / dz);
+      atomicAdd(gg + lin3(g, x, y, z - 1), -az / dz);
+    }
+    const double l = sqrt((double)nx * nx + (double)ny * ny + (double)nz * nz + 1e-16);
+    e += (l - 1.0) * (l - 1.0);
+    n += 1.0;
+  }
+  reduce_losses(o, e, 0.0, n);
+}
+
+__global__ void __launch_bounds__(256) k_curvature_list(const float* __restrict__ f, Grid g,
+                                                        const int64_t* __restrict__ verts, int64_t nv,
+                                                        float* __restrict__ gg, float weight, RegOut o) {
+  double c = 0, n = 0;
+  const float ex2 = g.eps[0] * g.eps[0], ey2 = g.eps[1] * g.eps[1], ez2 = g.eps[2] * g.eps[2];
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < nv; i += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t vx_ = verts[3 * i], vy_ = verts[3 * i + 1], vz_ = verts[3 * i + 2];
+    if (vx_ <= 0 || vx_ >= g.rx - 1 || vy_ <= 0 || vy_ >= g.ry - 1 || vz_ <= 0 || vz_ >= g.rz - 1) continue;
+    const int x = (int)vx_, y = (int)vy_, z = (int)vz_;
+    const float fc = __ldg(f + lin3(g, x, y, z));
+    const float Lx = (__ldg(f + lin3(g, x + 1, y, z)) + __ldg(f + lin3(g, x - 1, y, z)) - 2.0f * fc) / ex2;
+    const float Ly = (__ldg(f + lin3(g, x, y + 1, z)) + __ldg(f + lin3(g, x, y - 1, z)) - 2.0f * fc) / ey2;
+    const float Lz = (__ldg(f + lin3(g, x, y, z + 1)) + __ldg(f + lin3(g, x, y, z - 1)) - 2.0f * fc) / ez2;
+    const float scale = (2.0f / (float)nv) * weight;
+    if (gg) {
+      atomicAdd(gg + lin3(g, x, y, z), scale * (-2.0f * Lx / ex2 - 2.0f * Ly / ey2 - 2.0f * Lz / ez2));
+      atomicAdd(gg + lin3(g, x + 1, y, z), scale * (Lx / ex2));
+      atomicAdd(gg + lin3(g, x - 1, y, z), scale * (Lx / ex2));
+      atomicAdd(gg + lin3(g, x, y + 1, z), scale * (Ly / ey2));
+      atomicAdd(gg + lin3(g, x, y - 1, z), scale * (Ly / ey2));
+      atomicAdd(gg + lin3(g, x, y, z + 1), scale * (Lz / ez2));
+      atomicAdd(gg + lin3(g, x, y, z - 1), scale * (Lz / ez2));
+    }
+    c += (double)Lx * Lx + (double)Ly * Ly + (double)Lz * Lz;
+    n += 1.0;
+  }
+  reduce_losses(o, 0.0, c, n);
+}
+
+// ------------------------------------ gather form ------------------------------------------
+
+constexpr int TZ = 32, TY = 4, TX = 4;  // output tile (z fastest)
+constexpr int HZ = TZ + 4, HY = TY + 4, HX = TX + 4;  // SDF box, halo 2
+constexpr int MZ = TZ + 2, MY = TY + 2, MX = TX + 2;  // active-mask box, halo 1
+
+struct StencilArgs {
+  const float* f;
+  const uint32_t* bm;
+  Grid g;
+  const unsigned long long* counts;  // from vx_vr_count
+  float relax_r;
+  float band;
+  float w_eik, w_curv;
+  float* gg;
+  int tiles_z, tiles_y;
+};
+
+__device__ __forceinline__ bool vr_member(const StencilArgs& a, int x, int y, int z, bool relax_on) {
+  const int idx = lin3(a.g, x, y, z);
+  if (!(__ldg(a.bm + (idx >> 5)) & (1u << (idx & 31)))) return false;
+  if (relax_on) {
+    const float wx = __fadd_rn(a.g.lo[0], __fmul_rn((float)x, a.g.eps[0]));
+    const float wy = __fadd_rn(a.g.lo[1], __fmul_rn((float)y, a.g.eps[1]));
+    const float wz = __fadd_rn(a.g.lo[2], __fmul_rn((float)z, a.g.eps[2]));
+    if (!(sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(wx, wx), __fmul_rn(wy, wy)), __fmul_rn(wz, wz))) < a.relax_r))
+      return false;
+  }
+  if (a.band > 0.0f && !(fabsf(__ldg(a.f + idx)) < a.band)) return false;
+  return true;
+}
+
+// blockDim = (32, 4, 2); each thread owns output voxels (z, y, x) and (z, y, x + 2).
+__global__ void __launch_bounds__(256) k_reg_stencil(StencilArgs a, RegOut o) {
+  __shared__ float F[HX][HY][HZ];
+  __shared__ uint8_t M[MX][MY][MZ];
+  const int tz = blockIdx.x % a.tiles_z;
+  const int ty = (blockIdx.x / a.tiles_z) % a.tiles_y;
+  const int tx = blockIdx.x / (a.tiles_z * a.tiles_y);
+  const int z0 = tz * TZ, y0 = ty * TY, x0 = tx * TX;
+  const int tid = threadIdx.x + 32 * (threadIdx.y + 4 * threadIdx.z);
+  const unsigned long long nv = a.counts[a.band > 0.0f ? ((a.relax_r > 0.0f && a.counts[1] > 0) ? 3 : 2)
+                                                       : ((a.relax_r > 0.0f && a.counts[1] > 0) ? 1 : 0)];
+  const bool relax_on = a.relax_r > 0.0f && a.counts[1] > 0;
+  // active interior mask of the halo-1 box
+  int any = 0;
+  for (int q = tid; q < MX * MY * MZ; q += 256) {
+    const int mz = q % MZ, my = (q / MZ) % MY, mx = q / (MZ * MY);
+    const int x = x0 - 1 + mx, y = y0 - 1 + my, z = z0 - 1 + mz;
+    uint8_t m = 0;
+    if (x >= 1 && x <= a.g.rx - 2 && y >= 1 && y <= a.g.ry - 2 && z >= 1 && z <= a.g.rz - 2)
+      m = vr_member(a, x, y, z, relax_on) ? 1 : 0;
+    M[mx][my][mz] = m;
+    any |= m;
+  }
+  if (!__syncthreads_or(any)) {
+    reduce_losses(o, 0.0, 0.0, 0.0);
+    return;
+  }
+  for (int q = tid; q < HX * HY * HZ; q += 256) {
+    const int hz = q % HZ, hy = (q / HZ) % HY, hx = q / (HZ * HY);
+    const int x = x0 - 2 + hx, y = y0 - 2 + hy, z = z0 - 2 + hz;
+    float v = 0.0f;
+    if (x >= 0 && x < a.g.rx && y >= 0 && y < a.g.ry && z >= 0 && z < a.g.rz) v = __ldg(a.f + lin3(a.g, x, y, z));
+    F[hx][hy][hz] = v;
+  }
+  __syncthreads();
+  const float inv_nv = nv > 0 ? 2.0f / (float)nv : 0.0f;
+  const float dx = 2.0f * a.g.eps[0], dy = 2.0f * a.g.eps[1], dz = 2.0f * a.g.eps[2];
+  const float ex2 = a.g.eps[0] * a.g.eps[0], ey2 = a.g.eps[1] * a.g.eps[1], ez2 = a.g.eps[2] * a.g.eps[2];
+  const float sc = inv_nv * a.w_curv;
+  double le = 0, lc = 0, ln = 0;
+  const int lz = threadIdx.x, ly = threadIdx.y;
+#pragma unroll
+  for (int rep = 0; rep < 2; ++rep) {
+    const int lx = threadIdx.z + 2 * rep;
+    const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+    if (x >= a.g.rx || y >= a.g.ry || z >= a.g.rz) continue;
+    // SDF box coordinates of this voxel: (lx+2, ly+2, lz+2); mask box: (lx+1, ly+1, lz+1)
+    float acc = 0.0f;
+    bool touched = false;
+    // contribution of vertex v at mask-box (mx,my,mz) along axis ax with sign +1 when the
+    // output voxel is v + e_ax, -1 when it is v - e_ax; 0 means v itself (curvature centre)
+#pragma unroll
+    for (int nb = 0; nb < 7; ++nb) {
+      const int ax = nb == 0 ? -1 : (nb - 1) >> 1;
+      const int sgn = nb == 0 ? 0 : (((nb - 1) & 1) ? 1 : -1);  // v = voxel + sgn * e_ax
+      const int mx = lx + 1 + (ax == 0 ? sgn : 0);
+      const int my = ly + 1 + (ax == 1 ? sgn : 0);
+      const int mz = lz + 1 + (ax == 2 ? sgn : 0);
+      if (!M[mx][my][mz]) continue;
+      touched = true;
+      const int hx = mx + 1, hy = my + 1, hz = mz + 1;
+      const float fc = F[hx][hy][hz];
+      const float fxp = F[hx + 1][hy][hz], fxm = F[hx - 1][hy][hz];
+      const float fyp = F[hx][hy + 1][hz], fym = F[hx][hy - 1][hz];
+      const float fzp = F[hx][hy][hz + 1], fzm = F[hx][hy][hz - 1];
+      const float Lx = (fxp + fxm - 2.0f * fc) / ex2;
+      const float Ly = (fyp + fym - 2.0f * fc) / ey2;
+      const float Lz = (fzp + fzm - 2.0f * fc) / ez2;
+      const float nx = (fxp - fxm) / dx, ny = (fyp - fym) / dy, nz = (fzp - fzm) / dz;
+      const float len = sqrtf(nx * nx + ny * ny + nz * nz);
+      if (nb == 0) {
+        acc += sc * (-2.0f * Lx / ex2 - 2.0f * Ly / ey2 - 2.0f * Lz / ez2);
+        const double l = sqrt((double)nx * nx + (double)ny * ny + (double)nz * nz + 1e-16);
+        le += (l - 1.0) * (l - 1.0);
+        lc += (double)Lx * Lx + (double)Ly * Ly + (double)Lz * Lz;
+        ln += 1.0;
+        continue;
+      }
+      const float se = inv_nv * (1.0f - 1.0f / (len + 1e-8f)) * a.w_eik;
+      const float na = ax == 0 ? nx : (ax == 1 ? ny : nz);
+      const float da = ax == 0 ? dx : (ax == 1 ? dy : dz);
+      const float La = ax == 0 ? Lx : (ax == 1 ? Ly : Lz);
+      const float ea2 = ax == 0 ? ex2 : (ax == 1 ? ey2 : ez2);
+      // the voxel is v - sgn*e_ax: sgn = -1 -> voxel = v + e_ax (eikonal +), sgn = +1 -> voxel = v - e_ax (eikonal -)
+      const float ve = (se * na) / da;
+      acc += (sgn < 0) ? ve : -ve;
+      acc += sc * (La / ea2);
+    }
+    if (touched && acc != 0.0f) {
+      float* p = a.gg + lin3(a.g, x, y, z);
+      *p += acc;
+    }
+  }
+  reduce_losses(o, le, lc, ln);
+}
+
+static int check_reg(const int32_t res[3]) {
+  VX_REQUIRE(res && res[0] >= 3 && res[1] >= 3 && res[2] >= 3, "grid resolution must be >= 3 per axis");
+  VX_REQUIRE((int64_t)res[0] * res[1] * res[2] < (int64_t(1) << 31), "grid has 2^31 or more voxels");
+  return VX_OK;
+}
+
+static Grid grid_eps(const int32_t res[3], const float eps[3]) {
+  const float lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+  Grid g = make_grid(res, lo, hi);
+  for (int a = 0; a < 3; ++a) g.eps[a] = eps[a];
+  return g;
+}
+
+}  // namespace vx
+
+using namespace vx;
+
+extern "C" {
+
+int vx_reg_list_blocks(int64_t n_verts) { return (int)grid_for(n_verts, 256, 4); }
+
+int vx_eikonal_grad(const float* grid, const int32_t res[3], const int64_t* verts, int64_t n_verts, float* grad_grid,
+                    const float eps[3], float weight, double* partials, int n_partials, unsigned int* counter,
+                    float* losses, void* stream) {
+  if (int s = check_reg(res)) return s;
+  VX_REQUIRE(n_verts >= 0, "n_verts < 0");
+  if (n_verts == 0) return VX_OK;
+  VX_REQUIRE(grid && verts && eps && partials && counter, "null pointer");
+  const int blocks = vx_reg_list_blocks(n_verts);
+  VX_REQUIRE(n_partials >= 3 * blocks, "partials buffer too small (%d < %d)", n_partials, 3 * blocks);
+  RegOut o{partials, counter, losses};
+  k_eikonal_list<<<blocks, 256, 0, (cudaStream_t)stream>>>(grid, grid_eps(res, eps), verts, n_verts, grad_grid,
+                                                            weight, o);
+  count_launches(1);
+  return check_launch("eikonal_grad");
+}
+
+int vx_curvature_grad(const float* grid, const int32_t res[3], const int64_t* verts, int64_t n_verts,
+                      float* grad_grid, const float eps[3], float weight, double* partials, int n_partials,
+                      unsigned int* counter, float* losses, void* stream) {
+  if (int s = check_reg(res)) return s;
+  VX_REQUIRE(n_verts >= 0, "n_verts < 0");
+  if (n_verts == 0) return VX_OK;
+  VX_REQUIRE(grid && verts && eps && partials && counter, "null pointer");
+  const int blocks = vx_reg_list_blocks(n_verts);
+  VX_REQUIRE(n_partials >= 3 * blocks, "partials buffer too small (%d < %d)", n_partials, 3 * blocks);
+  RegOut o{partials, counter, losses};
+  k_curvature_list<<<blocks, 256, 0, (cudaStream_t)stream>>>(grid, grid_eps(res, eps), verts, n_verts, grad_grid,
+                                                              weight, o);
+  count_launches(1);
+  return check_launch("curvature_grad");
+}
+
+int64_t vx_reg_stencil_blocks(const int32_t res[3]) {
+  return (int64_t)((res[2] + TZ - 1) / TZ) * ((res[1] + TY - 1) / TY) * ((res[0] + TX - 1) / TX);
+}
+
+int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[3], const float xyz_min[3],
+                   const float xyz_max[3], float relax_radius, float band, const unsigned long long* counts,
+                   float w_eik, float w_curv, float* grad_grid, double* partials, int64_t n_partials,
+                   unsigned int* counter, float* losses, void* stream) {
+  if (int s = check_reg(res)) return s;
+  VX_REQUIRE(grid && bitmap && counts && grad_grid && partials && counter && xyz_min && xyz_max, "null pointer");
+  const int64_t nb = vx_reg_stencil_blocks(res);
+  VX_REQUIRE(nb < (int64_t(1) << 31), "grid too large");
+  VX_REQUIRE(n_partials >= 3 * nb, "partials buffer too small (%lld < %lld)", (long long)n_partials,
+             (long long)(3 * nb));
+  StencilArgs a;
+  a.f = grid;
+  a.bm = bitmap;
+  a.g = make_grid(res, xyz_min, xyz_max);
+  a.counts = counts;
+  a.relax_r = relax_radius;
+  a.band = band;
+  a.w_eik = w_eik;
+  a.w_curv = w_curv;
+  a.gg = grad_grid;
+  a.tiles_z = (res[2] + TZ - 1) / TZ;
+  a.tiles_y = (res[1] + TY - 1) / TY;
+  RegOut o{partials, counter, losses};
+  k_reg_stencil<<<(unsigned)nb, dim3(32, 4, 2), 0, (cudaStream_t)stream>>>(a, o);
+  count_launches(1);
+  return check_launch("reg_stencil");
+}
+
+}  // extern "C"

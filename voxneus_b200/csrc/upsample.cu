@@ -1,0 +1,136 @@
+// Trilinear grid upsampling with align_corners=True (geometry/upsample.py:12-39, the
+// F.interpolate call of models/sdf_grid.py:183-195) and the sparse/dense grid Adam updates
+// (training/optimizer.py:32-116; adam_upd_kernel.cu of the reference extension).
+//
+// Upsampling is write-bound (a 128^3 -> 256^3 pass reads 8 MiB, L2-resident, and writes
+// 64 MiB): one thread per 4 consecutive z outputs, 16-byte stores when the row allows.
+#include "common.cuh"
+
+namespace vx {
+
+struct Axis {
+  float scale;
+  int in;
+};
+
+// ATen's align_corners source index: src = scale * dst, scale = (in - 1) / (out - 1).
+__device__ __forceinline__ void src_index(const Axis& a, int o, int& i0, int& ip, float& l0, float& l1) {
+  const float r = a.scale * (float)o;
+  i0 = (int)r;
+  ip = (i0 < a.in - 1) ? 1 : 0;
+  l1 = r - (float)i0;
+  l0 = 1.0f - l1;
+}
+
+__global__ void __launch_bounds__(256) k_grid_upsample(const float* __restrict__ src, int ix, int iy, int iz,
+                                                       float* __restrict__ dst, int ox, int oy, int oz, Axis ax, Axis ay,
+                                                       Axis az) {
+  const int zq = (oz + 3) / 4;
+  const int64_t total = (int64_t)ox * oy * zq;
+  const bool vec = (oz % 4) == 0;
+  for (int64_t q = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; q < total; q += (int64_t)gridDim.x * blockDim.x) {
+    const int zb = (int)(q % zq) * 4;
+    const int64_t r = q / zq;
+    const int y = (int)(r % oy);
+    const int x = (int)(r / oy);
+    int x0, xp, y0, yp;
+    float lx0, lx1, ly0, ly1;
+    src_index(ax, x, x0, xp, lx0, lx1);
+    src_index(ay, y, y0, yp, ly0, ly1);
+    const float* r00 = src + ((int64_t)x0 * iy + y0) * iz;
+    const float* r01 = src + ((int64_t)x0 * iy + y0 + yp) * iz;
+    const float* r10 = src + ((int64_t)(x0 + xp) * iy + y0) * iz;
+    const float* r11 = src + ((int64_t)(x0 + xp) * iy + y0 + yp) * iz;
+    float v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int z = zb + k;
+      if (z >= oz) {
+        v[k] = 0.0f;
+        continue;
+      }
+      int z0, zp;
+      float lz0, lz1;
+      src_index(az, z, z0, zp, lz0, lz1);
+      v[k] = lx0 * (ly0 * (lz0 * __ldg(r00 + z0) + lz1 * __ldg(r00 + z0 + zp)) +
+                    ly1 * (lz0 * __ldg(r01 + z0) + lz1 * __ldg(r01 + z0 + zp))) +
+             lx1 * (ly0 * (lz0 * __ldg(r10 + z0) + lz1 * __ldg(r10 + z0 + zp)) +
+                    ly1 * (lz0 * __ldg(r11 + z0) + lz1 * __ldg(r11 + z0 + zp)));
+    }
+    float* out = dst + ((int64_t)x * oy + y) * oz + zb;
+    if (vec) {
+      *reinterpret_cast<float4*>(out) = make_float4(v[0], v[1], v[2], v[3]);
+    } else {
+      for (int k = 0; k < 4 && zb + k < oz; ++k) out[k] = v[k];
+    }
+  }
+}
+
+template <bool kMasked>
+__global__ void __launch_bounds__(256) k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
+                                              float* __restrict__ v, int64_t n, float step_size, float b1, float b2,
+                                              float eps) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    const float gi = g[i];
+    if (kMasked && gi == 0.0f) continue;
+    const float mi = b1 * m[i] + (1.0f - b1) * gi;
+    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    p[i] -= step_size * mi / (sqrtf(vi) + eps);
+  }
+}
+
+}  // namespace vx
+
+using namespace vx;
+
+extern "C" {
+
+int vx_grid_upsample(const float* src, const int32_t res_in[3], float* dst, const int32_t res_out[3], void* stream) {
+  VX_REQUIRE(res_in && res_out, "null resolution");
+  for (int a = 0; a < 3; ++a) VX_REQUIRE(res_in[a] >= 1 && res_out[a] >= 1, "resolutions must be positive");
+  VX_REQUIRE((int64_t)res_out[0] * res_out[1] * res_out[2] < (int64_t(1) << 31), "output has 2^31 or more voxels");
+  VX_REQUIRE(src && dst, "null pointer");
+  VX_REQUIRE(((uintptr_t)dst & 15) == 0, "dst must be 16-byte aligned");
+  Axis ax[3];
+  for (int a = 0; a < 3; ++a) {
+    ax[a].in = res_in[a];
+    ax[a].scale = res_out[a] > 1 ? (float)(res_in[a] - 1) / (float)(res_out[a] - 1) : 0.0f;
+  }
+  const int64_t total = (int64_t)res_out[0] * res_out[1] * ((res_out[2] + 3) / 4);
+  k_grid_upsample<<<grid_for(total, 256, 8), 256, 0, (cudaStream_t)stream>>>(
+      src, res_in[0], res_in[1], res_in[2], dst, res_out[0], res_out[1], res_out[2], ax[0], ax[1], ax[2]);
+  count_launches(1);
+  return check_launch("grid_upsample");
+}
+
+static int adam_common(bool masked, float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n,
+                       int step, float beta1, float beta2, float lr, float eps, void* stream) {
+  VX_REQUIRE(n >= 0, "n < 0");
+  VX_REQUIRE(step >= 1, "step must be >= 1");
+  if (n == 0) return VX_OK;
+  VX_REQUIRE(param && grad && exp_avg && exp_avg_sq, "null pointer");
+  // adam_upd_kernel.cu: step_size = lr * sqrt(1 - b2^t) / (1 - b1^t), evaluated on the host
+  const float step_size = lr * sqrtf(1.0f - powf(beta2, (float)step)) / (1.0f - powf(beta1, (float)step));
+  if (masked)
+    k_adam<true><<<grid_for(n, 256, 8), 256, 0, (cudaStream_t)stream>>>(param, grad, exp_avg, exp_avg_sq, n, step_size,
+                                                                        beta1, beta2, eps);
+  else
+    k_adam<false><<<grid_for(n, 256, 8), 256, 0, (cudaStream_t)stream>>>(param, grad, exp_avg, exp_avg_sq, n,
+                                                                         step_size, beta1, beta2, eps);
+  count_launches(1);
+  return check_launch(masked ? "masked_adam_upd" : "adam_upd");
+}
+
+int vx_adam_upd(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, int step, float beta1,
+                float beta2, float lr, float eps, void* stream) {
+  return adam_common(false, param, grad, exp_avg, exp_avg_sq, n, step, beta1, beta2, lr, eps, stream);
+}
+
+int vx_masked_adam_upd(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, int step,
+                       float beta1, float beta2, float lr, float eps, void* stream) {
+  return adam_common(true, param, grad, exp_avg, exp_avg_sq, n, step, beta1, beta2, lr, eps, stream);
+}
+
+}  // extern "C"
