@@ -1,0 +1,352 @@
+"""Training-step throughput of the fused VoxNeuS hot path on B200 (one JSON line on rank 0).
+
+Workload (the throughput configuration): 256^3 FP32 SDF grid, upsampled on the device from a
+128^3 union of 8 random spheres/boxes + N(0, 0.005) noise; 8192 rays per step per GPU from 64
+hemisphere cameras at 800x600 (focal 700 px); 64 stratified + 4 x 16 upsampled samples per ray
+(perturbed); appearance 16-level hash grid (2 features, 2^19 entries) + 64-wide MLP; V_R =
+render corners within the 1.2 relax sphere and the |f| < 3 voxel narrow band; eikonal 0.1,
+curvature 5e-4; Huber loss on U[0,1] targets; optimizer steps included. A step is one full
+training iteration over one ray batch.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+
+--impl reference times the oracle (a CPU restatement of the reference's own PyTorch path) on
+the host cores, all threads, on bounded ray samples of the same workload.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import torch
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd rays/s at 256^3 grid (fused training step)"
+UNIT = "rays/s"
+N_SAMPLES, N_IMPORTANCE, STEPS_UP = 64, 64, 4
+CPU_SAMPLE_RAYS = 1024
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="fused", choices=["fused", "reference"])
+    ap.add_argument("--rays", type=int, default=8192)
+    ap.add_argument("--res", type=int, default=256)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def config(args, world):
+    return {"workload": "training step, 256^3 grid from 128^3 shapes, 8192 rays x (64+4x16) samples per GPU",
+            "grid": args.res, "rays_per_gpu": args.rays, "global_rays": args.rays * world,
+            "samples_per_ray": N_SAMPLES + N_IMPORTANCE, "hash": "16 levels x 2 x 2^19", "mlp": "51-64-3",
+            "band_voxels": 3, "w_eik": 0.1, "w_curv": 5e-4, "perturb": True, "optimizer_step": True,
+            "parallelism": f"dp{world}" if world > 1 else "single",
+            "l2": "working set (grid, hash table, grads, Adam state > 700 MiB) exceeds the 126 MB L2"}
+
+
+def make_scene(res, device, seed=0):
+    from voxneus_b200 import synthetic
+    from voxneus_b200.models import VoxNeuS
+
+    torch.manual_seed(seed)
+    m = VoxNeuS(grid_res=res // 2, occupancy_res=128).to(device)
+    with torch.no_grad():
+        m.sdf_grid.grid.copy_(synthetic.shapes_grid(res // 2, seed=seed).to(device))
+        m.radiance_hash.encoder.embeddings.uniform_(-1e-2, 1e-2)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    m.sdf_grid.scale_volume_grid(res)  # trilinear 128^3 -> 256^3 on the device
+    t1.record()
+    torch.cuda.synchronize()
+    return m, t0.elapsed_time(t1)
+
+
+class ClockSampler:
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 8:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                mx = float(parts[1])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[4:8]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def peak_hbm():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def algorithmic_bytes(name, n_rays, n_samples, res, n_levels=16, ld=52, nnz=None):
+    """Logical global-memory bytes of one launch (each operand counted once; no cache credit)."""
+    P = n_rays * n_samples
+    per = N_IMPORTANCE // STEPS_UP
+    q = N_SAMPLES + (STEPS_UP - 1) * per
+    occ = sum(N_SAMPLES + k * per - 1 for k in range(STEPS_UP))
+    voxels = res ** 3
+    table = {
+        "vx_sample_multistep": n_rays * (24 + 4 * N_SAMPLES + 4 * N_IMPORTANCE + 32 * q + occ + 8 * n_samples),
+        "vx_render_geometry_forward": n_rays * 24 + P * (4 + 128 + 4 + 12 + 4),
+        "vx_appearance_forward": n_rays * 24 + P * (4 + n_levels * 8 * 8 + 12 + 4 * ld),
+        "vx_composite_forward": n_rays * (24 + 32) + P * 48,
+        "vx_composite_backward": n_rays * (24 + 32) + P * 64,
+        "vx_hash_encode_backward": n_rays * 24 + P * (4 + 4 * 2 * n_levels + n_levels * 8 * 16),
+        "vx_render_geometry_backward": n_rays * 24 + P * (4 + 4 + 12 + 12 + 128 + 256),
+        "vx_vr_count": voxels // 8,
+        "vx_reg_stencil": voxels * 12 + voxels // 8,
+    }
+    if nnz is not None:
+        table["vx_masked_adam_upd"] = voxels * 4 + nnz * 24
+    return table.get(name)
+
+
+def load_traffic():
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.json")
+    try:
+        with open(p) as f:
+            return json.load(f)
+    except (OSError, ValueError):
+        return {}
+
+
+def cpu_baseline(args, n_rays=CPU_SAMPLE_RAYS, steps=3):
+    """The oracle's training step on the host cores (bounded sample of the same workload)."""
+    from oracle import reference_path as O
+    from voxneus_b200 import synthetic
+
+    torch.set_num_threads(os.cpu_count() or 1)
+    torch.manual_seed(0)
+    g128 = synthetic.shapes_grid(args.res // 2, seed=0)
+    grid = O.upsample_grid(g128, args.res).clone().requires_grad_(True)
+    emb = (torch.rand(16, 2 ** 19, 2) * 2e-2 - 1e-2).requires_grad_(True)
+    l0 = torch.nn.Linear(51, 64)
+    l1 = torch.nn.Linear(64, 3)
+    sc = O.OracleScene(grid, torch.tensor(0.3, requires_grad=True), emb, l0.weight.detach().clone().requires_grad_(True),
+                       l0.bias.detach().clone().requires_grad_(True), l1.weight.detach().clone().requires_grad_(True),
+                       l1.bias.detach().clone().requires_grad_(True), occupancy=torch.ones(128, 128, 128, dtype=torch.bool))
+    pool = synthetic.RayPool(seed=1)
+    times = []
+    for i in range(steps + 1):
+        o, d = pool.sample(n_rays)
+        tgt = torch.rand(n_rays, 3)
+        t_rand, us = O.sampler_draws(n_rays, N_SAMPLES, N_IMPORTANCE, STEPS_UP, True)
+        t0 = time.perf_counter()
+        sc.train_step(o, d, tgt, band_voxels=3.0, optimize=True, n_samples=N_SAMPLES, n_importance=N_IMPORTANCE,
+                      steps=STEPS_UP, perturb=True, t_rand=t_rand, us=us)
+        if i > 0:
+            times.append(time.perf_counter() - t0)
+    med = statistics.median(times)
+    return {"value": n_rays / med, "unit": UNIT, "cores": torch.get_num_threads(), "kind": "port",
+            "sample": f"{n_rays} rays/step of the 256^3 workload, median of {steps} steps after 1 warm-up "
+                      f"(oracle: the reference's torch ops restated, float32 on CPU)"}, med
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    steps = max(1, min(args.steps, 5))
+    cb, med = cpu_baseline(args, CPU_SAMPLE_RAYS, steps)
+    line = {"metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": args.gpus, "steps": steps,
+            "warmup": 1, "ms_per_step": med * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic", "impl": "reference",
+            "config": config(args, 1), "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_fused(args):
+    from voxneus_b200 import _lib, ops
+    from voxneus_b200 import synthetic
+    from voxneus_b200.rendering import RaySampler
+    from voxneus_b200.training import FusedTrainer
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    exchange = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        from voxneus_b200.dataparallel import GradExchange
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        exchange = GradExchange()
+    _lib.load()
+    torch.backends.cuda.matmul.allow_tf32 = False
+    m, up_ms = make_scene(args.res, dev)
+    tr = FusedTrainer(m, RaySampler(N_SAMPLES, N_IMPORTANCE, perturb=True), band_voxels=3.0, exchange=exchange)
+    pool = synthetic.RayPool(seed=100 + rank)
+    nb = 8
+    batches = []
+    for _ in range(nb):
+        o, d = pool.sample(args.rays)
+        batches.append((o.to(dev), d.to(dev), torch.rand(args.rays, 3).to(dev)))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+
+    # warm-up, with a per-kernel attribution pass on the last warm-up step
+    for i in range(max(args.warmup, 3)):
+        timer = _lib.KernelTimer() if i == max(args.warmup, 3) - 1 else None
+        _lib.set_timer(timer)
+        o, d, t = batches[i % nb]
+        tr.step(o, d, t, step=i)
+        _lib.set_timer(None)
+    torch.cuda.synchronize()
+    per_kernel = {k: sum(v) for k, v in timer.durations_ms().items()}
+    nnz = int((m.sdf_grid.grid.grad != 0).sum().item()) if m.sdf_grid.grid.grad is not None else None
+    sizes = dict(n_rays=args.rays, n_samples=N_SAMPLES + N_IMPORTANCE, res=args.res, nnz=nnz)
+    cands = {k: v for k, v in per_kernel.items() if algorithmic_bytes(k, **sizes) is not None}
+    dominant = max(cands, key=cands.get)
+
+    # timed region: K steps, events around the dominant kernel, clocks sampled alongside
+    dom_timer = _lib.KernelTimer([dominant])
+    l0 = _lib.launch_count()
+    barrier()
+    torch.cuda.synchronize()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        ev0.record()
+        _lib.set_timer(dom_timer)
+        for i in range(args.steps):
+            o, d, t = batches[i % nb]
+            tr.step(o, d, t, step=args.warmup + i)
+        _lib.set_timer(None)
+        ev1.record()
+        torch.cuda.synchronize()
+    barrier()
+    launches = _lib.launch_count() - l0
+    ms = ev0.elapsed_time(ev1) / args.steps
+    if world > 1:
+        import torch.distributed as dist
+
+        t_ms = torch.tensor([ms], device=dev)
+        dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
+        ms = float(t_ms.item())
+    value = args.rays * world / (ms / 1e3)
+    durs = dom_timer.durations_ms()[dominant]
+    dom_ms = sum(durs) / len(durs)
+    ab = algorithmic_bytes(dominant, **sizes)
+    peak, peak_kind = peak_hbm()
+    achieved = ab / (dom_ms / 1e3) / 1e9
+    traffic = load_traffic().get(dominant)
+
+    # end to end through the public API: pinned host rays/targets in, loss out, every step
+    host = [(o.cpu().pin_memory(), d.cpu().pin_memory(), t.cpu().pin_memory()) for o, d, t in batches]
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        ho, hd, ht = host[i % nb]
+        o = ho.to(dev, non_blocking=True)
+        d = hd.to(dev, non_blocking=True)
+        t = ht.to(dev, non_blocking=True)
+        out = tr.step(o, d, t, step=args.warmup + args.steps + i)
+        out["loss_rgb"].item()
+    e2e_s = (time.perf_counter() - t0) / args.steps
+    if world > 1:
+        import torch.distributed as dist
+
+        t_e = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
+        e2e_s = float(t_e.item())
+    e2e = {"value": args.rays * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": args.rays * 9 * 4,
+           "d2h_bytes_per_step": 4, "ms_per_step": e2e_s * 1e3}
+
+    if rank != 0:
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.destroy_process_group()
+        return
+    cb = None
+    if world == 1 and not args.no_cpu_baseline:
+        cb, _ = cpu_baseline(args)
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, rays and targets)",
+            "config": config(args, world), "e2e": e2e, "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "kernel": dominant, "achieved": achieved, "peak": peak, "peak_kind": peak_kind,
+                         "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
+                         "algorithmic_bytes_per_launch": ab, "ms_per_launch": dom_ms},
+            "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(per_kernel.items(), key=lambda x: -x[1])},
+            "grid_upsample_128_to_256_ms": up_ms, "clocks": clk.summary(), "cpu_baseline": cb}
+    print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_fused(args)
+
+
+if __name__ == "__main__":
+    main()

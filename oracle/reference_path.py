@@ -553,6 +553,29 @@ def upsample_grid(grid5: torch.Tensor, new_res) -> torch.Tensor:
 # ---------------------------------------------------------------------------------------
 
 
+def sparse_adam_step(p, grad, state, lr, betas=(0.9, 0.99), eps=1e-8):
+    """SparseGridAdam's torch path (training/optimizer.py:86-113): update only grad != 0 entries."""
+    b1, b2 = betas
+    if not state:
+        state["step"] = 0
+        state["exp_avg"] = torch.zeros_like(p)
+        state["exp_avg_sq"] = torch.zeros_like(p)
+    state["step"] += 1
+    t = state["step"]
+    with torch.no_grad():
+        mask = grad != 0.0
+        if not bool(mask.any()):
+            return
+        g = grad[mask]
+        m = state["exp_avg"][mask] * b1 + (1.0 - b1) * g
+        v = state["exp_avg_sq"][mask] * b2 + (1.0 - b2) * (g * g)
+        state["exp_avg"][mask] = m
+        state["exp_avg_sq"][mask] = v
+        step_size = lr / (1.0 - b1 ** t)
+        den = torch.sqrt(v) / math.sqrt(1.0 - b2 ** t) + eps
+        p[mask] -= step_size * (m / den)
+
+
 class OracleScene:
     """Parameters of one scene with the reference's state_dict naming (models/voxneus.py:21-92)."""
 
@@ -603,7 +626,7 @@ class OracleScene:
         return out
 
     def train_step(self, o, d, target, w_eik=0.1, w_curv=5e-4, band_voxels=None, amplify_k=None,
-                   huber_delta=0.1, **render_kw):
+                   huber_delta=0.1, optimize=False, **render_kw):
         """The timed unit: training/trainer.py:188-326 without the optimizer step.
 
         Returns a dict with losses, |V_R| and the gradients of every parameter.
@@ -627,6 +650,15 @@ class OracleScene:
         amplified = False
         if amplify_k is not None:
             amplified = amplify_s_gradient(self.variance, amplify_k)
+        if optimize:
+            # training/optimizer.py:119-154: SparseGridAdam(0.9, 0.99) for the grid, Adam for the rest
+            if not hasattr(self, "_opt_state"):
+                self._opt_state = {}
+                self._net_opt = torch.optim.Adam([{"params": [self.embeddings], "lr": 0.01},
+                                                  {"params": [self.w0, self.b0, self.w1, self.b1], "lr": 0.001},
+                                                  {"params": [self.variance], "lr": 0.0005}], betas=(0.9, 0.999))
+            sparse_adam_step(self.grid, self.grid.grad, self._opt_state, lr=0.1)
+            self._net_opt.step()
         return {"loss_rgb": loss.detach(), "loss_eik": le, "loss_curv": lc, "n_active": verts.shape[0],
                 "amplified": amplified, "render": out,
                 "grads": {"grid": self.grid.grad.clone(), "variance": self.variance.grad.clone(),

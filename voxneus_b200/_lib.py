@@ -108,11 +108,41 @@ def exported_symbols() -> Sequence[str]:
     return list(_PROTOS) + ["vx_last_error", "vx_version", "vx_launch_count"]
 
 
+class KernelTimer:
+    """CUDA events around selected entry points, recorded on the launching (current) stream."""
+
+    def __init__(self, names=None):
+        self.names = None if names is None else set(names)
+        self.events = {}
+
+    def wants(self, name: str) -> bool:
+        return self.names is None or name in self.names
+
+    def durations_ms(self):
+        return {k: [s.elapsed_time(e) for s, e in v] for k, v in self.events.items()}
+
+
+_timer: Optional[KernelTimer] = None
+
+
+def set_timer(timer: Optional[KernelTimer]) -> None:
+    global _timer
+    _timer = timer
+
+
 def call(name: str, *args):
     """Call an entry point; raise RuntimeError with the library's message on failure."""
     lib = load()
     fn = getattr(lib, name)
-    st = fn(*args)
+    t = _timer
+    if t is not None and t.wants(name):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        st = fn(*args)
+        e.record()
+        t.events.setdefault(name, []).append((s, e))
+    else:
+        st = fn(*args)
     if st != 0:
         msg = lib.vx_last_error().decode(errors="replace")
         raise RuntimeError(f"{name}: {msg}")

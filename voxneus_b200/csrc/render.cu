@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(128) k_composite_fwd(CompArgs a, float* __rest
   const int64_t wpb = blockDim.x >> 5;
   const float s = get_s(a);
   for (int64_t r = blockIdx.x * wpb + (threadIdx.x >> 5); r < a.N; r += (int64_t)gridDim.x * wpb) {
-    float carry = 1.0f;
+    double carry = 1.0;  // double accumulation, rounded once (the CPU cumprod does the same)
     float acc[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // rgb, depth, nsum, opacity
     for (int base = 0; base < a.S; base += 32) {
       const int i = base + lane;
@@ -207,10 +207,10 @@ __global__ void __launch_bounds__(128) k_composite_fwd(CompArgs a, float* __rest
         am = o.am;
         q = fminf(fmaxf(__fadd_rn(__fsub_rn(1.0f, am), 1e-7f), 0.0f), 1.0f);
       }
-      const float inc = warp_incl_prod(q, lane);
-      float T = __shfl_up_sync(0xffffffffu, inc, 1);
-      if (lane == 0) T = 1.0f;
-      T *= carry;
+      const double inc = warp_incl_prod_d((double)q, lane);
+      double Td = __shfl_up_sync(0xffffffffu, inc, 1);
+      if (lane == 0) Td = 1.0;
+      const float T = (float)(Td * carry);
       carry *= __shfl_sync(0xffffffffu, inc, 31);
       if (valid) {
         const int64_t k = r * a.S + i;
@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(128) k_composite_bwd(CompArgs a, CompGrads gr)
   double ds_acc = 0.0;
   for (int64_t r = blockIdx.x * wpb + warp; r < a.N; r += (int64_t)gridDim.x * wpb) {
     // pass 1: alpha, transmittance and the normal sum
-    float carry = 1.0f;
+    double carry = 1.0;  // double accumulation, rounded once (the CPU cumprod does the same)
     float ns[3] = {0.f, 0.f, 0.f};
     for (int base = 0; base < a.S; base += 32) {
       const int i = base + lane;
@@ -308,10 +308,10 @@ __global__ void __launch_bounds__(128) k_composite_bwd(CompArgs a, CompGrads gr)
         am = o.am;
         q = fminf(fmaxf(__fadd_rn(__fsub_rn(1.0f, am), 1e-7f), 0.0f), 1.0f);
       }
-      const float inc = warp_incl_prod(q, lane);
-      float T = __shfl_up_sync(0xffffffffu, inc, 1);
-      if (lane == 0) T = 1.0f;
-      T *= carry;
+      const double inc = warp_incl_prod_d((double)q, lane);
+      double Td = __shfl_up_sync(0xffffffffu, inc, 1);
+      if (lane == 0) Td = 1.0;
+      const float T = (float)(Td * carry);
       carry *= __shfl_sync(0xffffffffu, inc, 31);
       if (i < a.S) {
         T_s[i] = T;
@@ -363,18 +363,18 @@ __global__ void __launch_bounds__(128) k_composite_bwd(CompArgs a, CompGrads gr)
     }
     __syncwarp();
     // reverse exclusive scan over tiles, last tile first: G_i = sum_{j > i} (dT_j T_j)
-    float rcarry = 0.0f;
+    double rcarry = 0.0;
     const int ntiles = (a.S + 31) / 32;
     for (int tI = ntiles - 1; tI >= 0; --tI) {
       const int i = tI * 32 + (31 - lane);  // lane 0 holds the tile's last element
-      const float v = (i < a.S) ? G_s[i] : 0.0f;
-      const float inc = warp_incl_sum(v, lane);
-      float ex = __shfl_up_sync(0xffffffffu, inc, 1);
-      if (lane == 0) ex = 0.0f;
+      const double v = (i < a.S) ? (double)G_s[i] : 0.0;
+      const double inc = warp_incl_sum_d(v, lane);
+      double ex = __shfl_up_sync(0xffffffffu, inc, 1);
+      if (lane == 0) ex = 0.0;
       ex += rcarry;
       rcarry += __shfl_sync(0xffffffffu, inc, 31);
       __syncwarp();
-      if (i < a.S) G_s[i] = ex;
+      if (i < a.S) G_s[i] = (float)ex;
       __syncwarp();
     }
     // pass 3: per-sample adjoint
@@ -518,15 +518,15 @@ __global__ void __launch_bounds__(128) k_composite_weights(const float* __restri
   float* T_s = sm + warp * 2 * S;
   float* G_s = T_s + S;
   for (int64_t r = blockIdx.x * wpb + warp; r < N; r += (int64_t)gridDim.x * wpb) {
-    float carry = 1.0f;
+    double carry = 1.0;  // double accumulation, rounded once (the CPU cumprod does the same)
     for (int base = 0; base < S; base += 32) {
       const int i = base + lane;
       const float am = (i < S) ? alpha[r * S + i] : 0.0f;
       const float q = (i < S) ? fminf(fmaxf(__fadd_rn(__fsub_rn(1.0f, am), 1e-7f), 0.0f), 1.0f) : 1.0f;
-      const float inc = warp_incl_prod(q, lane);
-      float T = __shfl_up_sync(0xffffffffu, inc, 1);
-      if (lane == 0) T = 1.0f;
-      T *= carry;
+      const double inc = warp_incl_prod_d((double)q, lane);
+      double Td = __shfl_up_sync(0xffffffffu, inc, 1);
+      if (lane == 0) Td = 1.0;
+      const float T = (float)(Td * carry);
       carry *= __shfl_sync(0xffffffffu, inc, 31);
       if (i < S) {
         T_s[i] = T;
@@ -543,18 +543,18 @@ __global__ void __launch_bounds__(128) k_composite_weights(const float* __restri
     }
     if (!d_alpha) continue;
     __syncwarp();
-    float rcarry = 0.0f;
+    double rcarry = 0.0;
     const int ntiles = (S + 31) / 32;
     for (int tI = ntiles - 1; tI >= 0; --tI) {
       const int i = tI * 32 + (31 - lane);
-      const float v = (i < S) ? G_s[i] : 0.0f;
-      const float inc = warp_incl_sum(v, lane);
-      float ex = __shfl_up_sync(0xffffffffu, inc, 1);
-      if (lane == 0) ex = 0.0f;
+      const double v = (i < S) ? (double)G_s[i] : 0.0;
+      const double inc = warp_incl_sum_d(v, lane);
+      double ex = __shfl_up_sync(0xffffffffu, inc, 1);
+      if (lane == 0) ex = 0.0;
       ex += rcarry;
       rcarry += __shfl_sync(0xffffffffu, inc, 31);
       __syncwarp();
-      if (i < S) G_s[i] = ex;
+      if (i < S) G_s[i] = (float)ex;
       __syncwarp();
     }
     for (int base = 0; base < S; base += 32) {

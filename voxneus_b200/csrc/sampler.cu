@@ -64,16 +64,18 @@ __device__ void warp_sample_pdf(const WarpArrays& A, int n, int ns, const float*
                                 const float* __restrict__ u_det, int lane, float* out_vals, int64_t* out_idx,
                                 float& my_new, int& my_idx) {
   const int nb = n - 1;  // number of weights
-  float part = 0.0f;
-  for (int i = lane; i < nb; i += 32) part += A.w[i] + 1e-5f;
-  const float total = warp_sum(part);
+  // sums and scans accumulate in double and round once to float, like the reference's CPU
+  // reductions (at::acc_type<float, false> is double)
+  double part = 0.0;
+  for (int i = lane; i < nb; i += 32) part += (double)(A.w[i] + 1e-5f);
+  const float total = (float)warp_sum_d(part);
   // cdf[0] = 0, cdf[i+1] = sum_{j<=i} pdf_j
-  float carry = 0.0f;
+  double carry = 0.0;
   for (int base = 0; base < nb; base += 32) {
     const int i = base + lane;
     const float pdf = (i < nb) ? (A.w[i] + 1e-5f) / total : 0.0f;
-    const float inc = warp_incl_sum(pdf, lane) + carry;
-    if (i < nb) A.cdf[i + 1] = inc;
+    const double inc = warp_incl_sum_d((double)pdf, lane) + carry;
+    if (i < nb) A.cdf[i + 1] = (float)inc;
     carry = __shfl_sync(0xffffffffu, inc, 31);
   }
   if (lane == 0) A.cdf[0] = 0.0f;
@@ -130,16 +132,16 @@ __device__ void warp_upsample_weights(const WarpArrays& A, int n, float inv_s, f
   }
   __syncwarp();
   // exclusive product scan: T_i = prod_{j<i} (1 - alpha_j + 1e-7); w_i = alpha_i T_i
-  float carry = 1.0f;
+  double carry = 1.0;
   for (int base = 0; base < nb; base += 32) {
     const int i = base + lane;
-    const float q = (i < nb) ? A.cdf[i] : 1.0f;
-    const float inc = warp_incl_prod(q, lane);
-    float exc = __shfl_up_sync(0xffffffffu, inc, 1);
-    if (lane == 0) exc = 1.0f;
+    const double q = (i < nb) ? (double)A.cdf[i] : 1.0;
+    const double inc = warp_incl_prod_d(q, lane);
+    double exc = __shfl_up_sync(0xffffffffu, inc, 1);
+    if (lane == 0) exc = 1.0;
     exc *= carry;
     if (i < nb) {
-      float w = A.w[i] * exc;
+      float w = A.w[i] * (float)exc;
       if (oc.mask) {
         const float zm = (A.z[i] + A.z[i + 1]) * 0.5f;
         const float occ = occupied(oc, ray_at(ox, dx, zm), ray_at(oy, dy, zm), ray_at(oz, dz, zm)) ? 1.0f : 0.0f;

@@ -78,8 +78,9 @@ class FusedTrainer:
                  w_curv: float = 5e-4, band_voxels: Optional[float] = None, relax_radius: float = 1.2,
                  amplify_k: float = 5.0, s_warmup_steps: int = 5000, total_steps: int = 40000, lr_sdf: float = 0.1,
                  lr_hash: float = 0.01, lr_mlp: float = 0.001, lr_variance: float = 0.0005, up_sample_steps: int = 4,
-                 huber_delta: float = 0.1, optimize: bool = True):
+                 huber_delta: float = 0.1, optimize: bool = True, exchange=None):
         self.model = model
+        self.exchange = exchange  # dataparallel.GradExchange for world_size > 1
         self.sampler = sampler or RaySampler(64, 64, perturb=True)
         self.w_eik, self.w_curv = w_eik, w_curv
         self.relax_radius = relax_radius
@@ -113,11 +114,19 @@ class FusedTrainer:
         self.bitmap.zero_()
         self.counts.zero_()
         amp_k = self.amplify_k if step >= self.s_warmup_steps else 0.0
+        ex = self.exchange
         out = m.render(rays_o, rays_d, self.sampler, None, None, up_sample_steps=self.up_sample_steps,
-                       sphere_radius=1.0, randoms=randoms, vr_bitmap=self.bitmap, extras=False, amplify_k=amp_k,
-                       amp_flag=self.amp_flag)
+                       sphere_radius=1.0, randoms=randoms, vr_bitmap=self.bitmap, extras=False,
+                       amplify_k=0.0 if ex is not None else amp_k, amp_flag=self.amp_flag)
         loss = compute_huber_color_loss(out["rgb"], target, self.huber_delta)
         loss.backward()
+        if ex is not None:
+            from .dataparallel import amplify_after_reduce
+
+            ex.reduce_grads(list(m.parameters()))
+            ex.union_bitmap(self.bitmap)
+            if amp_k > 0:
+                self.amp_flag.copy_(amplify_after_reduce(m.variance_net.variance, amp_k).reshape(1).int())
         grid = m.sdf_grid.grid
         lo, hi = m.sdf_grid.bounds()
         ops.vr_count(self.bitmap, grid.detach(), self.res, lo, hi, self.relax_radius, self.band, self.counts)
