@@ -58,14 +58,33 @@ __device__ void reduce_losses(const RegOut& o, double e, double c, double n) {
     is_last = (atomicAdd(o.counter, 1u) == nblocks - 1);
   }
   __syncthreads();
-  if (is_last && tid == 0) {
-    __threadfence();
-    const volatile double* p = o.partials;
-    double a = 0, b = 0, k = 0;
-    for (unsigned i = 0; i < nblocks; ++i) {
-      a += p[3 * i];
-      b += p[3 * i + 1];
-      k += p[3 * i + 2];
+  if (!is_last) return;
+  // last block: every thread sums a fixed strided subset, then a fixed-order warp/block tree
+  // (deterministic for a given launch shape)
+  __threadfence();
+  const volatile double* p = o.partials;
+  double a = 0, b = 0, k = 0;
+  for (unsigned i = tid; i < nblocks; i += nthreads) {
+    a += p[3 * i];
+    b += p[3 * i + 1];
+    k += p[3 * i + 2];
+  }
+  a = warp_sum_d(a);
+  b = warp_sum_d(b);
+  k = warp_sum_d(k);
+  __syncthreads();
+  if (wl == 0) {
+    s[0][ww] = a;
+    s[1][ww] = b;
+    s[2][ww] = k;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    a = b = k = 0;
+    for (int w = 0; w < (nthreads + 31) / 32; ++w) {
+      a += s[0][w];
+      b += s[1][w];
+      k += s[2][w];
     }
     if (o.losses) {
       o.losses[0] = k > 0 ? (float)(a / k) : 0.0f;

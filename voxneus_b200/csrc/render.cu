@@ -442,11 +442,18 @@ __global__ void __launch_bounds__(128) k_composite_bwd(CompArgs a, CompGrads gr)
     is_last = (prev == gridDim.x - 1);
   }
   __syncthreads();
-  if (is_last && threadIdx.x == 0) {
-    __threadfence();
+  if (!is_last) return;
+  __threadfence();
+  double part = 0.0;
+  const volatile double* p = gr.partials;
+  for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) part += p[b];
+  part = warp_sum_d(part);
+  __syncthreads();
+  if (lane == 0) ds_warp[warp] = part;
+  __syncthreads();
+  if (threadIdx.x == 0) {
     double tot = 0.0;
-    const volatile double* p = gr.partials;
-    for (unsigned b = 0; b < gridDim.x; ++b) tot += p[b];
+    for (int w = 0; w < (int)wpb; ++w) tot += ds_warp[w];
     float out = (float)tot;
     if (a.s_is_var) {
       // s = clamp(exp(10 v), 1e-4, s_max): dv = ds * exp(10 v) * 10 inside the clamp range
