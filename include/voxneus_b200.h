@@ -178,6 +178,26 @@ int vx_hash_encode_backward(float* table_grad, int n_levels, int log2_size, int 
                             const float xyz_max[3], int64_t n_points, const float* d_out, int64_t ld_d,
                             void* stream);
 
+/* Radiance MLP (models/radiance_mlp.py:42-53,81-98): rows x (n_points, in_dim) with row stride
+ * ldx -> Linear(51,64) -> ReLU -> Linear(64,3) -> Sigmoid -> colors (n_points, 3). W0 (64,51),
+ * b0 (64), W1 (3,64), b1 (3) as nn.Linear stores them. Only the 51 -> 64 -> 3 shape is fused. */
+int vx_radiance_mlp_forward(const float* x, int64_t ldx, int64_t n_points, int in_dim, int hidden, int out_dim,
+                            const float* W0, const float* b0, const float* W1, const float* b1, float* colors,
+                            void* stream);
+
+/* Blocks of vx_radiance_mlp_backward and the floats of one block's weight-gradient partial. */
+int vx_mlp_blocks(int64_t n_points);
+int vx_mlp_partial_floats(void);
+
+/* Adjoint of vx_radiance_mlp_forward (recomputes the hidden layer): d_colors (n,3) -> d_hash (n,32)
+ * (gradient of input columns 0..31), d_normal (n,3) (columns 48..50), and the weight gradients
+ * dW0, db0, dW1, db1 (written, not accumulated; summed over blocks in a fixed order).
+ * partials: >= vx_mlp_blocks(n) * vx_mlp_partial_floats() floats. */
+int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int in_dim, int hidden, int out_dim,
+                             const float* W0, const float* b0, const float* W1, const float* b1, const float* d_colors,
+                             float* d_hash, float* d_normal, float* dW0, float* db0, float* dW1, float* db1,
+                             float* partials, int64_t n_partial_floats, void* stream);
+
 /* ---------------------------------------------------------- render (per ray) --------------- */
 
 /* Blocks used by the per-ray kernels; vx_composite_backward's partials hold one double per block. */

@@ -46,6 +46,10 @@ _PROTOS = {
     "vx_appearance_forward": [P, I32, I32, I32, HI3, HF3, P, P, P, P, I32, HF3, HF3, I64, P, I64, I32, P, I64, I32,
                               P, I32, P],
     "vx_hash_encode_backward": [P, I32, I32, I32, HI3, HF3, P, P, P, P, I32, HF3, HF3, I64, P, I64, P],
+    "vx_radiance_mlp_forward": [P, I64, I64, I32, I32, I32, P, P, P, P, P, P],
+    "vx_mlp_blocks": [I64],
+    "vx_mlp_partial_floats": [],
+    "vx_radiance_mlp_backward": [P, I64, I64, I32, I32, I32, P, P, P, P, P, P, P, P, P, P, P, P, I64, P],
     "vx_composite_workspace_blocks": [I64],
     "vx_composite_forward": [P, P, P, P, I64, I64, P, P, P, P, P, I32, F32, F32, P, I32, I32, F32, I64, I32, P, P, P,
                              P, P, P, P, P],

@@ -1,0 +1,379 @@
+// Radiance MLP [hash 32 | SH 16 | normal 3] -> 64 ReLU -> 3 Sigmoid (models/radiance_mlp.py:42-53,
+// 81-98) as two fused FP32 kernels: the forward writes only the colours; the adjoint recomputes
+// the hidden layer, writes dL/d(hash features) and dL/d(normal), and reduces the weight gradients
+// into per-block partials that a second kernel sums in a fixed order (deterministic).
+//
+// Both kernels stage a 128-sample tile of input rows in shared memory and run the 51 -> 64 layer
+// as a register-tiled SIMT GEMM: thread (lane, warp) owns samples 4*lane..4*lane+3 and hidden
+// units 8*warp..8*warp+7, reading the inputs as 16-byte shared loads and the weights as
+// warp-broadcast loads. FP32 throughout (the parity bar of the colours is 1e-5 relative).
+#include "common.cuh"
+
+namespace vx {
+
+constexpr int KIN = 51;   // input features
+constexpr int KP = 52;    // padded
+constexpr int NH = 64;    // hidden units
+constexpr int NO = 3;     // colours
+constexpr int TM = 128;   // samples per tile
+constexpr int DZS = 132;  // row stride of the transposed dL/dz tile (16-byte aligned rows)
+constexpr int XRS = 53;   // row stride of the row-major input tile
+constexpr int NDX = 35;   // input gradients produced: hash columns 0..31, normal columns 48..50
+constexpr int WG = NH * KP + NO * NH + NH + NO;  // per-block weight-gradient partial size
+
+struct MlpW {
+  const float* W0;  // (64, 51)
+  const float* b0;  // (64)
+  const float* W1;  // (3, 64)
+  const float* b1;  // (3)
+};
+
+__device__ __forceinline__ void load_weights(const MlpW& w, float (*W0T)[NH], float* B0, float (*W1s)[NH], float* B1,
+                                             int tid, int nthreads) {
+  for (int i = tid; i < KP * NH; i += nthreads) {
+    const int k = i / NH, n = i % NH;
+    W0T[k][n] = (k < KIN) ? w.W0[n * KIN + k] : 0.0f;
+  }
+  for (int i = tid; i < NH; i += nthreads) B0[i] = w.b0[i];
+  for (int i = tid; i < NO * NH; i += nthreads) W1s[i / NH][i % NH] = w.W1[i];
+  if (tid < NO) B1[tid] = w.b1[tid];
+}
+
+// hidden pre-activations z[s][j] for samples 4*tm+s, units 8*tn+j
+__device__ __forceinline__ void layer0(const float (*XT)[TM], const float (*W0T)[NH], const float* B0, int tm, int tn,
+                                       float z[4][8]) {
+#pragma unroll
+  for (int s = 0; s < 4; ++s)
+#pragma unroll
+    for (int j = 0; j < 8; ++j) z[s][j] = B0[8 * tn + j];
+#pragma unroll 4
+  for (int k = 0; k < KIN; ++k) {
+    const float4 a = *reinterpret_cast<const float4*>(&XT[k][4 * tm]);
+    const float4 w0 = *reinterpret_cast<const float4*>(&W0T[k][8 * tn]);
+    const float4 w1 = *reinterpret_cast<const float4*>(&W0T[k][8 * tn + 4]);
+    const float av[4] = {a.x, a.y, a.z, a.w};
+    const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) z[s][j] = fmaf(av[s], wv[j], z[s][j]);
+  }
+}
+
+// Stage rows m0..m0+127 (row stride ldx) as XT[k][m] (and XR[m][k] when given).
+__device__ __forceinline__ void load_tile(const float* __restrict__ X, int64_t ldx, int64_t P, int64_t m0,
+                                          float (*XT)[TM], float (*XR)[XRS], int tid) {
+  if (tid < TM) {
+    const int64_t m = m0 + tid;
+    const bool ok = m < P;
+    const float* row = X + m * ldx;
+#pragma unroll 4
+    for (int k = 0; k < KP; ++k) {
+      const float v = (ok && k < KIN) ? __ldg(row + k) : 0.0f;
+      XT[k][tid] = v;
+      if (XR) XR[tid][k] = v;
+    }
+  }
+}
+
+__global__ void __launch_bounds__(256) k_mlp_fwd(const float* __restrict__ X, int64_t ldx, int64_t P, MlpW w,
+                                                 float* __restrict__ out) {
+  __shared__ __align__(16) float XT[KP][TM];
+  __shared__ __align__(16) float W0T[KP][NH];
+  __shared__ float B0[NH], W1s[NO][NH], B1[NO];
+  const int tid = threadIdx.x, tm = tid & 31, tn = tid >> 5;
+  load_weights(w, W0T, B0, W1s, B1, tid, blockDim.x);
+  const int64_t ntiles = (P + TM - 1) / TM;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t m0 = t * TM;
+    __syncthreads();
+    load_tile(X, ldx, P, m0, XT, nullptr, tid);
+    __syncthreads();
+    float z[4][8];
+    layer0(XT, W0T, B0, tm, tn, z);
+    float part[4][NO];
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int c = 0; c < NO; ++c) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc = fmaf(W1s[c][8 * tn + j], fmaxf(z[s][j], 0.0f), acc);
+        part[s][c] = acc;
+      }
+    __syncthreads();  // XT reads done: reuse it for the layer-1 partial sums
+    float* red = &XT[0][0];
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int c = 0; c < NO; ++c) red[(tn * TM + 4 * tm + s) * NO + c] = part[s][c];
+    __syncthreads();
+    if (tid < TM && m0 + tid < P) {
+#pragma unroll
+      for (int c = 0; c < NO; ++c) {
+        float o = B1[c];
+#pragma unroll
+        for (int g = 0; g < 8; ++g) o += red[(g * TM + tid) * NO + c];
+        out[(m0 + tid) * NO + c] = sigmoidf_ref(o);
+      }
+    }
+  }
+}
+
+// Adjoint. d_out (P,3) -> d_hash (P,32), d_normal (P,3), per-block weight-gradient partials.
+__global__ void __launch_bounds__(256, 2) k_mlp_bwd(const float* __restrict__ X, int64_t ldx, int64_t P, MlpW w,
+                                                 const float* __restrict__ d_out, float* __restrict__ d_hash,
+                                                 float* __restrict__ d_normal, float* __restrict__ partials) {
+  extern __shared__ __align__(16) float smem[];
+  float(*XT)[TM] = reinterpret_cast<float(*)[TM]>(smem);                  // KP x TM
+  float(*XR)[XRS] = reinterpret_cast<float(*)[XRS]>(smem + KP * TM);      // TM x XRS
+  float(*DZT)[DZS] = reinterpret_cast<float(*)[DZS]>(smem + KP * TM + TM * XRS);  // NH x DZS
+  float(*W0T)[NH] = reinterpret_cast<float(*)[NH]>(smem + KP * TM + TM * XRS + NH * DZS);
+  float* B0 = smem + KP * TM + TM * XRS + NH * DZS + KP * NH;
+  float(*W1s)[NH] = reinterpret_cast<float(*)[NH]>(B0 + NH);
+  float* B1 = B0 + NH + NO * NH;
+  float(*DO)[NO] = reinterpret_cast<float(*)[NO]>(B1 + 4);
+  const int tid = threadIdx.x, tm = tid & 31, tn = tid >> 5;
+  load_weights(w, W0T, B0, W1s, B1, tid, blockDim.x);
+  // weight-gradient accumulators (across all tiles of this block)
+  float gW0[8][2];  // units 8*tn+j, input columns lane and lane+32
+#pragma unroll
+  for (int j = 0; j < 8; ++j) gW0[j][0] = gW0[j][1] = 0.0f;
+  float gW1[NO][8], gB0[8], gB1[NO];
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    gB0[j] = 0.0f;
+#pragma unroll
+    for (int c = 0; c < NO; ++c) gW1[c][j] = 0.0f;
+  }
+#pragma unroll
+  for (int c = 0; c < NO; ++c) gB1[c] = 0.0f;
+  const int64_t ntiles = (P + TM - 1) / TM;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t m0 = t * TM;
+    __syncthreads();
+    load_tile(X, ldx, P, m0, XT, XR, tid);
+    if (tid < TM) {
+#pragma unroll
+      for (int c = 0; c < NO; ++c) DO[tid][c] = (m0 + tid < P) ? d_out[(m0 + tid) * NO + c] : 0.0f;
+    }
+    __syncthreads();
+    float z[4][8];
+    layer0(XT, W0T, B0, tm, tn, z);
+    // recompute the colours for the sigmoid adjoint
+    float* red = &DZT[0][0];
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int c = 0; c < NO; ++c) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc = fmaf(W1s[c][8 * tn + j], fmaxf(z[s][j], 0.0f), acc);
+        red[(tn * TM + 4 * tm + s) * NO + c] = acc;
+      }
+    __syncthreads();
+    if (tid < TM) {
+#pragma unroll
+      for (int c = 0; c < NO; ++c) {
+        float o = B1[c];
+#pragma unroll
+        for (int g = 0; g < 8; ++g) o += red[(g * TM + tid) * NO + c];
+        const float y = sigmoidf_ref(o);
+        DO[tid][c] = DO[tid][c] * ((1.0f - y) * y);  // dL/d(pre-sigmoid)
+      }
+    }
+    __syncthreads();
+    // dL/dh, ReLU adjoint, bias and layer-1 weight gradients; dL/dz staged transposed
+#pragma unroll
+    for (int s = 0; s < 4; ++s) {
+      const int m = 4 * tm + s;
+      const float d0 = DO[m][0], d1 = DO[m][1], d2 = DO[m][2];
+      if (tn == 0) {
+        gB1[0] += d0;
+        gB1[1] += d1;
+        gB1[2] += d2;
+      }
+#pragma unroll
+      for (int j = 0; j < 8; ++j) {
+        const int n = 8 * tn + j;
+        const float h = fmaxf(z[s][j], 0.0f);
+        gW1[0][j] = fmaf(d0, h, gW1[0][j]);
+        gW1[1][j] = fmaf(d1, h, gW1[1][j]);
+        gW1[2][j] = fmaf(d2, h, gW1[2][j]);
+        const float dh = d0 * W1s[0][n] + d1 * W1s[1][n] + d2 * W1s[2][n];
+        const float dz = (h > 0.0f) ? dh : 0.0f;
+        gB0[j] += dz;
+        z[s][j] = dz;
+      }
+    }
+#pragma unroll
+    for (int j = 0; j < 8; ++j)
+      *reinterpret_cast<float4*>(&DZT[8 * tn + j][4 * tm]) = make_float4(z[0][j], z[1][j], z[2][j], z[3][j]);
+    __syncthreads();
+    // dW0[n][k] += sum_m dz[m][n] x[m][k]: units 8*tn.., columns lane and lane+32
+    {
+      const int k0 = tm, k1 = tm + 32;
+      const bool has1 = k1 < KIN;
+#pragma unroll 4
+      for (int m = 0; m < TM; ++m) {
+        const float x0 = XR[m][k0];
+        const float x1 = has1 ? XR[m][k1] : 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) {
+          const float dz = DZT[8 * tn + j][m];
+          gW0[j][0] = fmaf(dz, x0, gW0[j][0]);
+          gW0[j][1] = fmaf(dz, x1, gW0[j][1]);
+        }
+      }
+    }
+    // dX[m][k] = sum_n dz[m][n] W0[n][k] for the 35 needed columns: q = 5*tn + i
+    float dx[4][5];
+    int kc[5];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const int q = 5 * tn + i;
+      kc[i] = q < 32 ? q : (q < NDX ? q + 16 : -1);
+#pragma unroll
+      for (int s = 0; s < 4; ++s) dx[s][i] = 0.0f;
+    }
+#pragma unroll 4
+    for (int n = 0; n < NH; ++n) {
+      const float4 d = *reinterpret_cast<const float4*>(&DZT[n][4 * tm]);
+#pragma unroll
+      for (int i = 0; i < 5; ++i) {
+        const float wv = kc[i] >= 0 ? W0T[kc[i]][n] : 0.0f;
+        dx[0][i] = fmaf(d.x, wv, dx[0][i]);
+        dx[1][i] = fmaf(d.y, wv, dx[1][i]);
+        dx[2][i] = fmaf(d.z, wv, dx[2][i]);
+        dx[3][i] = fmaf(d.w, wv, dx[3][i]);
+      }
+    }
+    __syncthreads();  // XR reads (dW0) done: stage dX rows in XR
+#pragma unroll
+    for (int i = 0; i < 5; ++i) {
+      const int q = 5 * tn + i;
+      if (q < NDX) {
+#pragma unroll
+        for (int s = 0; s < 4; ++s) XR[4 * tm + s][q] = dx[s][i];
+      }
+    }
+    __syncthreads();
+    for (int e = tid; e < TM * 32; e += blockDim.x) {
+      const int m = e >> 5, k = e & 31;
+      if (m0 + m < P) d_hash[(m0 + m) * 32 + k] = XR[m][k];
+    }
+    for (int e = tid; e < TM * 3; e += blockDim.x) {
+      const int m = e / 3, c = e % 3;
+      if (m0 + m < P) d_normal[(m0 + m) * 3 + c] = XR[m][32 + c];
+    }
+  }
+  // per-block weight-gradient partials: [dW0 (64 x 52) | dW1 (3 x 64) | db0 (64) | db1 (3)]
+  float* pb = partials + (int64_t)blockIdx.x * WG;
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+    const int n = 8 * tn + j;
+    pb[n * KP + tm] = gW0[j][0];
+    if (tm + 32 < KP) pb[n * KP + tm + 32] = gW0[j][1];
+  }
+#pragma unroll
+  for (int j = 0; j < 8; ++j) {
+#pragma unroll
+    for (int c = 0; c < NO; ++c) gW1[c][j] = warp_sum(gW1[c][j]);
+    gB0[j] = warp_sum(gB0[j]);
+  }
+#pragma unroll
+  for (int c = 0; c < NO; ++c) gB1[c] = warp_sum(gB1[c]);
+  if (tm == 0) {
+#pragma unroll
+    for (int j = 0; j < 8; ++j) {
+      const int n = 8 * tn + j;
+#pragma unroll
+      for (int c = 0; c < NO; ++c) pb[NH * KP + c * NH + n] = gW1[c][j];
+      pb[NH * KP + NO * NH + n] = gB0[j];
+    }
+    if (tn == 0) {
+#pragma unroll
+      for (int c = 0; c < NO; ++c) pb[NH * KP + NO * NH + NH + c] = gB1[c];
+    }
+  }
+}
+
+// Sum the per-block partials in block order into dW0 (64,51), dW1 (3,64), db0 (64), db1 (3).
+__global__ void k_mlp_wgrad_reduce(const float* __restrict__ partials, int nblocks, float* __restrict__ dW0,
+                                   float* __restrict__ db0, float* __restrict__ dW1, float* __restrict__ db1) {
+  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < WG; e += gridDim.x * blockDim.x) {
+    double acc = 0.0;
+    for (int b = 0; b < nblocks; ++b) acc += (double)partials[(int64_t)b * WG + e];
+    const float v = (float)acc;
+    if (e < NH * KP) {
+      const int n = e / KP, k = e % KP;
+      if (k < KIN) dW0[n * KIN + k] = v;
+    } else if (e < NH * KP + NO * NH) {
+      dW1[e - NH * KP] = v;
+    } else if (e < NH * KP + NO * NH + NH) {
+      db0[e - NH * KP - NO * NH] = v;
+    } else {
+      db1[e - NH * KP - NO * NH - NH] = v;
+    }
+  }
+}
+
+constexpr size_t kBwdSmem =
+    sizeof(float) * (KP * TM + TM * XRS + NH * DZS + KP * NH + NH + NO * NH + 4 + TM * NO);
+
+}  // namespace vx
+
+using namespace vx;
+
+extern "C" {
+
+int vx_mlp_blocks(int64_t n_points) {
+  const int64_t tiles = (n_points + TM - 1) / TM;
+  const int64_t cap = (int64_t)kSMs * 2;
+  return (int)(tiles < 1 ? 1 : (tiles < cap ? tiles : cap));
+}
+
+int vx_mlp_partial_floats(void) { return WG; }
+
+int vx_radiance_mlp_forward(const float* x, int64_t ldx, int64_t n_points, int in_dim, int hidden, int out_dim,
+                            const float* W0, const float* b0, const float* W1, const float* b1, float* colors,
+                            void* stream) {
+  VX_REQUIRE(in_dim == KIN && hidden == NH && out_dim == NO, "the fused MLP is %d -> %d -> %d (got %d -> %d -> %d)",
+             KIN, NH, NO, in_dim, hidden, out_dim);
+  VX_REQUIRE(n_points >= 0 && ldx >= KIN, "bad sizes");
+  if (n_points == 0) return VX_OK;
+  VX_REQUIRE(x && W0 && b0 && W1 && b1 && colors, "null pointer");
+  MlpW w{W0, b0, W1, b1};
+  const int64_t tiles = (n_points + TM - 1) / TM;
+  const unsigned blocks = (unsigned)(tiles < (int64_t)kSMs * 4 ? tiles : (int64_t)kSMs * 4);
+  k_mlp_fwd<<<blocks, 256, 0, (cudaStream_t)stream>>>(x, ldx, n_points, w, colors);
+  count_launches(1);
+  return check_launch("radiance_mlp_forward");
+}
+
+int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int in_dim, int hidden, int out_dim,
+                             const float* W0, const float* b0, const float* W1, const float* b1, const float* d_colors,
+                             float* d_hash, float* d_normal, float* dW0, float* db0, float* dW1, float* db1,
+                             float* partials, int64_t n_partial_floats, void* stream) {
+  VX_REQUIRE(in_dim == KIN && hidden == NH && out_dim == NO, "the fused MLP is %d -> %d -> %d", KIN, NH, NO);
+  VX_REQUIRE(n_points >= 0 && ldx >= KIN, "bad sizes");
+  VX_REQUIRE(x && W0 && b0 && W1 && b1 && d_colors && d_hash && d_normal && dW0 && db0 && dW1 && db1 && partials,
+             "null pointer");
+  const int nb = vx_mlp_blocks(n_points);
+  VX_REQUIRE(n_partial_floats >= (int64_t)nb * WG, "partials buffer holds %lld floats, need %lld",
+             (long long)n_partial_floats, (long long)nb * WG);
+  MlpW w{W0, b0, W1, b1};
+  cudaStream_t st = (cudaStream_t)stream;
+  cudaError_t e = cudaFuncSetAttribute(k_mlp_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmem);
+  if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "radiance_mlp_backward: %s", cudaGetErrorString(e));
+  if (n_points > 0) {
+    k_mlp_bwd<<<nb, 256, kBwdSmem, st>>>(x, ldx, n_points, w, d_colors, d_hash, d_normal, partials);
+  } else {
+    cudaMemsetAsync(partials, 0, sizeof(float) * WG, st);
+  }
+  k_mlp_wgrad_reduce<<<(WG + 255) / 256, 256, 0, st>>>(partials, n_points > 0 ? nb : 1, dW0, db0, dW1, db1);
+  count_launches(2);
+  return check_launch("radiance_mlp_backward");
+}
+
+}  // extern "C"

@@ -188,100 +188,171 @@ __device__ __forceinline__ bool vr_member(const StencilArgs& a, int x, int y, in
   return true;
 }
 
-// blockDim = (32, 4, 2); each thread owns output voxels (z, y, x) and (z, y, x + 2).
-__global__ void __launch_bounds__(256) k_reg_stencil(StencilArgs a, RegOut o) {
+// Does the halo-1 box of a tile hold any V_R bit? Word-level test, one thread per (x, y) row of
+// the box (z range [z0-1, z0+TZ] covers at most 3 words).
+__device__ __forceinline__ bool tile_has_bits(const StencilArgs& a, int x0, int y0, int z0, int tid) {
+  bool hit = false;
+  if (tid < MX * MY) {
+    const int x = x0 - 1 + tid / MY, y = y0 - 1 + tid % MY;
+    if (x >= 0 && x < a.g.rx && y >= 0 && y < a.g.ry) {
+      const int zlo = max(z0 - 1, 0), zhi = min(z0 + TZ, a.g.rz - 1);
+      const int b0 = lin3(a.g, x, y, zlo), b1 = lin3(a.g, x, y, zhi);
+      for (int w = b0 >> 5; w <= (b1 >> 5); ++w) {
+        uint32_t m = 0xffffffffu;
+        if (w == (b0 >> 5)) m &= 0xffffffffu << (b0 & 31);
+        if (w == (b1 >> 5)) m &= 0xffffffffu >> (31 - (b1 & 31));
+        hit |= (__ldg(a.bm + w) & m) != 0u;
+      }
+    }
+  }
+  return hit;
+}
+
+// Persistent grid over 32x4x4 tiles; blockDim = (32, 4, 2), each thread owns output voxels
+// (z, y, x) and (z, y, x + 2) of the current tile. Tiles whose halo box holds no V_R bit are
+// skipped after one word-level test. Per-block loss partials; k_reg_finalize reduces them.
+__global__ void __launch_bounds__(256) k_reg_stencil(StencilArgs a, double* __restrict__ partials, int ntiles) {
   __shared__ float F[HX][HY][HZ];
   __shared__ uint8_t M[MX][MY][MZ];
-  const int tz = blockIdx.x % a.tiles_z;
-  const int ty = (blockIdx.x / a.tiles_z) % a.tiles_y;
-  const int tx = blockIdx.x / (a.tiles_z * a.tiles_y);
-  const int z0 = tz * TZ, y0 = ty * TY, x0 = tx * TX;
+  __shared__ double red[3][8];
   const int tid = threadIdx.x + 32 * (threadIdx.y + 4 * threadIdx.z);
-  const unsigned long long nv = a.counts[a.band > 0.0f ? ((a.relax_r > 0.0f && a.counts[1] > 0) ? 3 : 2)
-                                                       : ((a.relax_r > 0.0f && a.counts[1] > 0) ? 1 : 0)];
   const bool relax_on = a.relax_r > 0.0f && a.counts[1] > 0;
-  // active interior mask of the halo-1 box
-  int any = 0;
-  for (int q = tid; q < MX * MY * MZ; q += 256) {
-    const int mz = q % MZ, my = (q / MZ) % MY, mx = q / (MZ * MY);
-    const int x = x0 - 1 + mx, y = y0 - 1 + my, z = z0 - 1 + mz;
-    uint8_t m = 0;
-    if (x >= 1 && x <= a.g.rx - 2 && y >= 1 && y <= a.g.ry - 2 && z >= 1 && z <= a.g.rz - 2)
-      m = vr_member(a, x, y, z, relax_on) ? 1 : 0;
-    M[mx][my][mz] = m;
-    any |= m;
-  }
-  if (!__syncthreads_or(any)) {
-    reduce_losses(o, 0.0, 0.0, 0.0);
-    return;
-  }
-  for (int q = tid; q < HX * HY * HZ; q += 256) {
-    const int hz = q % HZ, hy = (q / HZ) % HY, hx = q / (HZ * HY);
-    const int x = x0 - 2 + hx, y = y0 - 2 + hy, z = z0 - 2 + hz;
-    float v = 0.0f;
-    if (x >= 0 && x < a.g.rx && y >= 0 && y < a.g.ry && z >= 0 && z < a.g.rz) v = __ldg(a.f + lin3(a.g, x, y, z));
-    F[hx][hy][hz] = v;
-  }
-  __syncthreads();
+  const unsigned long long nv = a.counts[a.band > 0.0f ? (relax_on ? 3 : 2) : (relax_on ? 1 : 0)];
   const float inv_nv = nv > 0 ? 2.0f / (float)nv : 0.0f;
   const float dx = 2.0f * a.g.eps[0], dy = 2.0f * a.g.eps[1], dz = 2.0f * a.g.eps[2];
   const float ex2 = a.g.eps[0] * a.g.eps[0], ey2 = a.g.eps[1] * a.g.eps[1], ez2 = a.g.eps[2] * a.g.eps[2];
   const float sc = inv_nv * a.w_curv;
   double le = 0, lc = 0, ln = 0;
-  const int lz = threadIdx.x, ly = threadIdx.y;
+  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int tz = t % a.tiles_z;
+    const int ty = (t / a.tiles_z) % a.tiles_y;
+    const int tx = t / (a.tiles_z * a.tiles_y);
+    const int z0 = tz * TZ, y0 = ty * TY, x0 = tx * TX;
+    if (!__syncthreads_or(tile_has_bits(a, x0, y0, z0, tid))) continue;
+    // active interior mask of the halo-1 box
+    for (int q = tid; q < MX * MY * MZ; q += 256) {
+      const int mz = q % MZ, my = (q / MZ) % MY, mx = q / (MZ * MY);
+      const int x = x0 - 1 + mx, y = y0 - 1 + my, z = z0 - 1 + mz;
+      uint8_t m = 0;
+      if (x >= 1 && x <= a.g.rx - 2 && y >= 1 && y <= a.g.ry - 2 && z >= 1 && z <= a.g.rz - 2)
+        m = vr_member(a, x, y, z, relax_on) ? 1 : 0;
+      M[mx][my][mz] = m;
+    }
+    for (int q = tid; q < HX * HY * HZ; q += 256) {
+      const int hz = q % HZ, hy = (q / HZ) % HY, hx = q / (HZ * HY);
+      const int x = x0 - 2 + hx, y = y0 - 2 + hy, z = z0 - 2 + hz;
+      float v = 0.0f;
+      if (x >= 0 && x < a.g.rx && y >= 0 && y < a.g.ry && z >= 0 && z < a.g.rz) v = __ldg(a.f + lin3(a.g, x, y, z));
+      F[hx][hy][hz] = v;
+    }
+    __syncthreads();
+    const int lz = threadIdx.x, ly = threadIdx.y;
 #pragma unroll
-  for (int rep = 0; rep < 2; ++rep) {
-    const int lx = threadIdx.z + 2 * rep;
-    const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
-    if (x >= a.g.rx || y >= a.g.ry || z >= a.g.rz) continue;
-    // SDF box coordinates of this voxel: (lx+2, ly+2, lz+2); mask box: (lx+1, ly+1, lz+1)
-    float acc = 0.0f;
-    bool touched = false;
-    // contribution of vertex v at mask-box (mx,my,mz) along axis ax with sign +1 when the
-    // output voxel is v + e_ax, -1 when it is v - e_ax; 0 means v itself (curvature centre)
+    for (int rep = 0; rep < 2; ++rep) {
+      const int lx = threadIdx.z + 2 * rep;
+      const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+      if (x >= a.g.rx || y >= a.g.ry || z >= a.g.rz) continue;
+      // SDF box coordinates of this voxel: (lx+2, ly+2, lz+2); mask box: (lx+1, ly+1, lz+1)
+      float acc = 0.0f;
+      bool touched = false;
+      // vertex v = voxel + sgn * e_ax contributes to this voxel; nb == 0 is v = voxel itself
 #pragma unroll
-    for (int nb = 0; nb < 7; ++nb) {
-      const int ax = nb == 0 ? -1 : (nb - 1) >> 1;
-      const int sgn = nb == 0 ? 0 : (((nb - 1) & 1) ? 1 : -1);  // v = voxel + sgn * e_ax
-      const int mx = lx + 1 + (ax == 0 ? sgn : 0);
-      const int my = ly + 1 + (ax == 1 ? sgn : 0);
-      const int mz = lz + 1 + (ax == 2 ? sgn : 0);
-      if (!M[mx][my][mz]) continue;
-      touched = true;
-      const int hx = mx + 1, hy = my + 1, hz = mz + 1;
-      const float fc = F[hx][hy][hz];
-      const float fxp = F[hx + 1][hy][hz], fxm = F[hx - 1][hy][hz];
-      const float fyp = F[hx][hy + 1][hz], fym = F[hx][hy - 1][hz];
-      const float fzp = F[hx][hy][hz + 1], fzm = F[hx][hy][hz - 1];
-      const float Lx = (fxp + fxm - 2.0f * fc) / ex2;
-      const float Ly = (fyp + fym - 2.0f * fc) / ey2;
-      const float Lz = (fzp + fzm - 2.0f * fc) / ez2;
-      const float nx = (fxp - fxm) / dx, ny = (fyp - fym) / dy, nz = (fzp - fzm) / dz;
-      const float len = sqrtf(nx * nx + ny * ny + nz * nz);
-      if (nb == 0) {
-        acc += sc * (-2.0f * Lx / ex2 - 2.0f * Ly / ey2 - 2.0f * Lz / ez2);
-        const double l = sqrt((double)nx * nx + (double)ny * ny + (double)nz * nz + 1e-16);
-        le += (l - 1.0) * (l - 1.0);
-        lc += (double)Lx * Lx + (double)Ly * Ly + (double)Lz * Lz;
-        ln += 1.0;
-        continue;
+      for (int nb = 0; nb < 7; ++nb) {
+        const int ax = nb == 0 ? -1 : (nb - 1) >> 1;
+        const int sgn = nb == 0 ? 0 : (((nb - 1) & 1) ? 1 : -1);
+        const int mx = lx + 1 + (ax == 0 ? sgn : 0);
+        const int my = ly + 1 + (ax == 1 ? sgn : 0);
+        const int mz = lz + 1 + (ax == 2 ? sgn : 0);
+        if (!M[mx][my][mz]) continue;
+        touched = true;
+        const int hx = mx + 1, hy = my + 1, hz = mz + 1;
+        const float fc = F[hx][hy][hz];
+        const float fxp = F[hx + 1][hy][hz], fxm = F[hx - 1][hy][hz];
+        const float fyp = F[hx][hy + 1][hz], fym = F[hx][hy - 1][hz];
+        const float fzp = F[hx][hy][hz + 1], fzm = F[hx][hy][hz - 1];
+        const float Lx = (fxp + fxm - 2.0f * fc) / ex2;
+        const float Ly = (fyp + fym - 2.0f * fc) / ey2;
+        const float Lz = (fzp + fzm - 2.0f * fc) / ez2;
+        const float nx = (fxp - fxm) / dx, ny = (fyp - fym) / dy, nz = (fzp - fzm) / dz;
+        if (nb == 0) {
+          // curvature centre term (curvature_grad.cu: scale * (-2 Lx/ex^2 - 2 Ly/ey^2 - 2 Lz/ez^2))
+          acc += sc * (-2.0f * Lx / ex2 - 2.0f * Ly / ey2 - 2.0f * Lz / ez2);
+          const double l = sqrt((double)nx * nx + (double)ny * ny + (double)nz * nz + 1e-16);
+          le += (l - 1.0) * (l - 1.0);
+          lc += (double)Lx * Lx + (double)Ly * Ly + (double)Lz * Lz;
+          ln += 1.0;
+          continue;
+        }
+        const float len = sqrtf(nx * nx + ny * ny + nz * nz);
+        const float se = inv_nv * (1.0f - 1.0f / (len + 1e-8f)) * a.w_eik;
+        const float na = ax == 0 ? nx : (ax == 1 ? ny : nz);
+        const float da = ax == 0 ? dx : (ax == 1 ? dy : dz);
+        const float La = ax == 0 ? Lx : (ax == 1 ? Ly : Lz);
+        const float ea2 = ax == 0 ? ex2 : (ax == 1 ? ey2 : ez2);
+        // sgn < 0: voxel = v + e_ax receives +dL/dn_ax / (2 eps); sgn > 0: voxel = v - e_ax receives -
+        const float ve = (se * na) / da;
+        acc += (sgn < 0) ? ve : -ve;
+        acc += sc * (La / ea2);
       }
-      const float se = inv_nv * (1.0f - 1.0f / (len + 1e-8f)) * a.w_eik;
-      const float na = ax == 0 ? nx : (ax == 1 ? ny : nz);
-      const float da = ax == 0 ? dx : (ax == 1 ? dy : dz);
-      const float La = ax == 0 ? Lx : (ax == 1 ? Ly : Lz);
-      const float ea2 = ax == 0 ? ex2 : (ax == 1 ? ey2 : ez2);
-      // the voxel is v - sgn*e_ax: sgn = -1 -> voxel = v + e_ax (eikonal +), sgn = +1 -> voxel = v - e_ax (eikonal -)
-      const float ve = (se * na) / da;
-      acc += (sgn < 0) ? ve : -ve;
-      acc += sc * (La / ea2);
+      if (touched && acc != 0.0f) {
+        float* p = a.gg + lin3(a.g, x, y, z);
+        *p += acc;
+      }
     }
-    if (touched && acc != 0.0f) {
-      float* p = a.gg + lin3(a.g, x, y, z);
-      *p += acc;
-    }
+    __syncthreads();  // F and M are rewritten by the next tile
   }
-  reduce_losses(o, le, lc, ln);
+  le = warp_sum_d(le);
+  lc = warp_sum_d(lc);
+  ln = warp_sum_d(ln);
+  const int wl = tid & 31, ww = tid >> 5;
+  if (wl == 0) {
+    red[0][ww] = le;
+    red[1][ww] = lc;
+    red[2][ww] = ln;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    double s0 = 0, s1 = 0, s2 = 0;
+    for (int w = 0; w < 8; ++w) {
+      s0 += red[0][w];
+      s1 += red[1][w];
+      s2 += red[2][w];
+    }
+    partials[3 * blockIdx.x] = s0;
+    partials[3 * blockIdx.x + 1] = s1;
+    partials[3 * blockIdx.x + 2] = s2;
+  }
+}
+
+// Mean losses over interior vertices from the per-block partials, fixed reduction order.
+__global__ void __launch_bounds__(256) k_reg_finalize(const double* __restrict__ partials, int nblocks,
+                                                      float* __restrict__ losses) {
+  __shared__ double red[3][8];
+  double a = 0, b = 0, k = 0;
+  for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
+    a += partials[3 * i];
+    b += partials[3 * i + 1];
+    k += partials[3 * i + 2];
+  }
+  a = warp_sum_d(a);
+  b = warp_sum_d(b);
+  k = warp_sum_d(k);
+  if ((threadIdx.x & 31) == 0) {
+    red[0][threadIdx.x >> 5] = a;
+    red[1][threadIdx.x >> 5] = b;
+    red[2][threadIdx.x >> 5] = k;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    a = b = k = 0;
+    for (int w = 0; w < 8; ++w) {
+      a += red[0][w];
+      b += red[1][w];
+      k += red[2][w];
+    }
+    losses[0] = k > 0 ? (float)(a / k) : 0.0f;
+    losses[1] = k > 0 ? (float)(b / k) : 0.0f;
+  }
 }
 
 static int check_reg(const int32_t res[3]) {
@@ -337,8 +408,14 @@ int vx_curvature_grad(const float* grid, const int32_t res[3], const int64_t* ve
   return check_launch("curvature_grad");
 }
 
-int64_t vx_reg_stencil_blocks(const int32_t res[3]) {
+static int64_t stencil_tiles(const int32_t res[3]) {
   return (int64_t)((res[2] + TZ - 1) / TZ) * ((res[1] + TY - 1) / TY) * ((res[0] + TX - 1) / TX);
+}
+
+int64_t vx_reg_stencil_blocks(const int32_t res[3]) {
+  const int64_t t = stencil_tiles(res);
+  const int64_t cap = (int64_t)kSMs * 4;
+  return t < cap ? t : cap;
 }
 
 int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[3], const float xyz_min[3],
@@ -346,7 +423,7 @@ int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[
                    float w_eik, float w_curv, float* grad_grid, double* partials, int64_t n_partials,
                    unsigned int* counter, float* losses, void* stream) {
   if (int s = check_reg(res)) return s;
-  VX_REQUIRE(grid && bitmap && counts && grad_grid && partials && counter && xyz_min && xyz_max, "null pointer");
+  VX_REQUIRE(grid && bitmap && counts && grad_grid && partials && xyz_min && xyz_max, "null pointer");
   const int64_t nb = vx_reg_stencil_blocks(res);
   VX_REQUIRE(nb < (int64_t(1) << 31), "grid too large");
   VX_REQUIRE(n_partials >= 3 * nb, "partials buffer too small (%lld < %lld)", (long long)n_partials,
@@ -363,9 +440,11 @@ int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[
   a.gg = grad_grid;
   a.tiles_z = (res[2] + TZ - 1) / TZ;
   a.tiles_y = (res[1] + TY - 1) / TY;
-  RegOut o{partials, counter, losses};
-  k_reg_stencil<<<(unsigned)nb, dim3(32, 4, 2), 0, (cudaStream_t)stream>>>(a, o);
-  count_launches(1);
+  (void)counter;
+  const int64_t ntiles = stencil_tiles(res);
+  k_reg_stencil<<<(unsigned)nb, dim3(32, 4, 2), 0, (cudaStream_t)stream>>>(a, partials, (int)ntiles);
+  if (losses) k_reg_finalize<<<1, 256, 0, (cudaStream_t)stream>>>(partials, (int)nb, losses);
+  count_launches(losses ? 2 : 1);
   return check_launch("reg_stencil");
 }
 

@@ -278,7 +278,8 @@ class VoxNeuS(nn.Module):
 
     def render(self, rays_o, rays_d, sampler, near=None, far=None, background_rgb=None, cos_anneal_ratio=0.0,
                use_iter_cos_annealing=False, active_levels=None, up_sample_steps=4, sphere_radius=1.0,
-               *, randoms=None, vr_bitmap=None, extras=True, amplify_k=0.0, amp_flag=None) -> Dict[str, torch.Tensor]:
+               *, randoms=None, vr_bitmap=None, extras=True, amplify_k=0.0, amp_flag=None,
+               fused_mlp=True) -> Dict[str, torch.Tensor]:
         """Fused render (models/voxneus.py:169-260).
 
         near/far None: computed from the unit sphere inside the sampler kernel. randoms:
@@ -302,9 +303,15 @@ class VoxNeuS(nn.Module):
                                                  up_sample_steps, perturb, t_rand, u, occ.occupancy_mask,
                                                  *occ.bounds(), want_z=False)
         sdf, normal, gsamp = ops.RenderGeometryFn.apply(self.sdf_grid.grid, o, d, mid, lo, hi, vr_bitmap, extras)
-        x = ops.AppearanceInputFn.apply(self.radiance_hash.encoder.embeddings, normal, o, d, mid, lo, hi,
-                                        self.radiance_hash.encoder.cfg, active_levels)
-        colors = self.radiance_mlp.forward_rows(x).reshape(nr, mid.shape[1], 3)
+        if fused_mlp:
+            l0, l1 = self.radiance_mlp.net[0], self.radiance_mlp.net[2]
+            colors = ops.AppearanceMLPFn.apply(self.radiance_hash.encoder.embeddings, normal, l0.weight, l0.bias,
+                                               l1.weight, l1.bias, o, d, mid, lo, hi, self.radiance_hash.encoder.cfg,
+                                               active_levels)
+        else:
+            x = ops.AppearanceInputFn.apply(self.radiance_hash.encoder.embeddings, normal, o, d, mid, lo, hi,
+                                            self.radiance_hash.encoder.cfg, active_levels)
+            colors = self.radiance_mlp.forward_rows(x).reshape(nr, mid.shape[1], 3)
         out_t = ops.CompositeFn.apply(colors, sdf, normal, self.variance_net.variance, d, mid, dists, None, o, True,
                                       self.variance_net._s_max, sphere_radius if sphere_radius else 0.0,
                                       background_rgb, use_iter_cos_annealing, cos_anneal_ratio, amplify_k, amp_flag)

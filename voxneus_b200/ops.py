@@ -418,6 +418,99 @@ class AppearanceInputFn(torch.autograd.Function):
         return d_emb, d_n, None, None, None, None, None, None, None
 
 
+def mlp_forward(rows: torch.Tensor, W0, b0, W1, b1) -> torch.Tensor:
+    """Fused radiance MLP on input rows (P, >=51) with any row stride: colours (P, 3)."""
+    p = rows.shape[0]
+    if rows.stride(1) != 1:
+        raise RuntimeError("MLP rows must have unit column stride")
+    out = torch.empty(p, 3, device=rows.device)
+    call("vx_radiance_mlp_forward", ptr(rows), rows.stride(0), p, rows.shape[1], W0.shape[0], W1.shape[0],
+         ptr(W0.detach()), ptr(b0.detach()), ptr(W1.detach()), ptr(b1.detach()), ptr(out), stream_ptr(rows.device))
+    return out
+
+
+def mlp_backward(rows, W0, b0, W1, b1, d_colors):
+    dev = rows.device
+    p = rows.shape[0]
+    nb = int(L.query("vx_mlp_blocks", p))
+    nf = int(L.query("vx_mlp_partial_floats"))
+    sc = Scratch.get(dev)
+    if not hasattr(sc, "mlp_partials") or sc.mlp_partials.numel() < nb * nf:
+        sc.mlp_partials = torch.empty(nb * nf, device=dev)
+    d_hash = torch.empty(p, 32, device=dev)
+    d_normal = torch.empty(p, 3, device=dev)
+    dW0, db0, dW1, db1 = (torch.empty_like(t) for t in (W0, b0, W1, b1))
+    call("vx_radiance_mlp_backward", ptr(rows), rows.stride(0), p, rows.shape[1], W0.shape[0], W1.shape[0],
+         ptr(W0.detach()), ptr(b0.detach()), ptr(W1.detach()), ptr(b1.detach()),
+         ptr(check_tensor(d_colors.contiguous(), "d_colors")), ptr(d_hash), ptr(d_normal), ptr(dW0), ptr(db0),
+         ptr(dW1), ptr(db1), ptr(sc.mlp_partials), sc.mlp_partials.numel(), stream_ptr(dev))
+    return d_hash, d_normal, dW0, db0, dW1, db1
+
+
+class RadianceMLPFn(torch.autograd.Function):
+    """The 51-64-3 radiance MLP on pre-assembled rows, fused forward and adjoint."""
+
+    @staticmethod
+    def forward(ctx, rows, W0, b0, W1, b1):
+        ctx.save_for_backward(rows, W0, b0, W1, b1)
+        return mlp_forward(rows.detach(), W0, b0, W1, b1)
+
+    @staticmethod
+    def backward(ctx, g):
+        rows, W0, b0, W1, b1 = ctx.saved_tensors
+        d_hash, d_normal, dW0, db0, dW1, db1 = mlp_backward(rows.detach(), W0, b0, W1, b1, g)
+        d_rows = None
+        if ctx.needs_input_grad[0]:
+            d_rows = torch.zeros(rows.shape, device=rows.device)
+            d_rows[:, :32] = d_hash
+            d_rows[:, 48:51] = d_normal
+        return d_rows, dW0, db0, dW1, db1
+
+
+class AppearanceMLPFn(torch.autograd.Function):
+    """Hash encoding + SH + normal rows -> fused MLP -> colours for (rays, midpoints).
+
+    models/voxneus.py:147-157 without materialising the hidden layer: the rows buffer is kept
+    for the adjoint, which recomputes the hidden layer and scatters into the hash table.
+    """
+
+    @staticmethod
+    def forward(ctx, embeddings, normals, W0, b0, W1, b1, rays_o, rays_d, mid, xyz_min, xyz_max, cfg, active_levels):
+        nr, ns = mid.shape
+        p = nr * ns
+        width = 2 * cfg.n_levels + 16 + 3
+        if width != 51:
+            raise RuntimeError("the fused appearance path needs 16 hash levels x 2 features")
+        ld = MLP_LD
+        rows = torch.empty(p, ld, device=mid.device)
+        nrm = normals.detach().contiguous()
+        call("vx_appearance_forward", ptr(embeddings.detach()), cfg.n_levels, cfg.log2_size, cfg.n_features,
+             cfg._res_c, cfg.level_weights(active_levels), None, ptr(rays_o), ptr(rays_d), ptr(mid), ns, f3(xyz_min),
+             f3(xyz_max), p, ptr(rows), ld, 2 * cfg.n_levels, None, 0, 2 * cfg.n_levels + 16, ptr(nrm), width,
+             stream_ptr(mid.device))
+        colors = mlp_forward(rows, W0, b0, W1, b1)
+        ctx.save_for_backward(rays_o, rays_d, mid, W0, b0, W1, b1)
+        ctx.rows = rows
+        ctx.meta = (xyz_min, xyz_max, cfg, active_levels, embeddings.shape, normals.shape)
+        return colors.reshape(nr, ns, 3)
+
+    @staticmethod
+    def backward(ctx, g):
+        rays_o, rays_d, mid, W0, b0, W1, b1 = ctx.saved_tensors
+        xyz_min, xyz_max, cfg, active_levels, eshape, nshape = ctx.meta
+        nr, ns = mid.shape
+        rows = ctx.rows
+        ctx.rows = None
+        d_hash, d_normal, dW0, db0, dW1, db1 = mlp_backward(rows, W0, b0, W1, b1, g.reshape(-1, 3))
+        d_emb = None
+        if ctx.needs_input_grad[0]:
+            d_emb = torch.zeros(eshape, device=g.device)
+            call("vx_hash_encode_backward", ptr(d_emb), cfg.n_levels, cfg.log2_size, cfg.n_features, cfg._res_c,
+                 cfg.level_weights(active_levels), None, ptr(rays_o), ptr(rays_d), ptr(mid), ns, f3(xyz_min),
+                 f3(xyz_max), nr * ns, ptr(d_hash), 32, stream_ptr(g.device))
+        return (d_emb, d_normal.reshape(nshape), dW0, db0, dW1, db1, None, None, None, None, None, None, None)
+
+
 class HashEncodeFn(torch.autograd.Function):
     """Hash encoding of normalised points (RadianceHashGrid.forward, radiance_hash.py:211-231)."""
 
