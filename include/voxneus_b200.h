@@ -269,6 +269,21 @@ int vx_vr_compact(const uint32_t* bitmap, const float* grid, const int32_t res[3
                   int* block_scratch, int64_t n_block_scratch, int64_t* verts_out, int64_t* linear_out,
                   int64_t capacity, void* stream);
 
+/* vx_vr_compact without caller scratch. No counterpart in the reference. For callers that
+ * cannot allocate device memory when they call in: embedders whose device memory belongs to
+ * another runtime's pool (no allocation hook reaches this library) and plugin hosts that forbid
+ * device allocation after start-up. Identical arguments and output to vx_vr_compact minus the
+ * block scratch, which lives in a 16 KiB file-scope device array held by every GPU that loads the
+ * library until exit. Limit: grids of at most 2^27 voxels (4096 compaction blocks, e.g. 512^3);
+ * larger grids are rejected with VX_ERR_INVALID before any launch. Allocates nothing (no
+ * cudaMalloc, cudaFree or allocating library call). The first call on each device looks up the
+ * array's device address with that device current; make that first call before any stream
+ * capture. All calls share the one array: calls that overlap on the GPU (other streams, other
+ * host threads) race and must be serialised by the caller. */
+int vx_vr_compact_noalloc(const uint32_t* bitmap, const float* grid, const int32_t res[3], const float xyz_min[3],
+                          const float xyz_max[3], float relax_radius, float band, const unsigned long long* counts,
+                          int64_t* verts_out, int64_t* linear_out, int64_t capacity, void* stream);
+
 /* Blocks of the fused regularizer; partials hold 3 doubles per block. */
 int64_t vx_reg_stencil_blocks(const int32_t res[3]);
 

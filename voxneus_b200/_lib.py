@@ -62,6 +62,7 @@ _PROTOS = {
     "vx_vr_mark_corners": [P, I64, HI3, P, P],
     "vx_vr_count": [P, P, HI3, HF3, HF3, F32, F32, P, P],
     "vx_vr_compact": [P, P, HI3, HF3, HF3, F32, F32, P, P, I64, P, P, I64, P],
+    "vx_vr_compact_noalloc": [P, P, HI3, HF3, HF3, F32, F32, P, P, P, I64, P],
     "vx_reg_stencil_blocks": [HI3],
     "vx_reg_stencil": [P, P, HI3, HF3, HF3, F32, F32, P, F32, F32, P, P, I64, P, P, P],
     "vx_grid_upsample": [P, HI3, P, HI3, P],

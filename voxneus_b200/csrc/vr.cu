@@ -10,6 +10,8 @@
 // counts[0] = |bits|, counts[1] = |bits & relax|, counts[2] = |bits & band|,
 // counts[3] = |bits & relax & band|. The relax filter applies only when counts[1] > 0
 // (the reference keeps all vertices when none passes).
+#include <mutex>
+
 #include "common.cuh"
 
 namespace vx {
@@ -230,11 +232,60 @@ static int make_vr(VrArgs& a, const uint32_t* bitmap, const float* grid, const i
   return VX_OK;
 }
 
+// Scratch of the allocation-free compaction entry point: per-block offsets in a file-scope
+// device array. 4096 entries (16 KiB) cover grids of up to 4096 * 32768 = 2^27 voxels
+// (512^3). Every GPU that loads the library holds this array until the process exits.
+constexpr int64_t kNoAllocMaxBlocks = 4096;
+static __device__ __align__(256) int g_vr_block_offsets[kNoAllocMaxBlocks];
+
+// Device address of g_vr_block_offsets, looked up once per device with that device
+// current (a host-side reference to the symbol is not a device address).
+static int noalloc_offsets(int** out) {
+  static std::mutex mu;
+  static int* addr[64] = {nullptr};
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "cudaGetDevice: %s", cudaGetErrorString(e));
+  if (dev < 0 || dev >= 64) return set_error(VX_ERR_INVALID, "device index %d out of range", dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_vr_block_offsets);
+    if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "cudaGetSymbolAddress: %s", cudaGetErrorString(e));
+    addr[dev] = static_cast<int*>(p);
+  }
+  *out = addr[dev];
+  return VX_OK;
+}
+
 }  // namespace vx
 
 using namespace vx;
 
 extern "C" {
+
+int vx_vr_compact_noalloc(const uint32_t* bitmap, const float* grid, const int32_t res[3], const float xyz_min[3],
+                          const float xyz_max[3], float relax_radius, float band, const unsigned long long* counts,
+                          int64_t* verts_out, int64_t* linear_out, int64_t capacity, void* stream) {
+  VrArgs a;
+  if (int s = make_vr(a, bitmap, grid, res, xyz_min, xyz_max, relax_radius, band)) return s;
+  VX_REQUIRE(counts, "counts is null");
+  const int64_t nb = (a.nwords + kWordsPerBlock - 1) / kWordsPerBlock;
+  VX_REQUIRE(nb <= kNoAllocMaxBlocks,
+             "grid of %lld voxels needs %lld compaction blocks; the allocation-free entry point holds %lld "
+             "(grids up to 2^27 voxels); use vx_vr_compact with caller scratch",
+             (long long)a.nvox, (long long)nb, (long long)kNoAllocMaxBlocks);
+  int* offsets = nullptr;
+  if (int s = noalloc_offsets(&offsets)) return s;
+  // every offset the write pass reads is produced by the count pass of this call: nothing in
+  // the array has to start at zero
+  cudaStream_t st = (cudaStream_t)stream;
+  k_vr_block_counts<<<(unsigned)nb, kCompactThreads, 0, st>>>(a, counts, offsets);
+  k_vr_scan<<<1, 1024, 0, st>>>(offsets, (int)nb);
+  k_vr_write<<<(unsigned)nb, kCompactThreads, 0, st>>>(a, counts, offsets, verts_out, linear_out, capacity);
+  count_launches(3);
+  return check_launch("vr_compact_noalloc");
+}
 
 int64_t vx_vr_bitmap_words(const int32_t res[3]) {
   return ((int64_t)res[0] * res[1] * res[2] + 31) / 32;
