@@ -44,6 +44,9 @@ def parse():
     ap.add_argument("--rays", type=int, default=8192)
     ap.add_argument("--res", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="train", choices=["train", "field", "serving"],
+                    help="train (the metric line), field (512^3 queries), serving (the request mix)")
+    ap.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
     return ap.parse_args()
 
 
@@ -340,10 +343,146 @@ def run_fused(args):
         dist.destroy_process_group()
 
 
+def _events():
+    return torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+
+def run_field(args):
+    """Large-grid field query: 512^3 grid of 32 Gaussian-bump spheres; SDF + Eq.7 normal on a 320^3
+    lattice and on 2^24 uniform points; the full-grid eikonal + curvature stencil (every voxel in
+    V_R, deterministic gather form)."""
+    from voxneus_b200 import _lib, ops, synthetic
+
+    _lib.load()
+    dev = torch.device("cuda")
+    res = 512
+    grid = synthetic.bumpy_spheres_grid(res, 32, seed=3, device=dev).contiguous()
+    lo, hi = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
+    peak, peak_kind = peak_hbm()
+    out = {"metric": "field query points/s (512^3 grid)", "unit": "points/s", "data": "synthetic",
+           "config": {"workload": "512^3 grid, 32 Gaussian-bump spheres; 320^3 lattice, 2^24 random points, "
+                                  "full-grid eikonal+curvature stencil", "grid": res}, "peak_hbm_gbs": peak,
+           "peak_kind": peak_kind}
+    reps = max(args.steps, 3)
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        s, e = _events()
+        torch.cuda.synchronize()
+        s.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e) / reps
+
+    n_lat = 320 ** 3
+    ms = timed(lambda: ops.field_query_lattice(grid, lo, hi, [320] * 3, lo, hi))
+    out["lattice_320"] = {"points_per_s": n_lat / (ms / 1e3), "ms": ms, "bytes_per_point": 144,
+                          "achieved_gbs": n_lat * 144 / (ms / 1e3) / 1e9}
+    g = torch.Generator(device=dev).manual_seed(5)
+    pts = (torch.rand(1 << 24, 3, device=dev, generator=g) * 2 - 1).contiguous()
+    ms = timed(lambda: ops.field_query(grid, lo, hi, pts, sdf=True, normal=True))
+    out["random_2^24"] = {"points_per_s": (1 << 24) / (ms / 1e3), "ms": ms, "bytes_per_point": 156,
+                          "achieved_gbs": (1 << 24) * 156 / (ms / 1e3) / 1e9}
+    bm = torch.full((ops.bitmap_words([res] * 3),), -1, dtype=torch.int32, device=dev)
+    counts = ops.vr_count(bm, grid, [res] * 3, lo, hi, 0.0, 0.0)
+    gg = torch.zeros_like(grid)
+    ms = timed(lambda: ops.reg_stencil(grid, bm, [res] * 3, lo, hi, 0.0, 0.0, counts, 0.1, 5e-4, gg))
+    vox = res ** 3
+    out["stencil_full_grid"] = {"voxels_per_s": vox / (ms / 1e3), "ms": ms, "bytes_per_voxel": 12,
+                                "achieved_gbs": vox * 12 / (ms / 1e3) / 1e9, "deterministic": True}
+    out["value"] = out["random_2^24"]["points_per_s"]
+    print(json.dumps(out), flush=True)
+
+
+def run_serving(args):
+    """Serving mix: 16 resident 256^3 scenes (own hash table and MLP each), Poisson arrivals at
+    200 req/s, 50/50 renders (log-uniform 4,096-480,000 rays from random views of the 64 cameras,
+    128 samples, deterministic sampler) and SDF/normal queries (log-uniform 2^16-2^22 points)."""
+    import math
+    import random
+
+    from voxneus_b200 import _lib, synthetic
+    from voxneus_b200.models import VoxNeuS
+    from voxneus_b200.serving import Request, SceneStore, ServingEngine, latency_stats
+
+    _lib.load()
+    dev = torch.device("cuda")
+    store = SceneStore(dev)
+    n_scenes = 16
+    for i in range(n_scenes):
+        torch.manual_seed(i)
+        m = VoxNeuS(grid_res=args.res // 2, occupancy_res=128).to(dev)
+        with torch.no_grad():
+            m.sdf_grid.grid.copy_(synthetic.shapes_grid(args.res // 2, seed=i).to(dev))
+            m.radiance_hash.encoder.embeddings.uniform_(-1e-2, 1e-2)
+        m.sdf_grid.scale_volume_grid(args.res)
+        store.add(f"scene{i}", m)
+    t0 = time.perf_counter()
+    eng = ServingEngine(store)
+    capture_s = time.perf_counter() - t0
+    rng = random.Random(11)
+    pool = synthetic.RayPool(seed=12)
+    views = [pool.view(c) for c in range(0, 64, 4)]  # 16 full 800x600 views (480,000 rays each)
+    views = [(o.pin_memory(), d.pin_memory()) for o, d in views]
+    qpool = [(torch.rand(1 << 22, 3, generator=torch.Generator().manual_seed(k)) * 2 - 1).pin_memory()
+             for k in range(4)]
+    duration = float(args.duration)
+    rate = 200.0
+    t = 0.0
+    plan = []
+    while True:
+        t += rng.expovariate(rate)
+        if t >= duration:
+            break
+        scene = f"scene{rng.randrange(n_scenes)}"
+        if rng.random() < 0.5:
+            n = int(round(math.exp(rng.uniform(math.log(4096), math.log(480000)))))
+            o, d = views[rng.randrange(len(views))]
+            s = rng.randrange(0, 480000 - n + 1)
+            plan.append((t, Request(scene, "render", (o[s:s + n], d[s:s + n]))))
+        else:
+            n = int(round(math.exp(rng.uniform(math.log(1 << 16), math.log(1 << 22)))))
+            q = qpool[rng.randrange(len(qpool))]
+            s = rng.randrange(0, (1 << 22) - n + 1)
+            plan.append((t, Request(scene, "query", (q[s:s + n],))))
+    with ClockSampler(0) as clk:
+        start = time.perf_counter()
+        for when, req in plan:
+            now = time.perf_counter() - start
+            if when > now:
+                time.sleep(when - now)
+            req.arrival = start + when
+            eng.submit(req)
+        for _, req in plan:
+            req.wait(600)
+        wall = time.perf_counter() - start
+    eng.close()
+    reqs = [r for _, r in plan]
+    rend = [r for r in reqs if r.kind == "render"]
+    qry = [r for r in reqs if r.kind == "query"]
+    line = {"metric": "serving render rays/s and p50/p99 latency (16 resident 256^3 scenes, Poisson 200 req/s)",
+            "value": sum(r.n for r in rend) / wall, "unit": "rays/s", "data": "synthetic",
+            "config": {"workload": "16 scenes 256^3 + 2^19 hash tables; 50/50 render (4K-480K rays, 128 samples) / "
+                                   "query (2^16-2^22 points); Poisson 200 req/s",
+                       "duration_s": duration, "requests": len(reqs), "buckets_render": eng.RENDER_BUCKETS,
+                       "buckets_query": eng.QUERY_BUCKETS, "graph_capture_s": capture_s},
+            "query_points_per_s": sum(r.n for r in qry) / wall, "wall_s": wall,
+            "latency_all": latency_stats(reqs), "latency_render": latency_stats(rend),
+            "latency_query": latency_stats(qry), "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse()
     if args.impl == "reference":
         run_reference(args)
+    elif args.workload == "field":
+        run_field(args)
+    elif args.workload == "serving":
+        run_serving(args)
     else:
         run_fused(args)
 

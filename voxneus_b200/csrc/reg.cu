@@ -188,33 +188,47 @@ __device__ __forceinline__ bool vr_member(const StencilArgs& a, int x, int y, in
   return true;
 }
 
-// Does the halo-1 box of a tile hold any V_R bit? Word-level test, one thread per (x, y) row of
-// the box (z range [z0-1, z0+TZ] covers at most 3 words).
-__device__ __forceinline__ bool tile_has_bits(const StencilArgs& a, int x0, int y0, int z0, int tid) {
-  bool hit = false;
-  if (tid < MX * MY) {
-    const int x = x0 - 1 + tid / MY, y = y0 - 1 + tid % MY;
-    if (x >= 0 && x < a.g.rx && y >= 0 && y < a.g.ry) {
-      const int zlo = max(z0 - 1, 0), zhi = min(z0 + TZ, a.g.rz - 1);
-      const int b0 = lin3(a.g, x, y, zlo), b1 = lin3(a.g, x, y, zhi);
-      for (int w = b0 >> 5; w <= (b1 >> 5); ++w) {
-        uint32_t m = 0xffffffffu;
-        if (w == (b0 >> 5)) m &= 0xffffffffu << (b0 & 31);
-        if (w == (b1 >> 5)) m &= 0xffffffffu >> (31 - (b1 & 31));
-        hit |= (__ldg(a.bm + w) & m) != 0u;
-      }
-    }
-  }
-  return hit;
+__device__ __forceinline__ void tile_origin(const StencilArgs& a, int t, int& x0, int& y0, int& z0) {
+  const int tz = t % a.tiles_z;
+  const int ty = (t / a.tiles_z) % a.tiles_y;
+  const int tx = t / (a.tiles_z * a.tiles_y);
+  z0 = tz * TZ;
+  y0 = ty * TY;
+  x0 = tx * TX;
 }
 
-// Persistent grid over 32x4x4 tiles; blockDim = (32, 4, 2), each thread owns output voxels
-// (z, y, x) and (z, y, x + 2) of the current tile. Tiles whose halo box holds no V_R bit are
-// skipped after one word-level test. Per-block loss partials; k_reg_finalize reduces them.
+// Does the halo-1 box of tile t hold any V_R bit? Word-level test by one warp, one lane per
+// (x, y) row of the box (the z range [z0-1, z0+TZ] covers at most 3 words).
+__device__ __forceinline__ bool tile_has_bits_warp(const StencilArgs& a, int t, int lane) {
+  int x0, y0, z0;
+  tile_origin(a, t, x0, y0, z0);
+  bool hit = false;
+  for (int r = lane; r < MX * MY; r += 32) {
+    const int x = x0 - 1 + r / MY, y = y0 - 1 + r % MY;
+    if (x < 0 || x >= a.g.rx || y < 0 || y >= a.g.ry) continue;
+    const int zlo = max(z0 - 1, 0), zhi = min(z0 + TZ, a.g.rz - 1);
+    const int b0 = lin3(a.g, x, y, zlo), b1 = lin3(a.g, x, y, zhi);
+    for (int w = b0 >> 5; w <= (b1 >> 5); ++w) {
+      uint32_t m = 0xffffffffu;
+      if (w == (b0 >> 5)) m &= 0xffffffffu << (b0 & 31);
+      if (w == (b1 >> 5)) m &= 0xffffffffu >> (31 - (b1 & 31));
+      hit |= (__ldg(a.bm + w) & m) != 0u;
+    }
+  }
+  return __any_sync(0xffffffffu, hit);
+}
+
+// Persistent grid over 32x4x4 tiles taken 8 at a time; blockDim = (32, 4, 2). Each warp tests one
+// tile of the batch with word-level bitmap reads, so an empty tile costs one load per lane and
+// an eighth of a barrier. For an active tile the SDF box (halo 2) is staged first, the active
+// interior mask (halo 1) is built from the bitmap with the narrow-band test read from that box,
+// and each thread owns output voxels (z, y, x) and (z, y, x + 2). Per-block loss partials;
+// k_reg_finalize reduces them.
 __global__ void __launch_bounds__(256) k_reg_stencil(StencilArgs a, double* __restrict__ partials, int ntiles) {
   __shared__ float F[HX][HY][HZ];
   __shared__ uint8_t M[MX][MY][MZ];
   __shared__ double red[3][8];
+  __shared__ int active[8];
   const int tid = threadIdx.x + 32 * (threadIdx.y + 4 * threadIdx.z);
   const bool relax_on = a.relax_r > 0.0f && a.counts[1] > 0;
   const unsigned long long nv = a.counts[a.band > 0.0f ? (relax_on ? 3 : 2) : (relax_on ? 1 : 0)];
@@ -223,27 +237,43 @@ __global__ void __launch_bounds__(256) k_reg_stencil(StencilArgs a, double* __re
   const float ex2 = a.g.eps[0] * a.g.eps[0], ey2 = a.g.eps[1] * a.g.eps[1], ez2 = a.g.eps[2] * a.g.eps[2];
   const float sc = inv_nv * a.w_curv;
   double le = 0, lc = 0, ln = 0;
-  for (int t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int tz = t % a.tiles_z;
-    const int ty = (t / a.tiles_z) % a.tiles_y;
-    const int tx = t / (a.tiles_z * a.tiles_y);
-    const int z0 = tz * TZ, y0 = ty * TY, x0 = tx * TX;
-    if (!__syncthreads_or(tile_has_bits(a, x0, y0, z0, tid))) continue;
-    // active interior mask of the halo-1 box
-    for (int q = tid; q < MX * MY * MZ; q += 256) {
-      const int mz = q % MZ, my = (q / MZ) % MY, mx = q / (MZ * MY);
-      const int x = x0 - 1 + mx, y = y0 - 1 + my, z = z0 - 1 + mz;
-      uint8_t m = 0;
-      if (x >= 1 && x <= a.g.rx - 2 && y >= 1 && y <= a.g.ry - 2 && z >= 1 && z <= a.g.rz - 2)
-        m = vr_member(a, x, y, z, relax_on) ? 1 : 0;
-      M[mx][my][mz] = m;
+  for (int tb = blockIdx.x * 8; tb < ntiles; tb += gridDim.x * 8) {
+    {
+      const int w = tid >> 5;
+      const bool hit = (tb + w < ntiles) ? tile_has_bits_warp(a, tb + w, tid & 31) : false;
+      if ((tid & 31) == 0) active[w] = hit;
     }
+    __syncthreads();
+    for (int wt = 0; wt < 8; ++wt) {
+    if (!active[wt]) continue;
+    int x0, y0, z0;
+    tile_origin(a, tb + wt, x0, y0, z0);
     for (int q = tid; q < HX * HY * HZ; q += 256) {
       const int hz = q % HZ, hy = (q / HZ) % HY, hx = q / (HZ * HY);
       const int x = x0 - 2 + hx, y = y0 - 2 + hy, z = z0 - 2 + hz;
       float v = 0.0f;
       if (x >= 0 && x < a.g.rx && y >= 0 && y < a.g.ry && z >= 0 && z < a.g.rz) v = __ldg(a.f + lin3(a.g, x, y, z));
       F[hx][hy][hz] = v;
+    }
+    __syncthreads();
+    // active interior mask of the halo-1 box (band test on the staged SDF)
+    for (int q = tid; q < MX * MY * MZ; q += 256) {
+      const int mz = q % MZ, my = (q / MZ) % MY, mx = q / (MZ * MY);
+      const int x = x0 - 1 + mx, y = y0 - 1 + my, z = z0 - 1 + mz;
+      uint8_t m = 0;
+      if (x >= 1 && x <= a.g.rx - 2 && y >= 1 && y <= a.g.ry - 2 && z >= 1 && z <= a.g.rz - 2) {
+        const int idx = lin3(a.g, x, y, z);
+        bool on = (__ldg(a.bm + (idx >> 5)) >> (idx & 31)) & 1u;
+        if (on && relax_on) {
+          const float wx = __fadd_rn(a.g.lo[0], __fmul_rn((float)x, a.g.eps[0]));
+          const float wy = __fadd_rn(a.g.lo[1], __fmul_rn((float)y, a.g.eps[1]));
+          const float wz = __fadd_rn(a.g.lo[2], __fmul_rn((float)z, a.g.eps[2]));
+          on = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(wx, wx), __fmul_rn(wy, wy)), __fmul_rn(wz, wz))) < a.relax_r;
+        }
+        if (on && a.band > 0.0f) on = fabsf(F[mx + 1][my + 1][mz + 1]) < a.band;
+        m = on ? 1 : 0;
+      }
+      M[mx][my][mz] = m;
     }
     __syncthreads();
     const int lz = threadIdx.x, ly = threadIdx.y;
@@ -300,6 +330,8 @@ __global__ void __launch_bounds__(256) k_reg_stencil(StencilArgs a, double* __re
       }
     }
     __syncthreads();  // F and M are rewritten by the next tile
+    }
+    __syncthreads();  // active[] is rewritten by the next batch
   }
   le = warp_sum_d(le);
   lc = warp_sum_d(lc);
@@ -413,7 +445,7 @@ static int64_t stencil_tiles(const int32_t res[3]) {
 }
 
 int64_t vx_reg_stencil_blocks(const int32_t res[3]) {
-  const int64_t t = stencil_tiles(res);
+  const int64_t t = (stencil_tiles(res) + 7) / 8;  // tiles are taken 8 per block iteration
   const int64_t cap = (int64_t)kSMs * 4;
   return t < cap ? t : cap;
 }

@@ -488,6 +488,7 @@ class AppearanceMLPFn(torch.autograd.Function):
              cfg._res_c, cfg.level_weights(active_levels), None, ptr(rays_o), ptr(rays_d), ptr(mid), ns, f3(xyz_min),
              f3(xyz_max), p, ptr(rows), ld, 2 * cfg.n_levels, None, 0, 2 * cfg.n_levels + 16, ptr(nrm), width,
              stream_ptr(mid.device))
+        rows = rows[:, :width]
         colors = mlp_forward(rows, W0, b0, W1, b1)
         ctx.save_for_backward(rays_o, rays_d, mid, W0, b0, W1, b1)
         ctx.rows = rows

@@ -1,0 +1,339 @@
+"""Render and SDF/normal-query serving over resident scenes with continuous batching.
+
+Semantics follow the reference's inference paths: a render request is `render_full_image`
+(scripts/render.py:35-54: RaySampler(64, 64, perturb=False), near/far from the unit sphere,
+outputs rgb and depth); a query request is the batched `query_normals` of
+`compute_mesh_normals` (geometry/mesh.py:80-114) plus `query_sdf`.
+
+Design:
+* SceneStore keeps every scene's parameters resident on the device (grid, hash table, MLP,
+  variance, occupancy mask).
+* Work is cut into chunks of a few fixed size buckets; each (scene, kind, bucket) has a CUDA
+  graph captured once (all graphs share one memory pool: they replay on one stream, one at a
+  time), so a chunk costs one graph launch whatever kernels it contains.
+* The engine thread admits pending requests while the reserved device memory stays under the
+  budget (a fraction of the free HBM measured at start), then each iteration takes one chunk
+  from every active request in turn (round robin), so requests that arrive while others are
+  running start at the next iteration and their chunks interleave with the older ones on the
+  device; input copies run on a separate copy stream ahead of the compute stream.
+* A result is the same alone and in any mix: every ray and point is computed independently,
+  with the same kernels and launch shapes, whatever chunk it falls in.
+* Failures stay on the host: malformed requests are rejected at submission, a request larger
+  than the budget is rejected, and an exception inside the engine fails the affected requests
+  and stops the engine cleanly.
+"""
+
+from __future__ import annotations
+
+import math
+import queue
+import threading
+import time
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+import torch
+
+from . import ops
+from .models import VoxNeuS
+from .rendering import RaySampler
+
+
+class RequestError(RuntimeError):
+    pass
+
+
+@dataclass
+class Request:
+    scene: str
+    kind: str  # "render" or "query"
+    inputs: Tuple[torch.Tensor, ...]  # render: (rays_o, rays_d) (n,3); query: (points,) (n,3); host or device
+    rid: int = -1
+    arrival: float = 0.0
+    admitted: float = 0.0
+    finished: float = 0.0
+    n: int = 0
+    outputs: Dict[str, torch.Tensor] = field(default_factory=dict)
+    error: Optional[str] = None
+    done: threading.Event = field(default_factory=threading.Event)
+    # engine state
+    _dev_in: Tuple[torch.Tensor, ...] = ()
+    _dev_out: Dict[str, torch.Tensor] = field(default_factory=dict)
+    _next: int = 0
+    _reserved: int = 0
+    _copy_evt: Optional[torch.cuda.Event] = None
+
+    @property
+    def latency(self) -> float:
+        return self.finished - self.arrival
+
+    def wait(self, timeout: Optional[float] = None) -> "Request":
+        if not self.done.wait(timeout):
+            raise TimeoutError(f"request {self.rid} not finished within {timeout}s")
+        if self.error:
+            raise RequestError(self.error)
+        return self
+
+
+class SceneStore:
+    """Resident scenes keyed by name."""
+
+    def __init__(self, device):
+        self.device = torch.device(device)
+        self.scenes: Dict[str, VoxNeuS] = {}
+
+    def add(self, name: str, model: VoxNeuS) -> None:
+        model = model.to(self.device).eval()
+        for p in model.parameters():
+            p.requires_grad_(False)
+        self.scenes[name] = model
+
+    def load_checkpoint(self, name: str, path: str, **model_kw) -> None:
+        """Load a reference checkpoint (training/checkpoint.py:11-33 layout) into the store."""
+        ck = torch.load(path, map_location="cpu", weights_only=False)
+        res = ck.get("grid_res", None)
+        m = VoxNeuS(grid_res=res if res is not None else 96, **model_kw)
+        m.load_state_dict(ck["model_state"])
+        self.add(name, m)
+
+    def bytes(self) -> int:
+        return sum(sum(t.numel() * t.element_size() for t in m.state_dict().values()) for m in self.scenes.values())
+
+
+class _GraphBucket:
+    """A captured render or query pipeline for one scene and one chunk size."""
+
+    def __init__(self, model: VoxNeuS, kind: str, size: int, sampler: RaySampler, pool, stream):
+        self.kind, self.size = kind, size
+        dev = model.sdf_grid.grid.device
+        if kind == "render":
+            self.inp = (torch.zeros(size, 3, device=dev), torch.zeros(size, 3, device=dev))
+            self.inp[0][:, 2] = 3.0
+            self.inp[1][:, 2] = -1.0
+        else:
+            self.inp = (torch.zeros(size, 3, device=dev),)
+        self.model, self.sampler = model, sampler
+        with torch.cuda.stream(stream), torch.no_grad():
+            self._run()  # warm caches (tables, scratch) outside capture
+            stream.synchronize()
+            self.graph = torch.cuda.CUDAGraph()
+            with torch.cuda.graph(self.graph, pool=pool, stream=stream):
+                self.out = self._run()
+
+    def _run(self):
+        m = self.model
+        if self.kind == "render":
+            out = m.render(self.inp[0], self.inp[1], self.sampler, None, None, extras=False)
+            return {"rgb": out["rgb"], "depth": out["depth"]}
+        lo, hi = m.sdf_grid.bounds()
+        sdf, _, nrm, _, _ = ops.field_query(m.sdf_grid.grid, lo, hi, self.inp[0], sdf=True, normal=True)
+        return {"sdf": sdf.unsqueeze(-1), "normal": nrm}
+
+
+class ServingEngine:
+    RENDER_BUCKETS = (4096, 16384, 65536)
+    QUERY_BUCKETS = (65536, 262144, 1048576)
+
+    def __init__(self, store: SceneStore, memory_fraction: float = 0.5, n_samples: int = 64,
+                 n_importance: int = 64, budget_bytes: Optional[int] = None, fault_injector=None,
+                 render_buckets: Optional[Tuple[int, ...]] = None, query_buckets: Optional[Tuple[int, ...]] = None):
+        if render_buckets:
+            self.RENDER_BUCKETS = tuple(sorted(render_buckets))
+        if query_buckets:
+            self.QUERY_BUCKETS = tuple(sorted(query_buckets))
+        self.store = store
+        self.device = store.device
+        self.sampler = RaySampler(n_samples, n_importance, perturb=False)
+        self.compute = torch.cuda.Stream(self.device)
+        self.copy = torch.cuda.Stream(self.device)
+        self.pool = torch.cuda.graph_pool_handle()
+        self.graphs: Dict[Tuple[str, str, int], _GraphBucket] = {}
+        for name, m in store.scenes.items():
+            for size in self.RENDER_BUCKETS:
+                self.graphs[(name, "render", size)] = _GraphBucket(m, "render", size, self.sampler, self.pool,
+                                                                   self.compute)
+            for size in self.QUERY_BUCKETS:
+                self.graphs[(name, "query", size)] = _GraphBucket(m, "query", size, self.sampler, self.pool,
+                                                                  self.compute)
+        torch.cuda.synchronize(self.device)
+        if budget_bytes is None:
+            free, _ = torch.cuda.mem_get_info(self.device)
+            budget_bytes = int(free * memory_fraction)
+        self.budget = budget_bytes
+        self.reserved = 0
+        self.pending: "queue.Queue[Request]" = queue.Queue()
+        self.waiting: List[Request] = []
+        self.active: List[Request] = []
+        self._inflight: List[Tuple[torch.cuda.Event, Request]] = []
+        self._rid = 0
+        self._stop = threading.Event()
+        self._failed: Optional[str] = None
+        self._fault = fault_injector
+        self._thread = threading.Thread(target=self._loop, name="voxneus-serving", daemon=True)
+        self._thread.start()
+
+    # ---------------------------------------------------------------- submission
+
+    @staticmethod
+    def _bytes_for(kind: str, n: int) -> int:
+        return n * 4 * (6 + 4) if kind == "render" else n * 4 * (3 + 4)
+
+    def submit(self, req: Request) -> Request:
+        if self._failed:
+            raise RequestError(f"engine stopped: {self._failed}")
+        if req.scene not in self.store.scenes:
+            raise RequestError(f"unknown scene {req.scene!r}")
+        if req.kind not in ("render", "query"):
+            raise RequestError(f"unknown request kind {req.kind!r}")
+        want = 2 if req.kind == "render" else 1
+        if len(req.inputs) != want:
+            raise RequestError(f"{req.kind} needs {want} input tensor(s)")
+        n = req.inputs[0].shape[0]
+        for t in req.inputs:
+            if t.dim() != 2 or t.shape[1] != 3 or t.shape[0] != n or t.dtype != torch.float32:
+                raise RequestError("inputs must be float32 (n, 3) tensors of equal length")
+            if not bool(torch.isfinite(t).all()):
+                raise RequestError("inputs contain NaN or Inf")
+        if n == 0:
+            raise RequestError("empty request")
+        if self._bytes_for(req.kind, n) > self.budget:
+            raise RequestError(f"request needs {self._bytes_for(req.kind, n)} bytes, budget is {self.budget}")
+        req.n = n
+        req.rid = self._rid
+        self._rid += 1
+        req.arrival = req.arrival or time.perf_counter()
+        self.pending.put(req)
+        return req
+
+    # ---------------------------------------------------------------- engine loop
+
+    def _admit(self):
+        while True:
+            try:
+                self.waiting.append(self.pending.get_nowait())
+            except queue.Empty:
+                break
+        still = []
+        for req in self.waiting:
+            need = self._bytes_for(req.kind, req.n)
+            if self.reserved + need > self.budget:
+                still.append(req)
+                continue
+            self.reserved += need
+            req._reserved = need
+            req.admitted = time.perf_counter()
+            with torch.cuda.stream(self.copy):
+                req._dev_in = tuple(t.to(self.device, non_blocking=True) for t in req.inputs)
+                if req.kind == "render":
+                    req._dev_out = {"rgb": torch.empty(req.n, 3, device=self.device),
+                                    "depth": torch.empty(req.n, 1, device=self.device)}
+                else:
+                    req._dev_out = {"sdf": torch.empty(req.n, 1, device=self.device),
+                                    "normal": torch.empty(req.n, 3, device=self.device)}
+                req._copy_evt = torch.cuda.Event()
+                req._copy_evt.record(self.copy)
+            self.active.append(req)
+        self.waiting = still
+
+    def _bucket(self, kind: str, remaining: int) -> int:
+        buckets = self.RENDER_BUCKETS if kind == "render" else self.QUERY_BUCKETS
+        for b in buckets:
+            if remaining <= b:
+                return b
+        return buckets[-1]
+
+    def _run_chunk(self, req: Request):
+        start = req._next
+        size = self._bucket(req.kind, req.n - start)
+        cnt = min(size, req.n - start)
+        gb = self.graphs[(req.scene, req.kind, size)]
+        s = self.compute
+        s.wait_event(req._copy_evt)
+        with torch.cuda.stream(s):
+            for dst, src in zip(gb.inp, req._dev_in):
+                dst[:cnt].copy_(src[start:start + cnt])
+                if cnt < size:
+                    dst[cnt:].copy_(src[start + cnt - 1:start + cnt].expand(size - cnt, 3))
+            gb.graph.replay()
+            for k, v in gb.out.items():
+                req._dev_out[k][start:start + cnt].copy_(v[:cnt])
+        req._next = start + cnt
+
+    def _finish(self, req: Request):
+        host = req.inputs[0].device.type == "cpu"
+        with torch.cuda.stream(self.compute):
+            if host:
+                req.outputs = {}
+                for k, v in req._dev_out.items():
+                    h = torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
+                    h.copy_(v, non_blocking=True)
+                    req.outputs[k] = h
+            else:
+                req.outputs = dict(req._dev_out)
+            evt = torch.cuda.Event()
+            evt.record(self.compute)
+        self._inflight.append((evt, req))
+
+    def _poll(self):
+        keep = []
+        for evt, req in self._inflight:
+            if evt.query():
+                req.finished = time.perf_counter()
+                self.reserved -= req._reserved
+                req._dev_in, req._dev_out = (), {}
+                req.done.set()
+            else:
+                keep.append((evt, req))
+        self._inflight = keep
+
+    def _loop(self):
+        torch.cuda.set_device(self.device)
+        try:
+            while not self._stop.is_set():
+                self._admit()
+                self._poll()
+                if not self.active:
+                    if not self._inflight:
+                        time.sleep(0.0002)
+                    continue
+                for req in list(self.active):
+                    if self._fault is not None:
+                        self._fault(req)
+                    self._run_chunk(req)
+                    if req._next >= req.n:
+                        self.active.remove(req)
+                        self._finish(req)
+        except Exception as e:  # host-side failure: fail every request and stop
+            self._failed = f"{type(e).__name__}: {e}"
+            for req in self.active + self.waiting + [r for _, r in self._inflight]:
+                req.error = self._failed
+                req.done.set()
+            while True:
+                try:
+                    r = self.pending.get_nowait()
+                    r.error = self._failed
+                    r.done.set()
+                except queue.Empty:
+                    break
+
+    def close(self):
+        self._stop.set()
+        self._thread.join(timeout=30)
+        torch.cuda.synchronize(self.device)
+
+    @property
+    def failed(self) -> Optional[str]:
+        return self._failed
+
+
+def latency_stats(reqs: List[Request]) -> Dict[str, float]:
+    lat = sorted(r.latency * 1e3 for r in reqs if not r.error)
+    if not lat:
+        return {}
+
+    def pct(p):
+        return lat[min(len(lat) - 1, max(0, int(math.ceil(p / 100.0 * len(lat))) - 1))]
+
+    wait = [(r.admitted - r.arrival) * 1e3 for r in reqs if not r.error]
+    return {"p50_ms": pct(50), "p99_ms": pct(99), "mean_ms": sum(lat) / len(lat), "n": len(lat),
+            "admission_wait_share": sum(wait) / max(sum(lat), 1e-9)}

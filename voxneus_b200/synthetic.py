@@ -94,17 +94,20 @@ def shapes_grid(res: int, n_shapes: int = 8, noise: float = 0.005, seed: int = 0
     return (f + noise * torch.randn(f.shape, generator=g)).reshape(1, 1, res, res, res)
 
 
-def bumpy_spheres_grid(res: int, n_spheres: int = 32, seed: int = 0) -> torch.Tensor:
-    """min_k ||x - c_k|| - r_k (1 + a_k exp(-||x - p_k||^2 / s_k^2)), (1,1,R,R,R)."""
+def bumpy_spheres_grid(res: int, n_spheres: int = 32, seed: int = 0, device="cpu") -> torch.Tensor:
+    """min_k ||x - c_k|| - r_k (1 + a_k exp(-||x - p_k||^2 / s_k^2)), (1,1,R,R,R).
+
+    Shape parameters come from a CPU generator (seeded); the field is evaluated on `device`.
+    """
     g = torch.Generator().manual_seed(seed)
-    ax = torch.linspace(-1.0, 1.0, res)
-    f = torch.full((res, res, res), 1e9)
+    ax = torch.linspace(-1.0, 1.0, res, device=device)
+    f = torch.full((res, res, res), 1e9, device=device)
     for _ in range(n_spheres):
-        c = (torch.rand(3, generator=g) - 0.5) * 1.2
+        c = ((torch.rand(3, generator=g) - 0.5) * 1.2).tolist()
         r = 0.1 + 0.3 * float(torch.rand(1, generator=g))
         a = (float(torch.rand(1, generator=g)) - 0.5) * 0.2
         s = 0.05 + 0.15 * float(torch.rand(1, generator=g))
-        pk = c + r * torch.nn.functional.normalize(torch.randn(3, generator=g), dim=0)
+        pk = [c[i] + r * v for i, v in enumerate(torch.nn.functional.normalize(torch.randn(3, generator=g), dim=0).tolist())]
         for i0 in range(0, res, 64):  # slabs keep the temporaries small at 512^3
             x = ax[i0:i0 + 64].view(-1, 1, 1)
             y = ax.view(1, -1, 1)
