@@ -38,7 +38,7 @@ CPU_SAMPLE_RAYS = 1024
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="fused", choices=["fused", "reference"])
     ap.add_argument("--rays", type=int, default=8192)
@@ -89,7 +89,7 @@ class ClockSampler:
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "50"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -387,9 +387,10 @@ def run_field(args):
     out["random_2^24"] = {"points_per_s": (1 << 24) / (ms / 1e3), "ms": ms, "bytes_per_point": 156,
                           "achieved_gbs": (1 << 24) * 156 / (ms / 1e3) / 1e9}
     bm = torch.full((ops.bitmap_words([res] * 3),), -1, dtype=torch.int32, device=dev)
-    counts = ops.vr_count(bm, grid, [res] * 3, lo, hi, 0.0, 0.0)
+    fb = ops.new_filtered([res] * 3, dev)
+    counts = ops.vr_count(bm, grid, [res] * 3, lo, hi, 0.0, 0.0, filtered=fb)
     gg = torch.zeros_like(grid)
-    ms = timed(lambda: ops.reg_stencil(grid, bm, [res] * 3, lo, hi, 0.0, 0.0, counts, 0.1, 5e-4, gg))
+    ms = timed(lambda: ops.reg_stencil(grid, fb, [res] * 3, lo, hi, 0.0, 0.0, counts, 0.1, 5e-4, gg))
     vox = res ** 3
     out["stencil_full_grid"] = {"voxels_per_s": vox / (ms / 1e3), "ms": ms, "bytes_per_voxel": 12,
                                 "achieved_gbs": vox * 12 / (ms / 1e3) / 1e9, "deterministic": True}

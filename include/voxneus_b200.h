@@ -178,12 +178,42 @@ int vx_hash_encode_backward(float* table_grad, int n_levels, int log2_size, int 
                             const float xyz_max[3], int64_t n_points, const float* d_out, int64_t ld_d,
                             void* stream);
 
+/* Deterministic variants of the two scatter adjoints (vx_render_geometry_backward,
+ * vx_hash_encode_backward): every contribution is emitted as a (destination, value) pair at a
+ * fixed slot, stably radix-sorted by destination and summed per destination in slot order, so the
+ * gradient is bitwise reproducible. The caller provides a workspace of the size the *_workspace
+ * query returns (0 = sizes out of range). Hash variant: level_res_dev / level_weights_dev are
+ * device arrays of n_levels int32 / float32. */
+size_t vx_geometry_backward_det_workspace(int64_t n_rays, int n_samples, const int32_t res[3]);
+int vx_render_geometry_backward_det(const float* grid, const int32_t res[3], const float xyz_min[3],
+                                    const float xyz_max[3], const float* rays_o, const float* rays_d, const float* mid,
+                                    int64_t n_rays, int n_samples, const float* d_sdf, const float* d_normal,
+                                    const float* d_normal2, int64_t ld2, float* grid_grad, void* workspace,
+                                    size_t workspace_bytes, void* stream);
+size_t vx_hash_backward_det_workspace(int64_t n_points, int n_levels, int log2_size);
+int vx_hash_encode_backward_det(float* table_grad, int n_levels, int log2_size, int n_features,
+                                const int32_t* level_res_dev, const float* level_weights_dev, const float* pts_norm,
+                                const float* rays_o, const float* rays_d, const float* mid, int n_samples,
+                                const float xyz_min[3], const float xyz_max[3], int64_t n_points, const float* d_out,
+                                int64_t ld_d, void* workspace, size_t workspace_bytes, void* stream);
+
 /* Radiance MLP (models/radiance_mlp.py:42-53,81-98): rows x (n_points, in_dim) with row stride
  * ldx -> Linear(51,64) -> ReLU -> Linear(64,3) -> Sigmoid -> colors (n_points, 3). W0 (64,51),
  * b0 (64), W1 (3,64), b1 (3) as nn.Linear stores them. Only the 51 -> 64 -> 3 shape is fused. */
 int vx_radiance_mlp_forward(const float* x, int64_t ldx, int64_t n_points, int in_dim, int hidden, int out_dim,
                             const float* W0, const float* b0, const float* W1, const float* b1, float* colors,
                             void* stream);
+
+/* Appearance branch + MLP in one pass (models/voxneus.py:147-157): hash features of o + d*mid
+ * (16 levels x 2), SH of the ray direction and the normal are built in shared memory and fed to
+ * the 51-64-3 MLP; writes colors (n,3) and, when rows is given, the MLP input rows (row stride
+ * ld_rows >= 52, multiple of 4, 16-byte aligned; the adjoint's input). */
+int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, int n_features,
+                              const int32_t* level_res, const float* level_weights, const float* rays_o,
+                              const float* rays_d, const float* mid, int n_samples, const float xyz_min[3],
+                              const float xyz_max[3], int64_t n_points, const float* normals, const float* W0,
+                              const float* b0, const float* W1, const float* b1, float* colors, float* rows,
+                              int64_t ld_rows, void* stream);
 
 /* Blocks of vx_radiance_mlp_backward and the floats of one block's weight-gradient partial. */
 int vx_mlp_blocks(int64_t n_points);
@@ -258,9 +288,11 @@ int vx_vr_mark_corners(const int64_t* corners, int64_t n_corners, const int32_t 
 
 /* Counts V_R (counts[4] device uint64, zeroed by the caller): [all, relax, band, relax & band] with
  * relax = |xyz_min + idx*eps| < relax_radius (training/trainer.py:262-266; <= 0 disables) and
- * band = |f| < band (<= 0 disables). */
+ * band = |f| < band (<= 0 disables). filtered (nullable, 2 x vx_vr_bitmap_words words) receives
+ * the bitmaps bits & band and bits & band & relax (the regularizer's input). */
 int vx_vr_count(const uint32_t* bitmap, const float* grid, const int32_t res[3], const float xyz_min[3],
-                const float xyz_max[3], float relax_radius, float band, unsigned long long* counts, void* stream);
+                const float xyz_max[3], float relax_radius, float band, unsigned long long* counts,
+                uint32_t* filtered, void* stream);
 
 /* Writes the V_R list in ascending linear order (torch.unique order): verts (V,3) and linear (V),
  * each nullable, up to capacity entries. The relax filter applies only when counts[1] > 0. */
@@ -288,9 +320,11 @@ int vx_vr_compact_noalloc(const uint32_t* bitmap, const float* grid, const int32
 int64_t vx_reg_stencil_blocks(const int32_t res[3]);
 
 /* Fused eikonal + curvature closed forms (regularization/eikonal.py:13-171 and curvature.py:13-165 as
- * called by training/trainer.py:268-319) over the V_R bitmap, gather form (deterministic, no
- * atomics), accumulated into grad_grid with weights w_eik and w_curv and scale 2/|V_R| (|V_R| from
- * counts). losses (device float[2]) receives the monitoring losses. */
+ * called by training/trainer.py:268-319), gather form (deterministic, no atomics), accumulated into
+ * grad_grid with weights w_eik and w_curv and scale 2/|V_R|. bitmap is the filtered pair written by
+ * vx_vr_count; counts selects its relax half (the reference applies the relax filter only when a
+ * vertex passes it) and gives |V_R|. band is unused (applied by vx_vr_count); counter may be NULL.
+ * losses (device float[2], nullable) receives the monitoring losses. */
 int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[3], const float xyz_min[3],
                    const float xyz_max[3], float relax_radius, float band, const unsigned long long* counts,
                    float w_eik, float w_curv, float* grad_grid, double* partials, int64_t n_partials,

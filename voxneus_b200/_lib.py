@@ -22,6 +22,7 @@ I64 = ctypes.c_int64
 F32 = ctypes.c_float
 HI3 = ctypes.POINTER(ctypes.c_int32)  # host int32[3]
 HF3 = ctypes.POINTER(ctypes.c_float)  # host float[3]
+SZ = ctypes.c_size_t
 
 # name -> argument types; every function returns int status unless listed in _RESTYPES
 _PROTOS = {
@@ -46,7 +47,13 @@ _PROTOS = {
     "vx_appearance_forward": [P, I32, I32, I32, HI3, HF3, P, P, P, P, I32, HF3, HF3, I64, P, I64, I32, P, I64, I32,
                               P, I32, P],
     "vx_hash_encode_backward": [P, I32, I32, I32, HI3, HF3, P, P, P, P, I32, HF3, HF3, I64, P, I64, P],
+    "vx_geometry_backward_det_workspace": [I64, I32, HI3],
+    "vx_render_geometry_backward_det": [P, HI3, HF3, HF3, P, P, P, I64, I32, P, P, P, I64, P, P, SZ, P],
+    "vx_hash_backward_det_workspace": [I64, I32, I32],
+    "vx_hash_encode_backward_det": [P, I32, I32, I32, P, P, P, P, P, P, I32, HF3, HF3, I64, P, I64, P, SZ, P],
     "vx_radiance_mlp_forward": [P, I64, I64, I32, I32, I32, P, P, P, P, P, P],
+    "vx_appearance_mlp_forward": [P, I32, I32, I32, HI3, HF3, P, P, P, I32, HF3, HF3, I64, P, P, P, P, P, P, P, I64,
+                                  P],
     "vx_mlp_blocks": [I64],
     "vx_mlp_partial_floats": [],
     "vx_radiance_mlp_backward": [P, I64, I64, I32, I32, I32, P, P, P, P, P, P, P, P, P, P, P, P, I64, P],
@@ -60,7 +67,7 @@ _PROTOS = {
     "vx_vr_bitmap_words": [HI3],
     "vx_vr_compact_blocks": [HI3],
     "vx_vr_mark_corners": [P, I64, HI3, P, P],
-    "vx_vr_count": [P, P, HI3, HF3, HF3, F32, F32, P, P],
+    "vx_vr_count": [P, P, HI3, HF3, HF3, F32, F32, P, P, P],
     "vx_vr_compact": [P, P, HI3, HF3, HF3, F32, F32, P, P, I64, P, P, I64, P],
     "vx_vr_compact_noalloc": [P, P, HI3, HF3, HF3, F32, F32, P, P, P, I64, P],
     "vx_reg_stencil_blocks": [HI3],
@@ -74,6 +81,8 @@ _RESTYPES = {
     "vx_vr_bitmap_words": I64,
     "vx_vr_compact_blocks": I64,
     "vx_reg_stencil_blocks": I64,
+    "vx_geometry_backward_det_workspace": ctypes.c_size_t,
+    "vx_hash_backward_det_workspace": ctypes.c_size_t,
 }
 
 _lib = None

@@ -8,106 +8,9 @@
 // size, L2-resident), and the adjoint scatters with float2 atomics (sm_90+ vector atomics).
 // Hash indices are computed in uint32 arithmetic: the low log2(T) bits of
 // x*1 ^ y*2654435761 ^ z*805459861 equal the reference's int64 value modulo 2^log2(T).
-#include "common.cuh"
+#include "hashgrid.cuh"
 
 namespace vx {
-
-constexpr int kMaxLevels = 32;
-
-struct HashArgs {
-  const float* table;  // (L, T, 2)
-  float* table_grad;   // adjoint output, (L, T, 2)
-  int L, log2T;
-  int res[kMaxLevels];
-  float lw[kMaxLevels];  // NeuS2 lambda level weights (0 = skipped level)
-  // position source: normalised points (P,3), or world positions o + d * t of (rays, S)
-  const float* pts;
-  const float* rays_o;
-  const float* rays_d;
-  const float* mid;
-  int S;
-  float lo[3], den[3];
-  int64_t P;
-  float* out;  // rows of length >= 2L
-  int64_t ld;
-  const float* d_out;  // adjoint input rows
-  int64_t ld_d;
-  int sh_col;          // -1: no SH
-  const float* dirs;   // per-sample dirs (row stride dir_ss) or per-ray via rays_d when null
-  int64_t dir_ss;
-  int nrm_col;         // -1: no normal copy
-  const float* normals;
-  int pad_col;         // -1: none; column set to 0
-};
-
-__device__ __forceinline__ void sample_pos(const HashArgs& a, int64_t i, float x[3]) {
-  if (a.pts) {
-    x[0] = a.pts[3 * i];
-    x[1] = a.pts[3 * i + 1];
-    x[2] = a.pts[3 * i + 2];
-  } else {
-    const int64_t r = i / a.S;
-    const float t = a.mid[i];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-      const float p = ray_at(__ldg(a.rays_o + 3 * r + c), __ldg(a.rays_d + 3 * r + c), t);
-      x[c] = __fdiv_rn(__fsub_rn(p, a.lo[c]), a.den[c]);
-    }
-  }
-  // RadianceHashGrid.forward clamps to [0, 1] (radiance_hash.py:213)
-#pragma unroll
-  for (int c = 0; c < 3; ++c) x[c] = fminf(fmaxf(x[c], 0.0f), 1.0f);
-}
-
-__device__ __forceinline__ uint32_t hash3(uint32_t x, uint32_t y, uint32_t z, uint32_t mask) {
-  return (x * 1u ^ y * 2654435761u ^ z * 805459861u) & mask;
-}
-
-struct LevelCell {
-  uint32_t h[8];
-  float w[8];
-};
-
-__device__ __forceinline__ void level_cell(const float x[3], int res, uint32_t mask, LevelCell& c) {
-  const float fr = (float)res;
-  int c0[3];
-  float d[3];
-#pragma unroll
-  for (int k = 0; k < 3; ++k) {
-    const float s = x[k] * fr;
-    const float fl = floorf(s);
-    c0[k] = (int)fl;
-    d[k] = s - fl;
-  }
-  const float ox = 1.0f - d[0], oy = 1.0f - d[1], oz = 1.0f - d[2];
-#pragma unroll
-  for (int k = 0; k < 8; ++k) {
-    const uint32_t cx = (uint32_t)(c0[0] + ((k >> 2) & 1));
-    const uint32_t cy = (uint32_t)(c0[1] + ((k >> 1) & 1));
-    const uint32_t cz = (uint32_t)(c0[2] + (k & 1));
-    c.h[k] = hash3(cx, cy, cz, mask);
-    c.w[k] = ((k & 4) ? d[0] : ox) * ((k & 2) ? d[1] : oy) * ((k & 1) ? d[2] : oz);
-  }
-}
-
-__device__ __forceinline__ void sh16(float x, float y, float z, float o[16]) {
-  o[0] = 0.28209479177387814f;
-  o[1] = -0.4886025119029199f * y;
-  o[2] = 0.4886025119029199f * z;
-  o[3] = -0.4886025119029199f * x;
-  o[4] = 1.0925484305920792f * x * y;
-  o[5] = -1.0925484305920792f * y * z;
-  o[6] = 0.31539156525252005f * (2.0f * z * z - x * x - y * y);
-  o[7] = -1.0925484305920792f * x * z;
-  o[8] = 0.5462742152960396f * (x * x - y * y);
-  o[9] = -0.5900435899266435f * y * (3.0f * x * x - y * y);
-  o[10] = 2.890611442640554f * x * y * z;
-  o[11] = -0.4570457994644658f * y * (4.0f * z * z - x * x - y * y);
-  o[12] = 0.3731763325901154f * z * (2.0f * z * z - 3.0f * x * x - 3.0f * y * y);
-  o[13] = -0.4570457994644658f * x * (4.0f * z * z - x * x - y * y);
-  o[14] = 1.445305721320277f * z * (x * x - y * y);
-  o[15] = -0.5900435899266435f * x * (x * x - 3.0f * y * y);
-}
 
 __global__ void __launch_bounds__(256) k_appearance_fwd(HashArgs a) {
   const uint32_t mask = (1u << a.log2T) - 1u;
@@ -192,36 +95,6 @@ __global__ void __launch_bounds__(256) k_hash_bwd(HashArgs a) {
 #pragma unroll
       for (int k = 0; k < 8; ++k) atomicAdd(tab + c.h[k], make_float2(c.w[k] * g0, c.w[k] * g1));
     }
-  }
-}
-
-static int fill_hash(HashArgs& a, const float* table, int n_levels, int log2_size, int n_features,
-                     const int32_t* level_res, const float* level_weights) {
-  VX_REQUIRE(n_levels >= 1 && n_levels <= kMaxLevels, "n_levels must be in [1, %d]", kMaxLevels);
-  VX_REQUIRE(log2_size >= 1 && log2_size <= 30, "log2 table size must be in [1, 30]");
-  VX_REQUIRE(n_features == 2, "only 2 features per level are supported (got %d)", n_features);
-  VX_REQUIRE(level_res, "level resolutions are null");
-  a.table = table;
-  a.L = n_levels;
-  a.log2T = log2_size;
-  for (int l = 0; l < n_levels; ++l) {
-    VX_REQUIRE(level_res[l] >= 1, "level resolution must be >= 1");
-    a.res[l] = level_res[l];
-    a.lw[l] = level_weights ? level_weights[l] : 1.0f;
-  }
-  return VX_OK;
-}
-
-static void fill_positions(HashArgs& a, const float* pts_norm, const float* rays_o, const float* rays_d,
-                           const float* mid, int S, const float xyz_min[3], const float xyz_max[3]) {
-  a.pts = pts_norm;
-  a.rays_o = rays_o;
-  a.rays_d = rays_d;
-  a.mid = mid;
-  a.S = S > 0 ? S : 1;
-  for (int c = 0; c < 3; ++c) {
-    a.lo[c] = xyz_min ? xyz_min[c] : 0.f;
-    a.den[c] = xyz_min ? (xyz_max[c] - xyz_min[c]) + 1e-8f : 1.f;
   }
 }
 

@@ -7,7 +7,7 @@
 // as a register-tiled SIMT GEMM: thread (lane, warp) owns samples 4*lane..4*lane+3 and hidden
 // units 8*warp..8*warp+7, reading the inputs as 16-byte shared loads and the weights as
 // warp-broadcast loads. FP32 throughout (the parity bar of the colours is 1e-5 relative).
-#include "common.cuh"
+#include "hashgrid.cuh"
 
 namespace vx {
 
@@ -115,6 +115,123 @@ __global__ void __launch_bounds__(256) k_mlp_fwd(const float* __restrict__ X, in
 #pragma unroll
         for (int g = 0; g < 8; ++g) o += red[(g * TM + tid) * NO + c];
         out[(m0 + tid) * NO + c] = sigmoidf_ref(o);
+      }
+    }
+  }
+}
+
+// Appearance + MLP forward for (rays, midpoints): the 51 input features of a 128-sample tile
+// are built straight into the shared tile — two threads per sample, each gathering 8 hash
+// levels (float2 corner features); SH of the view direction and the normal complete the row
+// — then the MLP runs on the tile. kRows also writes the rows (the adjoint's input), as
+// 16-byte stores of each thread's columns.
+template <bool kRows>
+__global__ void __launch_bounds__(256) k_appearance_mlp_fwd(HashArgs a, MlpW w, float* __restrict__ colors) {
+  __shared__ __align__(16) float XT[KP][TM];
+  __shared__ __align__(16) float W0T[KP][NH];
+  __shared__ float B0[NH], W1s[NO][NH], B1[NO];
+  const int tid = threadIdx.x, tm = tid & 31, tn = tid >> 5;
+  load_weights(w, W0T, B0, W1s, B1, tid, blockDim.x);
+  const uint32_t mask = (1u << a.log2T) - 1u;
+  const size_t T = (size_t)1 << a.log2T;
+  const int64_t ntiles = (a.P + TM - 1) / TM;
+  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
+    const int64_t m0 = t * TM;
+    __syncthreads();
+    {
+      const int m = tid & (TM - 1), half = tid >> 7;
+      const int64_t i = m0 + m;
+      float feat[16];
+      float extra[16];
+      if (i < a.P) {
+        float x[3];
+        sample_pos(a, i, x);
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+          const int l = 8 * half + q;
+          const float lw = a.lw[l];
+          float f0 = 0.0f, f1 = 0.0f;
+          if (lw != 0.0f) {
+            LevelCell c;
+            level_cell(x, a.res[l], mask, c);
+            const float2* tab = reinterpret_cast<const float2*>(a.table) + (size_t)l * T;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+              const float2 e = __ldg(tab + c.h[k]);
+              f0 = fmaf(c.w[k], e.x, f0);
+              f1 = fmaf(c.w[k], e.y, f1);
+            }
+            if (lw < 1.0f) {
+              f0 *= lw;
+              f1 *= lw;
+            }
+          }
+          feat[2 * q] = f0;
+          feat[2 * q + 1] = f1;
+        }
+        if (half == 0) {
+          const int64_t r = i / a.S;
+          sh16(__ldg(a.rays_d + 3 * r), __ldg(a.rays_d + 3 * r + 1), __ldg(a.rays_d + 3 * r + 2), extra);
+        } else {
+          extra[0] = a.normals[3 * i];
+          extra[1] = a.normals[3 * i + 1];
+          extra[2] = a.normals[3 * i + 2];
+          extra[3] = 0.0f;
+        }
+      } else {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) feat[q] = extra[q] = 0.0f;
+      }
+#pragma unroll
+      for (int q = 0; q < 16; ++q) XT[16 * half + q][m] = feat[q];
+      if (half == 0) {
+#pragma unroll
+        for (int q = 0; q < 16; ++q) XT[32 + q][m] = extra[q];
+      } else {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) XT[48 + q][m] = extra[q];
+      }
+      if (kRows && i < a.P) {
+        float4* row = reinterpret_cast<float4*>(a.out + i * a.ld);
+#pragma unroll
+        for (int q = 0; q < 4; ++q)
+          row[4 * half + q] = make_float4(feat[4 * q], feat[4 * q + 1], feat[4 * q + 2], feat[4 * q + 3]);
+        if (half == 0) {
+#pragma unroll
+          for (int q = 0; q < 4; ++q)
+            row[8 + q] = make_float4(extra[4 * q], extra[4 * q + 1], extra[4 * q + 2], extra[4 * q + 3]);
+        } else {
+          row[12] = make_float4(extra[0], extra[1], extra[2], extra[3]);
+        }
+      }
+    }
+    __syncthreads();
+    float z[4][8];
+    layer0(XT, W0T, B0, tm, tn, z);
+    float part[4][NO];
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int c = 0; c < NO; ++c) {
+        float acc = 0.0f;
+#pragma unroll
+        for (int j = 0; j < 8; ++j) acc = fmaf(W1s[c][8 * tn + j], fmaxf(z[s][j], 0.0f), acc);
+        part[s][c] = acc;
+      }
+    __syncthreads();
+    float* red = &XT[0][0];
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int c = 0; c < NO; ++c) red[(tn * TM + 4 * tm + s) * NO + c] = part[s][c];
+    __syncthreads();
+    if (tid < TM && m0 + tid < a.P) {
+#pragma unroll
+      for (int c = 0; c < NO; ++c) {
+        float o = B1[c];
+#pragma unroll
+        for (int g = 0; g < 8; ++g) o += red[(g * TM + tid) * NO + c];
+        colors[(m0 + tid) * NO + c] = sigmoidf_ref(o);
       }
     }
   }
@@ -326,6 +443,37 @@ constexpr size_t kBwdSmem =
 using namespace vx;
 
 extern "C" {
+
+int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, int n_features,
+                              const int32_t* level_res, const float* level_weights, const float* rays_o,
+                              const float* rays_d, const float* mid, int n_samples, const float xyz_min[3],
+                              const float xyz_max[3], int64_t n_points, const float* normals, const float* W0,
+                              const float* b0, const float* W1, const float* b1, float* colors, float* rows,
+                              int64_t ld_rows, void* stream) {
+  HashArgs a{};
+  if (int s = fill_hash(a, table, n_levels, log2_size, n_features, level_res, level_weights)) return s;
+  VX_REQUIRE(n_levels == 16, "the fused appearance MLP takes 16 hash levels x 2 features (got %d)", n_levels);
+  VX_REQUIRE(n_points >= 0 && n_samples >= 1, "bad sizes");
+  if (n_points == 0) return VX_OK;
+  VX_REQUIRE(table && rays_o && rays_d && mid && xyz_min && xyz_max && normals && W0 && b0 && W1 && b1 && colors,
+             "null pointer");
+  VX_REQUIRE(!rows || (ld_rows >= KP && ld_rows % 4 == 0 && ((uintptr_t)rows & 15) == 0),
+             "rows need a row stride >= 52 floats, a multiple of 4, and 16-byte alignment");
+  fill_positions(a, nullptr, rays_o, rays_d, mid, n_samples, xyz_min, xyz_max);
+  a.P = n_points;
+  a.out = rows;
+  a.ld = ld_rows;
+  a.normals = normals;
+  MlpW w{W0, b0, W1, b1};
+  const int64_t tiles = (n_points + TM - 1) / TM;
+  const unsigned blocks = (unsigned)(tiles < (int64_t)kSMs * 4 ? tiles : (int64_t)kSMs * 4);
+  if (rows)
+    k_appearance_mlp_fwd<true><<<blocks, 256, 0, (cudaStream_t)stream>>>(a, w, colors);
+  else
+    k_appearance_mlp_fwd<false><<<blocks, 256, 0, (cudaStream_t)stream>>>(a, w, colors);
+  count_launches(1);
+  return check_launch("appearance_mlp_forward");
+}
 
 int vx_mlp_blocks(int64_t n_points) {
   const int64_t tiles = (n_points + TM - 1) / TM;

@@ -160,33 +160,20 @@ __global__ void __launch_bounds__(256) k_curvature_list(const float* __restrict_
 
 constexpr int TZ = 32, TY = 4, TX = 4;  // output tile (z fastest)
 constexpr int HZ = TZ + 4, HY = TY + 4, HX = TX + 4;  // SDF box, halo 2
-constexpr int MZ = TZ + 2, MY = TY + 2, MX = TX + 2;  // active-mask box, halo 1
+constexpr int MZ = TZ + 2, MY = TY + 2, MX = TX + 2;  // vertex box, halo 1
+constexpr int NVB = MX * MY * MZ;                      // vertices in the halo-1 box
 
 struct StencilArgs {
   const float* f;
-  const uint32_t* bm;
+  const uint32_t* fb;  // filtered V_R bitmaps from vx_vr_count: [bits & band | bits & band & relax]
+  int64_t nwords;
   Grid g;
   const unsigned long long* counts;  // from vx_vr_count
   float relax_r;
-  float band;
   float w_eik, w_curv;
   float* gg;
   int tiles_z, tiles_y;
 };
-
-__device__ __forceinline__ bool vr_member(const StencilArgs& a, int x, int y, int z, bool relax_on) {
-  const int idx = lin3(a.g, x, y, z);
-  if (!(__ldg(a.bm + (idx >> 5)) & (1u << (idx & 31)))) return false;
-  if (relax_on) {
-    const float wx = __fadd_rn(a.g.lo[0], __fmul_rn((float)x, a.g.eps[0]));
-    const float wy = __fadd_rn(a.g.lo[1], __fmul_rn((float)y, a.g.eps[1]));
-    const float wz = __fadd_rn(a.g.lo[2], __fmul_rn((float)z, a.g.eps[2]));
-    if (!(sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(wx, wx), __fmul_rn(wy, wy)), __fmul_rn(wz, wz))) < a.relax_r))
-      return false;
-  }
-  if (a.band > 0.0f && !(fabsf(__ldg(a.f + idx)) < a.band)) return false;
-  return true;
-}
 
 __device__ __forceinline__ void tile_origin(const StencilArgs& a, int t, int& x0, int& y0, int& z0) {
   const int tz = t % a.tiles_z;
@@ -197,9 +184,9 @@ __device__ __forceinline__ void tile_origin(const StencilArgs& a, int t, int& x0
   x0 = tx * TX;
 }
 
-// Does the halo-1 box of tile t hold any V_R bit? Word-level test by one warp, one lane per
-// (x, y) row of the box (the z range [z0-1, z0+TZ] covers at most 3 words).
-__device__ __forceinline__ bool tile_has_bits_warp(const StencilArgs& a, int t, int lane) {
+// Does the halo-1 box of tile t hold any V_R vertex? Word-level test of the filtered bitmap by
+// one warp, one lane per (x, y) row of the box (z range [z0-1, z0+TZ] covers at most 3 words).
+__device__ __forceinline__ bool tile_has_bits_warp(const StencilArgs& a, const uint32_t* bm, int t, int lane) {
   int x0, y0, z0;
   tile_origin(a, t, x0, y0, z0);
   bool hit = false;
@@ -212,26 +199,31 @@ __device__ __forceinline__ bool tile_has_bits_warp(const StencilArgs& a, int t, 
       uint32_t m = 0xffffffffu;
       if (w == (b0 >> 5)) m &= 0xffffffffu << (b0 & 31);
       if (w == (b1 >> 5)) m &= 0xffffffffu >> (31 - (b1 & 31));
-      hit |= (__ldg(a.bm + w) & m) != 0u;
+      hit |= (__ldg(bm + w) & m) != 0u;
     }
   }
   return __any_sync(0xffffffffu, hit);
 }
 
 // Persistent grid over 32x4x4 tiles taken 8 at a time; blockDim = (32, 4, 2). Each warp tests one
-// tile of the batch with word-level bitmap reads, so an empty tile costs one load per lane and
-// an eighth of a barrier. For an active tile the SDF box (halo 2) is staged first, the active
-// interior mask (halo 1) is built from the bitmap with the narrow-band test read from that box,
-// and each thread owns output voxels (z, y, x) and (z, y, x + 2). Per-block loss partials;
-// k_reg_finalize reduces them.
+// tile of the batch against the filtered bitmap, so an empty tile costs one load per lane. For
+// an active tile: stage the SDF box (halo 2); evaluate every active interior vertex of the halo-1
+// box once, storing the contribution it makes to itself (curvature centre) and to each face
+// neighbour (eikonal +-dL/dn_a / 2eps_a plus curvature L_a/eps_a^2, scaled); then every output
+// voxel sums the <= 7 terms that land on it. Per-block loss partials; k_reg_finalize reduces them.
 __global__ void __launch_bounds__(256) k_reg_stencil(StencilArgs a, double* __restrict__ partials, int ntiles) {
   __shared__ float F[HX][HY][HZ];
-  __shared__ uint8_t M[MX][MY][MZ];
+  __shared__ float T[7][NVB];  // [0] centre, [1+2a] to v+e_a, [2+2a] to v-e_a
   __shared__ double red[3][8];
   __shared__ int active[8];
   const int tid = threadIdx.x + 32 * (threadIdx.y + 4 * threadIdx.z);
   const bool relax_on = a.relax_r > 0.0f && a.counts[1] > 0;
-  const unsigned long long nv = a.counts[a.band > 0.0f ? (relax_on ? 3 : 2) : (relax_on ? 1 : 0)];
+  const bool band_on = a.counts[2] != a.counts[0] || a.counts[3] != a.counts[1];
+  (void)band_on;
+  const uint32_t* bm = a.fb + (relax_on ? a.nwords : 0);
+  // |V_R| after the filters: counts[1 or 3] (relax) / counts[0 or 2] (no relax); the filtered
+  // bitmaps already carry the band, so the band count is the one to use
+  const unsigned long long nv = relax_on ? a.counts[3] : a.counts[2];
   const float inv_nv = nv > 0 ? 2.0f / (float)nv : 0.0f;
   const float dx = 2.0f * a.g.eps[0], dy = 2.0f * a.g.eps[1], dz = 2.0f * a.g.eps[2];
   const float ex2 = a.g.eps[0] * a.g.eps[0], ey2 = a.g.eps[1] * a.g.eps[1], ez2 = a.g.eps[2] * a.g.eps[2];
@@ -240,96 +232,89 @@ __global__ void __launch_bounds__(256) k_reg_stencil(StencilArgs a, double* __re
   for (int tb = blockIdx.x * 8; tb < ntiles; tb += gridDim.x * 8) {
     {
       const int w = tid >> 5;
-      const bool hit = (tb + w < ntiles) ? tile_has_bits_warp(a, tb + w, tid & 31) : false;
+      const bool hit = (tb + w < ntiles) ? tile_has_bits_warp(a, bm, tb + w, tid & 31) : false;
       if ((tid & 31) == 0) active[w] = hit;
     }
     __syncthreads();
     for (int wt = 0; wt < 8; ++wt) {
-    if (!active[wt]) continue;
-    int x0, y0, z0;
-    tile_origin(a, tb + wt, x0, y0, z0);
-    for (int q = tid; q < HX * HY * HZ; q += 256) {
-      const int hz = q % HZ, hy = (q / HZ) % HY, hx = q / (HZ * HY);
-      const int x = x0 - 2 + hx, y = y0 - 2 + hy, z = z0 - 2 + hz;
-      float v = 0.0f;
-      if (x >= 0 && x < a.g.rx && y >= 0 && y < a.g.ry && z >= 0 && z < a.g.rz) v = __ldg(a.f + lin3(a.g, x, y, z));
-      F[hx][hy][hz] = v;
-    }
-    __syncthreads();
-    // active interior mask of the halo-1 box (band test on the staged SDF)
-    for (int q = tid; q < MX * MY * MZ; q += 256) {
-      const int mz = q % MZ, my = (q / MZ) % MY, mx = q / (MZ * MY);
-      const int x = x0 - 1 + mx, y = y0 - 1 + my, z = z0 - 1 + mz;
-      uint8_t m = 0;
-      if (x >= 1 && x <= a.g.rx - 2 && y >= 1 && y <= a.g.ry - 2 && z >= 1 && z <= a.g.rz - 2) {
-        const int idx = lin3(a.g, x, y, z);
-        bool on = (__ldg(a.bm + (idx >> 5)) >> (idx & 31)) & 1u;
-        if (on && relax_on) {
-          const float wx = __fadd_rn(a.g.lo[0], __fmul_rn((float)x, a.g.eps[0]));
-          const float wy = __fadd_rn(a.g.lo[1], __fmul_rn((float)y, a.g.eps[1]));
-          const float wz = __fadd_rn(a.g.lo[2], __fmul_rn((float)z, a.g.eps[2]));
-          on = sqrtf(__fadd_rn(__fadd_rn(__fmul_rn(wx, wx), __fmul_rn(wy, wy)), __fmul_rn(wz, wz))) < a.relax_r;
+      if (!active[wt]) continue;
+      int x0, y0, z0;
+      tile_origin(a, tb + wt, x0, y0, z0);
+      for (int q = tid; q < HX * HY * HZ; q += 256) {
+        const int hz = q % HZ, hy = (q / HZ) % HY, hx = q / (HZ * HY);
+        const int x = x0 - 2 + hx, y = y0 - 2 + hy, z = z0 - 2 + hz;
+        float v = 0.0f;
+        if (x >= 0 && x < a.g.rx && y >= 0 && y < a.g.ry && z >= 0 && z < a.g.rz)
+          v = __ldg(a.f + lin3(a.g, x, y, z));
+        F[hx][hy][hz] = v;
+      }
+      __syncthreads();
+      // per-vertex terms of the halo-1 box
+      for (int q = tid; q < NVB; q += 256) {
+        const int mz = q % MZ, my = (q / MZ) % MY, mx = q / (MZ * MY);
+        const int x = x0 - 1 + mx, y = y0 - 1 + my, z = z0 - 1 + mz;
+        bool on = x >= 1 && x <= a.g.rx - 2 && y >= 1 && y <= a.g.ry - 2 && z >= 1 && z <= a.g.rz - 2;
+        if (on) {
+          const int idx = lin3(a.g, x, y, z);
+          on = (__ldg(bm + (idx >> 5)) >> (idx & 31)) & 1u;
         }
-        if (on && a.band > 0.0f) on = fabsf(F[mx + 1][my + 1][mz + 1]) < a.band;
-        m = on ? 1 : 0;
-      }
-      M[mx][my][mz] = m;
-    }
-    __syncthreads();
-    const int lz = threadIdx.x, ly = threadIdx.y;
-#pragma unroll
-    for (int rep = 0; rep < 2; ++rep) {
-      const int lx = threadIdx.z + 2 * rep;
-      const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
-      if (x >= a.g.rx || y >= a.g.ry || z >= a.g.rz) continue;
-      // SDF box coordinates of this voxel: (lx+2, ly+2, lz+2); mask box: (lx+1, ly+1, lz+1)
-      float acc = 0.0f;
-      bool touched = false;
-      // vertex v = voxel + sgn * e_ax contributes to this voxel; nb == 0 is v = voxel itself
-#pragma unroll
-      for (int nb = 0; nb < 7; ++nb) {
-        const int ax = nb == 0 ? -1 : (nb - 1) >> 1;
-        const int sgn = nb == 0 ? 0 : (((nb - 1) & 1) ? 1 : -1);
-        const int mx = lx + 1 + (ax == 0 ? sgn : 0);
-        const int my = ly + 1 + (ax == 1 ? sgn : 0);
-        const int mz = lz + 1 + (ax == 2 ? sgn : 0);
-        if (!M[mx][my][mz]) continue;
-        touched = true;
-        const int hx = mx + 1, hy = my + 1, hz = mz + 1;
-        const float fc = F[hx][hy][hz];
-        const float fxp = F[hx + 1][hy][hz], fxm = F[hx - 1][hy][hz];
-        const float fyp = F[hx][hy + 1][hz], fym = F[hx][hy - 1][hz];
-        const float fzp = F[hx][hy][hz + 1], fzm = F[hx][hy][hz - 1];
-        const float Lx = (fxp + fxm - 2.0f * fc) / ex2;
-        const float Ly = (fyp + fym - 2.0f * fc) / ey2;
-        const float Lz = (fzp + fzm - 2.0f * fc) / ez2;
-        const float nx = (fxp - fxm) / dx, ny = (fyp - fym) / dy, nz = (fzp - fzm) / dz;
-        if (nb == 0) {
-          // curvature centre term (curvature_grad.cu: scale * (-2 Lx/ex^2 - 2 Ly/ey^2 - 2 Lz/ez^2))
-          acc += sc * (-2.0f * Lx / ex2 - 2.0f * Ly / ey2 - 2.0f * Lz / ez2);
-          const double l = sqrt((double)nx * nx + (double)ny * ny + (double)nz * nz + 1e-16);
-          le += (l - 1.0) * (l - 1.0);
-          lc += (double)Lx * Lx + (double)Ly * Ly + (double)Lz * Lz;
-          ln += 1.0;
-          continue;
+        float t0 = 0.f, tpx = 0.f, tmx = 0.f, tpy = 0.f, tmy = 0.f, tpz = 0.f, tmz = 0.f;
+        if (on) {
+          const int hx = mx + 1, hy = my + 1, hz = mz + 1;
+          const float fc = F[hx][hy][hz];
+          const float fxp = F[hx + 1][hy][hz], fxm = F[hx - 1][hy][hz];
+          const float fyp = F[hx][hy + 1][hz], fym = F[hx][hy - 1][hz];
+          const float fzp = F[hx][hy][hz + 1], fzm = F[hx][hy][hz - 1];
+          const float Lx = (fxp + fxm - 2.0f * fc) / ex2;
+          const float Ly = (fyp + fym - 2.0f * fc) / ey2;
+          const float Lz = (fzp + fzm - 2.0f * fc) / ez2;
+          const float nx = (fxp - fxm) / dx, ny = (fyp - fym) / dy, nz = (fzp - fzm) / dz;
+          const float len = sqrtf(nx * nx + ny * ny + nz * nz);
+          // eikonal_grad.cu: scale = 2/|V_R| (1 - 1/(|n| + 1e-8)) w; +-scale*n_a / (2 eps_a)
+          const float se = inv_nv * (1.0f - 1.0f / (len + 1e-8f)) * a.w_eik;
+          const float ex = (se * nx) / dx, ey = (se * ny) / dy, ez = (se * nz) / dz;
+          // curvature_grad.cu: centre scale*(-2 Lx/ex^2 - 2 Ly/ey^2 - 2 Lz/ez^2), neighbours scale*L_a/eps_a^2
+          const float cx = sc * (Lx / ex2), cy = sc * (Ly / ey2), cz = sc * (Lz / ez2);
+          t0 = sc * (-2.0f * Lx / ex2 - 2.0f * Ly / ey2 - 2.0f * Lz / ez2);
+          tpx = ex + cx;
+          tmx = -ex + cx;
+          tpy = ey + cy;
+          tmy = -ey + cy;
+          tpz = ez + cz;
+          tmz = -ez + cz;
+          if (mx >= 1 && mx <= TX && my >= 1 && my <= TY && mz >= 1 && mz <= TZ) {  // owned by this tile
+            const double l = sqrt((double)nx * nx + (double)ny * ny + (double)nz * nz + 1e-16);
+            le += (l - 1.0) * (l - 1.0);
+            lc += (double)Lx * Lx + (double)Ly * Ly + (double)Lz * Lz;
+            ln += 1.0;
+          }
         }
-        const float len = sqrtf(nx * nx + ny * ny + nz * nz);
-        const float se = inv_nv * (1.0f - 1.0f / (len + 1e-8f)) * a.w_eik;
-        const float na = ax == 0 ? nx : (ax == 1 ? ny : nz);
-        const float da = ax == 0 ? dx : (ax == 1 ? dy : dz);
-        const float La = ax == 0 ? Lx : (ax == 1 ? Ly : Lz);
-        const float ea2 = ax == 0 ? ex2 : (ax == 1 ? ey2 : ez2);
-        // sgn < 0: voxel = v + e_ax receives +dL/dn_ax / (2 eps); sgn > 0: voxel = v - e_ax receives -
-        const float ve = (se * na) / da;
-        acc += (sgn < 0) ? ve : -ve;
-        acc += sc * (La / ea2);
+        T[0][q] = t0;
+        T[1][q] = tpx;
+        T[2][q] = tmx;
+        T[3][q] = tpy;
+        T[4][q] = tmy;
+        T[5][q] = tpz;
+        T[6][q] = tmz;
       }
-      if (touched && acc != 0.0f) {
-        float* p = a.gg + lin3(a.g, x, y, z);
-        *p += acc;
+      __syncthreads();
+      const int lz = threadIdx.x, ly = threadIdx.y;
+#pragma unroll
+      for (int rep = 0; rep < 2; ++rep) {
+        const int lx = threadIdx.z + 2 * rep;
+        const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
+        if (x >= a.g.rx || y >= a.g.ry || z >= a.g.rz) continue;
+        const int c = ((lx + 1) * MY + (ly + 1)) * MZ + (lz + 1);  // this voxel in the vertex box
+        float acc = T[0][c];
+        acc += T[1][c - MY * MZ] + T[2][c + MY * MZ];  // from v - e_x (to v + e_x) and v + e_x (to v - e_x)
+        acc += T[3][c - MZ] + T[4][c + MZ];
+        acc += T[5][c - 1] + T[6][c + 1];
+        if (acc != 0.0f) {
+          float* p = a.gg + lin3(a.g, x, y, z);
+          *p += acc;
+        }
       }
-    }
-    __syncthreads();  // F and M are rewritten by the next tile
+      __syncthreads();  // F and T are rewritten by the next tile
     }
     __syncthreads();  // active[] is rewritten by the next batch
   }
@@ -462,11 +447,12 @@ int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[
              (long long)(3 * nb));
   StencilArgs a;
   a.f = grid;
-  a.bm = bitmap;
+  a.fb = bitmap;
+  a.nwords = ((int64_t)res[0] * res[1] * res[2] + 31) / 32;
   a.g = make_grid(res, xyz_min, xyz_max);
   a.counts = counts;
   a.relax_r = relax_radius;
-  a.band = band;
+  (void)band;
   a.w_eik = w_eik;
   a.w_curv = w_curv;
   a.gg = grad_grid;

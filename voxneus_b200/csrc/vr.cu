@@ -67,10 +67,14 @@ __global__ void k_vr_mark_list(const int64_t* __restrict__ corners, int64_t n, G
   }
 }
 
-__global__ void __launch_bounds__(256) k_vr_count(VrArgs a, unsigned long long* __restrict__ counts) {
+// Counts, and (when `filtered` is given) the filtered bitmaps: filtered[w] = bits & band,
+// filtered[nwords + w] = bits & band & relax.
+__global__ void __launch_bounds__(256) k_vr_count(VrArgs a, unsigned long long* __restrict__ counts,
+                                                  uint32_t* __restrict__ filtered) {
   unsigned long long c[4] = {0, 0, 0, 0};
   for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < a.nwords; w += (int64_t)gridDim.x * blockDim.x) {
     uint32_t bits = a.bm[w];
+    uint32_t f_band = 0, f_both = 0;
     while (bits) {
       const int b = __ffs(bits) - 1;
       bits &= bits - 1;
@@ -84,6 +88,12 @@ __global__ void __launch_bounds__(256) k_vr_count(VrArgs a, unsigned long long* 
       c[1] += r;
       c[2] += bd;
       c[3] += (r && bd);
+      f_band |= (bd ? 1u : 0u) << b;
+      f_both |= ((r && bd) ? 1u : 0u) << b;
+    }
+    if (filtered) {
+      filtered[w] = f_band;
+      filtered[a.nwords + w] = f_both;
     }
   }
   __shared__ unsigned long long sc[4][8];
@@ -310,11 +320,12 @@ int vx_vr_mark_corners(const int64_t* corners, int64_t n_corners, const int32_t 
 }
 
 int vx_vr_count(const uint32_t* bitmap, const float* grid, const int32_t res[3], const float xyz_min[3],
-                const float xyz_max[3], float relax_radius, float band, unsigned long long* counts, void* stream) {
+                const float xyz_max[3], float relax_radius, float band, unsigned long long* counts,
+                uint32_t* filtered, void* stream) {
   VrArgs a;
   if (int s = make_vr(a, bitmap, grid, res, xyz_min, xyz_max, relax_radius, band)) return s;
   VX_REQUIRE(counts, "counts is null");
-  k_vr_count<<<grid_for(a.nwords, 256, 8), 256, 0, (cudaStream_t)stream>>>(a, counts);
+  k_vr_count<<<grid_for(a.nwords, 256, 8), 256, 0, (cudaStream_t)stream>>>(a, counts, filtered);
   count_launches(1);
   return check_launch("vr_count");
 }

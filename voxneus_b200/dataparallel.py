@@ -30,11 +30,17 @@ class GradExchange:
             p.grad.div_(self.world)
 
     def union_bitmap(self, bitmap: torch.Tensor) -> None:
-        gathered = torch.empty(self.world, bitmap.numel(), dtype=bitmap.dtype, device=bitmap.device)
-        dist.all_gather_into_tensor(gathered, bitmap.reshape(-1), group=self.group)
-        out = gathered[0].clone()
+        flat = bitmap.reshape(-1)
+        if dist.get_backend(self.group) == "nccl":
+            gathered = torch.empty(self.world, flat.numel(), dtype=flat.dtype, device=flat.device)
+            dist.all_gather_into_tensor(gathered, flat, group=self.group)
+            parts = list(gathered)
+        else:
+            parts = [torch.empty_like(flat) for _ in range(self.world)]
+            dist.all_gather(parts, flat, group=self.group)
+        out = parts[0].clone()
         for r in range(1, self.world):
-            out.bitwise_or_(gathered[r])
+            out.bitwise_or_(parts[r])
         bitmap.copy_(out.reshape(bitmap.shape))
 
 

@@ -345,9 +345,70 @@ class RenderGeometryFn(torch.autograd.Function):
         gg = torch.zeros(res, device=mid.device)
         d_sdf = None if d_sdf is None else d_sdf.contiguous()
         d_nrm = None if d_nrm is None else d_nrm.contiguous()
-        call("vx_render_geometry_backward", ptr(g), i3(res), f3(ctx.bounds[0]), f3(ctx.bounds[1]), ptr(rays_o),
-             ptr(rays_d), ptr(mid), nr, ns, ptr(d_sdf), ptr(d_nrm), None, 3, None, ptr(gg), stream_ptr(mid.device))
+        geometry_backward(g, res, ctx.bounds, rays_o, rays_d, mid, d_sdf, d_nrm, gg)
         return gg.reshape(grid.shape), None, None, None, None, None, None, None
+
+
+# ------------------------------------------------------------------ deterministic mode ------
+
+_deterministic = False
+
+
+def set_deterministic(flag: bool) -> None:
+    """Route the geometry and hash-table adjoints through the sorted segmented reduction
+    (bitwise reproducible) instead of float atomics."""
+    global _deterministic
+    _deterministic = bool(flag)
+
+
+def is_deterministic() -> bool:
+    return _deterministic
+
+
+def _workspace(dev, nbytes: int) -> torch.Tensor:
+    sc = Scratch.get(dev)
+    ws = getattr(sc, "det_ws", None)
+    if ws is None or ws.numel() < nbytes:
+        sc.det_ws = ws = torch.empty(int(nbytes), dtype=torch.uint8, device=dev)
+    return ws
+
+
+def geometry_backward(g, res, bounds, rays_o, rays_d, mid, d_sdf, d_normal, out):
+    nr, ns = mid.shape
+    dev = mid.device
+    if _deterministic:
+        need = int(L.query("vx_geometry_backward_det_workspace", nr, ns, i3(res)))
+        if need == 0:
+            raise RuntimeError("batch too large for one deterministic geometry pass")
+        ws = _workspace(dev, need)
+        call("vx_render_geometry_backward_det", ptr(g), i3(res), f3(bounds[0]), f3(bounds[1]), ptr(rays_o),
+             ptr(rays_d), ptr(mid), nr, ns, ptr(d_sdf), ptr(d_normal), None, 3, ptr(out), ptr(ws), ws.numel(),
+             stream_ptr(dev))
+    else:
+        call("vx_render_geometry_backward", ptr(g), i3(res), f3(bounds[0]), f3(bounds[1]), ptr(rays_o), ptr(rays_d),
+             ptr(mid), nr, ns, ptr(d_sdf), ptr(d_normal), None, 3, None, ptr(out), stream_ptr(dev))
+
+
+def hash_backward(d_emb, cfg, active_levels, pts, rays_o, rays_d, mid, n_samples, xyz_min, xyz_max, n_points,
+                  d_out, ld):
+    dev = d_out.device
+    lw = cfg.level_weights(active_levels)
+    if _deterministic:
+        need = int(L.query("vx_hash_backward_det_workspace", n_points, cfg.n_levels, cfg.log2_size))
+        if need == 0:
+            raise RuntimeError("batch too large for one deterministic hash pass")
+        ws = _workspace(dev, need)
+        res_d = torch.tensor(cfg.resolutions, dtype=torch.int32, device=dev)
+        lw_d = torch.tensor(list(lw)[:cfg.n_levels], dtype=torch.float32, device=dev)
+        call("vx_hash_encode_backward_det", ptr(d_emb), cfg.n_levels, cfg.log2_size, cfg.n_features, ptr(res_d),
+             ptr(lw_d), ptr(pts), ptr(rays_o), ptr(rays_d), ptr(mid), n_samples,
+             f3(xyz_min) if xyz_min is not None else None, f3(xyz_max) if xyz_max is not None else None, n_points,
+             ptr(d_out), ld, ptr(ws), ws.numel(), stream_ptr(dev))
+    else:
+        call("vx_hash_encode_backward", ptr(d_emb), cfg.n_levels, cfg.log2_size, cfg.n_features, cfg._res_c, lw,
+             ptr(pts), ptr(rays_o), ptr(rays_d), ptr(mid), n_samples,
+             f3(xyz_min) if xyz_min is not None else None, f3(xyz_max) if xyz_max is not None else None, n_points,
+             ptr(d_out), ld, stream_ptr(dev))
 
 
 class HashConfig:
@@ -408,9 +469,8 @@ class AppearanceInputFn(torch.autograd.Function):
         d_emb = None
         if ctx.needs_input_grad[0]:
             d_emb = torch.zeros(eshape, device=g.device)
-            call("vx_hash_encode_backward", ptr(d_emb), cfg.n_levels, cfg.log2_size, cfg.n_features, cfg._res_c,
-                 cfg.level_weights(active_levels), None, ptr(rays_o), ptr(rays_d), ptr(mid), ns, f3(xyz_min),
-                 f3(xyz_max), nr * ns, ptr(g), g.shape[1], stream_ptr(g.device))
+            hash_backward(d_emb, cfg, active_levels, None, rays_o, rays_d, mid, ns, xyz_min, xyz_max, nr * ns, g,
+                          g.shape[1])
         d_n = None
         if ctx.needs_input_grad[1]:
             c0 = 2 * cfg.n_levels + 16
@@ -482,14 +542,16 @@ class AppearanceMLPFn(torch.autograd.Function):
         if width != 51:
             raise RuntimeError("the fused appearance path needs 16 hash levels x 2 features")
         ld = MLP_LD
-        rows = torch.empty(p, ld, device=mid.device)
+        need_rows = any(ctx.needs_input_grad[:6])
+        rows = torch.empty(p, ld, device=mid.device) if need_rows else None
         nrm = normals.detach().contiguous()
-        call("vx_appearance_forward", ptr(embeddings.detach()), cfg.n_levels, cfg.log2_size, cfg.n_features,
-             cfg._res_c, cfg.level_weights(active_levels), None, ptr(rays_o), ptr(rays_d), ptr(mid), ns, f3(xyz_min),
-             f3(xyz_max), p, ptr(rows), ld, 2 * cfg.n_levels, None, 0, 2 * cfg.n_levels + 16, ptr(nrm), width,
-             stream_ptr(mid.device))
-        rows = rows[:, :width]
-        colors = mlp_forward(rows, W0, b0, W1, b1)
+        colors = torch.empty(p, 3, device=mid.device)
+        call("vx_appearance_mlp_forward", ptr(embeddings.detach()), cfg.n_levels, cfg.log2_size, cfg.n_features,
+             cfg._res_c, cfg.level_weights(active_levels), ptr(rays_o), ptr(rays_d), ptr(mid), ns, f3(xyz_min),
+             f3(xyz_max), p, ptr(nrm), ptr(W0.detach()), ptr(b0.detach()), ptr(W1.detach()), ptr(b1.detach()),
+             ptr(colors), ptr(rows), ld, stream_ptr(mid.device))
+        if rows is not None:
+            rows = rows[:, :width]
         ctx.save_for_backward(rays_o, rays_d, mid, W0, b0, W1, b1)
         ctx.rows = rows
         ctx.meta = (xyz_min, xyz_max, cfg, active_levels, embeddings.shape, normals.shape)
@@ -506,9 +568,8 @@ class AppearanceMLPFn(torch.autograd.Function):
         d_emb = None
         if ctx.needs_input_grad[0]:
             d_emb = torch.zeros(eshape, device=g.device)
-            call("vx_hash_encode_backward", ptr(d_emb), cfg.n_levels, cfg.log2_size, cfg.n_features, cfg._res_c,
-                 cfg.level_weights(active_levels), None, ptr(rays_o), ptr(rays_d), ptr(mid), ns, f3(xyz_min),
-                 f3(xyz_max), nr * ns, ptr(d_hash), 32, stream_ptr(g.device))
+            hash_backward(d_emb, cfg, active_levels, None, rays_o, rays_d, mid, ns, xyz_min, xyz_max, nr * ns, d_hash,
+                          32)
         return (d_emb, d_normal.reshape(nshape), dW0, db0, dW1, db1, None, None, None, None, None, None, None)
 
 
@@ -535,9 +596,7 @@ class HashEncodeFn(torch.autograd.Function):
         if ctx.needs_input_grad[0]:
             gc = g.reshape(-1, 2 * cfg.n_levels).contiguous()
             d_emb = torch.zeros(eshape, device=g.device)
-            call("vx_hash_encode_backward", ptr(d_emb), cfg.n_levels, cfg.log2_size, cfg.n_features, cfg._res_c,
-                 cfg.level_weights(active_levels), ptr(x), None, None, None, 1, None, None, x.shape[0], ptr(gc),
-                 gc.shape[1], stream_ptr(g.device))
+            hash_backward(d_emb, cfg, active_levels, x, None, None, None, 1, None, None, x.shape[0], gc, gc.shape[1])
         return d_emb, None, None, None
 
 
@@ -702,12 +761,18 @@ def vr_mark_corners(corners: torch.Tensor, res, bitmap: torch.Tensor):
     return bitmap
 
 
-def vr_count(bitmap, grid, res, xyz_min, xyz_max, relax_radius=0.0, band=0.0, counts=None):
+def vr_count(bitmap, grid, res, xyz_min, xyz_max, relax_radius=0.0, band=0.0, counts=None, filtered=None):
+    """Counts [all, relax, band, relax&band]; `filtered` (2 x words int32) receives the regularizer's
+    input bitmaps (bits & band, bits & band & relax)."""
     if counts is None:
         counts = torch.zeros(4, dtype=torch.int64, device=bitmap.device)
     call("vx_vr_count", ptr(bitmap), ptr(grid), i3(res), f3(xyz_min), f3(xyz_max), float(relax_radius), float(band),
-         ptr(counts), stream_ptr(bitmap.device))
+         ptr(counts), ptr(filtered), stream_ptr(bitmap.device))
     return counts
+
+
+def new_filtered(res, device) -> torch.Tensor:
+    return torch.zeros(2 * bitmap_words(res), dtype=torch.int32, device=device)
 
 
 def final_count(counts: torch.Tensor, relax_radius: float, band: float) -> torch.Tensor:
@@ -748,9 +813,11 @@ def reg_list(kind: str, grid3, verts, eps, weight, grad_out):
     return losses
 
 
-def reg_stencil(grid, bitmap, res, xyz_min, xyz_max, relax_radius, band, counts, w_eik, w_curv, grad_out,
+def reg_stencil(grid, filtered, res, xyz_min, xyz_max, relax_radius, band, counts, w_eik, w_curv, grad_out,
                 losses=None):
+    """Fused eikonal + curvature into grad_out; `filtered` and `counts` come from vr_count."""
     dev = grid.device
+    bitmap = filtered
     sc = Scratch.get(dev)
     nblk = int(L.query("vx_reg_stencil_blocks", i3(res)))
     partials = sc.partials_for(3 * nblk)

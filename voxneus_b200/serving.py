@@ -79,7 +79,10 @@ class SceneStore:
     """Resident scenes keyed by name."""
 
     def __init__(self, device):
-        self.device = torch.device(device)
+        dev = torch.device(device)
+        if dev.type == "cuda" and dev.index is None:
+            dev = torch.device("cuda", torch.cuda.current_device())
+        self.device = dev
         self.scenes: Dict[str, VoxNeuS] = {}
 
     def add(self, name: str, model: VoxNeuS) -> None:
@@ -287,8 +290,8 @@ class ServingEngine:
         self._inflight = keep
 
     def _loop(self):
-        torch.cuda.set_device(self.device)
         try:
+            torch.cuda.set_device(self.device)
             while not self._stop.is_set():
                 self._admit()
                 self._poll()

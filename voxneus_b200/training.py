@@ -98,6 +98,7 @@ class FusedTrainer:
         # |f| < band * eps_x, threshold rounded to float32 like a float32 tensor comparison
         self.band = float(torch.tensor(band_voxels * eps[0], dtype=torch.float32)) if band_voxels else 0.0
         self.bitmap = ops.new_bitmap(self.res, dev)
+        self.filtered = ops.new_filtered(self.res, dev)
         self.counts = torch.zeros(4, dtype=torch.int64, device=dev)
         self.reg_losses = torch.zeros(2, device=dev)
         self.amp_flag = torch.zeros(1, dtype=torch.int32, device=dev)
@@ -129,8 +130,9 @@ class FusedTrainer:
                 self.amp_flag.copy_(amplify_after_reduce(m.variance_net.variance, amp_k).reshape(1).int())
         grid = m.sdf_grid.grid
         lo, hi = m.sdf_grid.bounds()
-        ops.vr_count(self.bitmap, grid.detach(), self.res, lo, hi, self.relax_radius, self.band, self.counts)
-        ops.reg_stencil(grid.detach(), self.bitmap, self.res, lo, hi, self.relax_radius, self.band, self.counts,
+        ops.vr_count(self.bitmap, grid.detach(), self.res, lo, hi, self.relax_radius, self.band, self.counts,
+                     self.filtered)
+        ops.reg_stencil(grid.detach(), self.filtered, self.res, lo, hi, self.relax_radius, self.band, self.counts,
                         self.w_eik, self.w_curv, grid.grad, self.reg_losses)
         if self.optimize:
             lr_factor = (math.cos(math.pi * step / max(self.total_steps, 1)) + 1.0) * 0.5 * (1.0 - 0.05) + 0.05
