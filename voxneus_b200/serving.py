@@ -43,7 +43,7 @@ class RequestError(RuntimeError):
     pass
 
 
-@dataclass
+@dataclass(eq=False)  # requests compare by identity (the engine removes them from lists)
 class Request:
     scene: str
     kind: str  # "render" or "query"
