@@ -145,6 +145,8 @@ def algorithmic_bytes(name, n_rays, n_samples, res, n_levels=16, ld=52, nnz=None
         "vx_sample_multistep": n_rays * (24 + 4 * N_SAMPLES + 4 * N_IMPORTANCE + 32 * q + occ + 8 * n_samples),
         "vx_render_geometry_forward": n_rays * 24 + P * (4 + 128 + 4 + 12 + 4),
         "vx_appearance_forward": n_rays * 24 + P * (4 + n_levels * 8 * 8 + 12 + 4 * ld),
+        # fused appearance + MLP: midpoint, hash gathers, normal in; colours and the adjoint's rows out
+        "vx_appearance_mlp_forward": n_rays * 24 + P * (4 + n_levels * 8 * 8 + 12 + 12 + 4 * ld),
         "vx_composite_forward": n_rays * (24 + 32) + P * 48,
         "vx_composite_backward": n_rays * (24 + 32) + P * 64,
         "vx_hash_encode_backward": n_rays * 24 + P * (4 + 4 * 2 * n_levels + n_levels * 8 * 16),
@@ -155,6 +157,26 @@ def algorithmic_bytes(name, n_rays, n_samples, res, n_levels=16, ld=52, nnz=None
     if nnz is not None:
         table["vx_masked_adam_upd"] = voxels * 4 + nnz * 24
     return table.get(name)
+
+
+# FP32 FLOPs per sample of the MLP kernels (51 -> 64 ReLU -> 3 Sigmoid; the 52nd input column is padding)
+MLP_FLOPS = {
+    # hidden layer 2*52*64 + colour layer 2*64*3
+    "vx_appearance_mlp_forward": 2 * 52 * 64 + 2 * 64 * 3,
+    # hidden + colour recompute, dL/dh 2*3*64, dW1 2*3*64, dW0 (+db0) 2*52*64, dX (35 columns) 2*64*35
+    "vx_radiance_mlp_backward": 2 * 52 * 64 + 2 * 64 * 3 + 2 * 3 * 64 * 2 + 2 * 52 * 64 + 2 * 64 * 35,
+}
+
+
+def fp32_simt(per_kernel, n_points, sm_max_mhz):
+    """FLOP rate of the MLP kernels against the SIMT FP32 peak (148 SMs x 128 lanes x 2 x clock)."""
+    peak = 148 * 128 * 2 * (sm_max_mhz or 1965.0) * 1e6 / 1e12
+    out = {"peak_tflops_nominal": peak}
+    for k, fl in MLP_FLOPS.items():
+        if k in per_kernel and per_kernel[k] > 0:
+            tf = n_points * fl / (per_kernel[k] / 1e3) / 1e12
+            out[k] = {"flops_per_sample": fl, "tflops": tf, "frac": tf / peak}
+    return out
 
 
 def load_traffic():
@@ -335,6 +357,7 @@ def run_fused(args):
                          "unit": "GB/s", "frac": achieved / peak, "traffic": traffic,
                          "algorithmic_bytes_per_launch": ab, "ms_per_launch": dom_ms},
             "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(per_kernel.items(), key=lambda x: -x[1])},
+            "fp32_simt": fp32_simt(per_kernel, args.rays * (N_SAMPLES + N_IMPORTANCE), clk.summary()["sm_max_mhz"]),
             "grid_upsample_128_to_256_ms": up_ms, "clocks": clk.summary(), "cpu_baseline": cb}
     print(json.dumps(line), flush=True)
     if world > 1:
@@ -424,6 +447,22 @@ def run_serving(args):
     t0 = time.perf_counter()
     eng = ServingEngine(store)
     capture_s = time.perf_counter() - t0
+    # device time of one replay of each scene-0 graph (the engine thread is idle until submissions)
+    graph_ms = {}
+    for (name, kind, size), gb in eng.graphs.items():
+        if name != "scene0":
+            continue
+        with torch.cuda.stream(eng.compute):
+            for _ in range(3):
+                gb.graph.replay()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(eng.compute)
+            for _ in range(10):
+                gb.graph.replay()
+            e1.record(eng.compute)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1) / 10
+        graph_ms[f"{kind}_{size}"] = {"ms": ms, ("rays_per_s" if kind == "render" else "points_per_s"): size / ms * 1e3}
     rng = random.Random(11)
     pool = synthetic.RayPool(seed=12)
     views = [pool.view(c) for c in range(0, 64, 4)]  # 16 full 800x600 views (480,000 rays each)
@@ -470,6 +509,8 @@ def run_serving(args):
                                    "query (2^16-2^22 points); Poisson 200 req/s",
                        "duration_s": duration, "requests": len(reqs), "buckets_render": eng.RENDER_BUCKETS,
                        "buckets_query": eng.QUERY_BUCKETS, "graph_capture_s": capture_s},
+            "graph_replay": graph_ms,
+            "offered": {"rays_per_s": sum(r.n for r in rend) / duration, "points_per_s": sum(r.n for r in qry) / duration},
             "query_points_per_s": sum(r.n for r in qry) / wall, "wall_s": wall,
             "latency_all": latency_stats(reqs), "latency_render": latency_stats(rend),
             "latency_query": latency_stats(qry), "clocks": clk.summary()}

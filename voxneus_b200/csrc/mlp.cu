@@ -16,9 +16,8 @@ constexpr int KP = 52;    // padded
 constexpr int NH = 64;    // hidden units
 constexpr int NO = 3;     // colours
 constexpr int TM = 128;   // samples per tile
-constexpr int DZS = 132;  // row stride of the transposed dL/dz tile (16-byte aligned rows)
-constexpr int XRS = 53;   // row stride of the row-major input tile
-constexpr int NDX = 35;   // input gradients produced: hash columns 0..31, normal columns 48..50
+constexpr int DZS = TM;   // row stride of the transposed dL/dz tile
+constexpr int XRS = KP;   // row stride of the row-major input tile (16-byte rows)
 constexpr int WG = NH * KP + NO * NH + NH + NO;  // per-block weight-gradient partial size
 
 struct MlpW {
@@ -60,19 +59,15 @@ __device__ __forceinline__ void layer0(const float (*XT)[TM], const float (*W0T)
   }
 }
 
-// Stage rows m0..m0+127 (row stride ldx) as XT[k][m] (and XR[m][k] when given).
+// Stage rows m0..m0+127 (row stride ldx) as XT[k][m].
 __device__ __forceinline__ void load_tile(const float* __restrict__ X, int64_t ldx, int64_t P, int64_t m0,
-                                          float (*XT)[TM], float (*XR)[XRS], int tid) {
+                                          float (*XT)[TM], int tid) {
   if (tid < TM) {
     const int64_t m = m0 + tid;
     const bool ok = m < P;
     const float* row = X + m * ldx;
 #pragma unroll 4
-    for (int k = 0; k < KP; ++k) {
-      const float v = (ok && k < KIN) ? __ldg(row + k) : 0.0f;
-      XT[k][tid] = v;
-      if (XR) XR[tid][k] = v;
-    }
+    for (int k = 0; k < KP; ++k) XT[k][tid] = (ok && k < KIN) ? __ldg(row + k) : 0.0f;
   }
 }
 
@@ -87,7 +82,7 @@ __global__ void __launch_bounds__(256) k_mlp_fwd(const float* __restrict__ X, in
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t m0 = t * TM;
     __syncthreads();
-    load_tile(X, ldx, P, m0, XT, nullptr, tid);
+    load_tile(X, ldx, P, m0, XT, tid);
     __syncthreads();
     float z[4][8];
     layer0(XT, W0T, B0, tm, tn, z);
@@ -237,46 +232,95 @@ __global__ void __launch_bounds__(256) k_appearance_mlp_fwd(HashArgs a, MlpW w, 
   }
 }
 
+// Stage rows m0..m0+127 of X as XR[m][0..51] with column 51 = 1 on real rows and whole rows of
+// zeros past P (the ones column turns the dW0 reduction's last column into db0; W0T's row 51 is
+// zero, so the column adds nothing to the hidden layer).
+__device__ __forceinline__ void load_rows(const float* __restrict__ X, int64_t ldx, int64_t P, int64_t m0,
+                                          float (*XR)[XRS], int tid, int nthreads) {
+  const int64_t nrows = P - m0 < TM ? P - m0 : TM;
+  if ((ldx & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0) {
+    for (int e = tid; e < TM * (KP / 4); e += nthreads) {
+      const int m = e / (KP / 4), c = e - (KP / 4) * m;
+      float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      if (m < nrows) {
+        v = __ldg(reinterpret_cast<const float4*>(X + (m0 + m) * ldx) + c);
+        if (c == KP / 4 - 1) v.w = 1.0f;
+      }
+      *reinterpret_cast<float4*>(&XR[m][4 * c]) = v;
+    }
+  } else {
+    for (int e = tid; e < TM * KP; e += nthreads) {
+      const int m = e / KP, k = e - KP * m;
+      XR[m][k] = m < nrows ? (k < KIN ? __ldg(X + (m0 + m) * ldx + k) : 1.0f) : 0.0f;
+    }
+  }
+}
+
 // Adjoint. d_out (P,3) -> d_hash (P,32), d_normal (P,3), per-block weight-gradient partials.
+// Thread (lane, warp) owns samples lane + 32 s (s = 0..3), so row-major 16-byte tile reads are
+// bank-conflict free (rows 208 bytes apart); dL/dz is staged as DZT[n][4 lane + s]. The weight
+// gradient runs on 4x4 micro-tiles (threads 0..207: units 4*(t/13).., columns 4*(t%13)..).
 __global__ void __launch_bounds__(256, 2) k_mlp_bwd(const float* __restrict__ X, int64_t ldx, int64_t P, MlpW w,
                                                  const float* __restrict__ d_out, float* __restrict__ d_hash,
                                                  float* __restrict__ d_normal, float* __restrict__ partials) {
   extern __shared__ __align__(16) float smem[];
-  float(*XT)[TM] = reinterpret_cast<float(*)[TM]>(smem);                  // KP x TM
-  float(*XR)[XRS] = reinterpret_cast<float(*)[XRS]>(smem + KP * TM);      // TM x XRS
-  float(*DZT)[DZS] = reinterpret_cast<float(*)[DZS]>(smem + KP * TM + TM * XRS);  // NH x DZS
-  float(*W0T)[NH] = reinterpret_cast<float(*)[NH]>(smem + KP * TM + TM * XRS + NH * DZS);
-  float* B0 = smem + KP * TM + TM * XRS + NH * DZS + KP * NH;
+  float(*XR)[XRS] = reinterpret_cast<float(*)[XRS]>(smem);                   // TM x XRS
+  float(*DZT)[DZS] = reinterpret_cast<float(*)[DZS]>(smem + TM * XRS);       // NH x DZS
+  float(*W0T)[NH] = reinterpret_cast<float(*)[NH]>(smem + TM * XRS + NH * DZS);
+  float* B0 = smem + TM * XRS + NH * DZS + KP * NH;
   float(*W1s)[NH] = reinterpret_cast<float(*)[NH]>(B0 + NH);
   float* B1 = B0 + NH + NO * NH;
   float(*DO)[NO] = reinterpret_cast<float(*)[NO]>(B1 + 4);
   const int tid = threadIdx.x, tm = tid & 31, tn = tid >> 5;
   load_weights(w, W0T, B0, W1s, B1, tid, blockDim.x);
-  // weight-gradient accumulators (across all tiles of this block)
-  float gW0[8][2];  // units 8*tn+j, input columns lane and lane+32
+  const bool wtile = tid < 16 * (KP / 4);
+  const int n4 = tid / (KP / 4), k4 = tid - (KP / 4) * n4;
+  float gW0[4][4];  // units 4*n4+j, columns 4*k4+i (column 51 accumulates db0)
 #pragma unroll
-  for (int j = 0; j < 8; ++j) gW0[j][0] = gW0[j][1] = 0.0f;
-  float gW1[NO][8], gB0[8], gB1[NO];
+  for (int j = 0; j < 4; ++j)
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    gB0[j] = 0.0f;
+    for (int i = 0; i < 4; ++i) gW0[j][i] = 0.0f;
+  float gW1[NO][8], gB1[NO];
+#pragma unroll
+  for (int j = 0; j < 8; ++j)
 #pragma unroll
     for (int c = 0; c < NO; ++c) gW1[c][j] = 0.0f;
-  }
 #pragma unroll
   for (int c = 0; c < NO; ++c) gB1[c] = 0.0f;
   const int64_t ntiles = (P + TM - 1) / TM;
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t m0 = t * TM;
     __syncthreads();
-    load_tile(X, ldx, P, m0, XT, XR, tid);
+    load_rows(X, ldx, P, m0, XR, tid, blockDim.x);
     if (tid < TM) {
 #pragma unroll
       for (int c = 0; c < NO; ++c) DO[tid][c] = (m0 + tid < P) ? d_out[(m0 + tid) * NO + c] : 0.0f;
     }
     __syncthreads();
+    // hidden pre-activations, k in the same order as the forward kernels (bit-identical z)
     float z[4][8];
-    layer0(XT, W0T, B0, tm, tn, z);
+#pragma unroll
+    for (int s = 0; s < 4; ++s)
+#pragma unroll
+      for (int j = 0; j < 8; ++j) z[s][j] = B0[8 * tn + j];
+#pragma unroll 1
+    for (int k = 0; k < KP; k += 4) {
+      float4 xa[4];
+#pragma unroll
+      for (int s = 0; s < 4; ++s) xa[s] = *reinterpret_cast<const float4*>(&XR[tm + 32 * s][k]);
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float4 w0 = *reinterpret_cast<const float4*>(&W0T[k + i][8 * tn]);
+        const float4 w1 = *reinterpret_cast<const float4*>(&W0T[k + i][8 * tn + 4]);
+        const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+          const float xv = i == 0 ? xa[s].x : (i == 1 ? xa[s].y : (i == 2 ? xa[s].z : xa[s].w));
+#pragma unroll
+          for (int j = 0; j < 8; ++j) z[s][j] = fmaf(xv, wv[j], z[s][j]);
+        }
+      }
+    }
     // recompute the colours for the sigmoid adjoint
     float* red = &DZT[0][0];
 #pragma unroll
@@ -286,7 +330,7 @@ __global__ void __launch_bounds__(256, 2) k_mlp_bwd(const float* __restrict__ X,
         float acc = 0.0f;
 #pragma unroll
         for (int j = 0; j < 8; ++j) acc = fmaf(W1s[c][8 * tn + j], fmaxf(z[s][j], 0.0f), acc);
-        red[(tn * TM + 4 * tm + s) * NO + c] = acc;
+        red[(tn * TM + tm + 32 * s) * NO + c] = acc;
       }
     __syncthreads();
     if (tid < TM) {
@@ -300,10 +344,10 @@ __global__ void __launch_bounds__(256, 2) k_mlp_bwd(const float* __restrict__ X,
       }
     }
     __syncthreads();
-    // dL/dh, ReLU adjoint, bias and layer-1 weight gradients; dL/dz staged transposed
+    // dL/dh, ReLU adjoint and layer-1 weight gradients; dL/dz staged as DZT[n][4 lane + s]
 #pragma unroll
     for (int s = 0; s < 4; ++s) {
-      const int m = 4 * tm + s;
+      const int m = tm + 32 * s;
       const float d0 = DO[m][0], d1 = DO[m][1], d2 = DO[m][2];
       if (tn == 0) {
         gB1[0] += d0;
@@ -318,66 +362,75 @@ __global__ void __launch_bounds__(256, 2) k_mlp_bwd(const float* __restrict__ X,
         gW1[1][j] = fmaf(d1, h, gW1[1][j]);
         gW1[2][j] = fmaf(d2, h, gW1[2][j]);
         const float dh = d0 * W1s[0][n] + d1 * W1s[1][n] + d2 * W1s[2][n];
-        const float dz = (h > 0.0f) ? dh : 0.0f;
-        gB0[j] += dz;
-        z[s][j] = dz;
+        z[s][j] = (h > 0.0f) ? dh : 0.0f;
       }
     }
 #pragma unroll
     for (int j = 0; j < 8; ++j)
       *reinterpret_cast<float4*>(&DZT[8 * tn + j][4 * tm]) = make_float4(z[0][j], z[1][j], z[2][j], z[3][j]);
     __syncthreads();
-    // dW0[n][k] += sum_m dz[m][n] x[m][k]: units 8*tn.., columns lane and lane+32
-    {
-      const int k0 = tm, k1 = tm + 32;
-      const bool has1 = k1 < KIN;
-#pragma unroll 4
-      for (int m = 0; m < TM; ++m) {
-        const float x0 = XR[m][k0];
-        const float x1 = has1 ? XR[m][k1] : 0.0f;
+    // dW0[n][k] += sum_m dz[m][n] x[m][k]; slot p of DZT holds sample (p >> 2) + 32 (p & 3)
+    if (wtile) {
+#pragma unroll 2
+      for (int p = 0; p < TM; p += 4) {
+        float4 d[4], x[4];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) {
-          const float dz = DZT[8 * tn + j][m];
-          gW0[j][0] = fmaf(dz, x0, gW0[j][0]);
-          gW0[j][1] = fmaf(dz, x1, gW0[j][1]);
+        for (int j = 0; j < 4; ++j) d[j] = *reinterpret_cast<const float4*>(&DZT[4 * n4 + j][p]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) x[q] = *reinterpret_cast<const float4*>(&XR[(p >> 2) + 32 * q][4 * k4]);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+          const float xv[4] = {x[q].x, x[q].y, x[q].z, x[q].w};
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const float dv = q == 0 ? d[j].x : (q == 1 ? d[j].y : (q == 2 ? d[j].z : d[j].w));
+#pragma unroll
+            for (int i = 0; i < 4; ++i) gW0[j][i] = fmaf(dv, xv[i], gW0[j][i]);
+          }
         }
       }
     }
-    // dX[m][k] = sum_n dz[m][n] W0[n][k] for the 35 needed columns: q = 5*tn + i
-    float dx[4][5];
-    int kc[5];
+    // dX[m][k] = sum_n dz[m][n] W0[n][k]: hash columns 4*warp..+3, normal column 48+warp (warps 0..2)
+    float dx[4][4], dn[4];
 #pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      const int q = 5 * tn + i;
-      kc[i] = q < 32 ? q : (q < NDX ? q + 16 : -1);
+    for (int s = 0; s < 4; ++s) {
+      dn[s] = 0.0f;
 #pragma unroll
-      for (int s = 0; s < 4; ++s) dx[s][i] = 0.0f;
+      for (int i = 0; i < 4; ++i) dx[s][i] = 0.0f;
     }
-#pragma unroll 4
-    for (int n = 0; n < NH; ++n) {
-      const float4 d = *reinterpret_cast<const float4*>(&DZT[n][4 * tm]);
+#pragma unroll 1
+    for (int n = 0; n < NH; n += 4) {
+      float4 wq[4];
 #pragma unroll
-      for (int i = 0; i < 5; ++i) {
-        const float wv = kc[i] >= 0 ? W0T[kc[i]][n] : 0.0f;
-        dx[0][i] = fmaf(d.x, wv, dx[0][i]);
-        dx[1][i] = fmaf(d.y, wv, dx[1][i]);
-        dx[2][i] = fmaf(d.z, wv, dx[2][i]);
-        dx[3][i] = fmaf(d.w, wv, dx[3][i]);
+      for (int i = 0; i < 4; ++i) wq[i] = *reinterpret_cast<const float4*>(&W0T[4 * tn + i][n]);
+      const float4 wn = tn < 3 ? *reinterpret_cast<const float4*>(&W0T[48 + tn][n]) : make_float4(0, 0, 0, 0);
+#pragma unroll
+      for (int jj = 0; jj < 4; ++jj) {
+        const float4 d = *reinterpret_cast<const float4*>(&DZT[n + jj][4 * tm]);
+        const float dv[4] = {d.x, d.y, d.z, d.w};
+        const float wnj = jj == 0 ? wn.x : (jj == 1 ? wn.y : (jj == 2 ? wn.z : wn.w));
+#pragma unroll
+        for (int s = 0; s < 4; ++s) {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            const float wv = jj == 0 ? wq[i].x : (jj == 1 ? wq[i].y : (jj == 2 ? wq[i].z : wq[i].w));
+            dx[s][i] = fmaf(dv[s], wv, dx[s][i]);
+          }
+          dn[s] = fmaf(dv[s], wnj, dn[s]);
+        }
       }
     }
     __syncthreads();  // XR reads (dW0) done: stage dX rows in XR
 #pragma unroll
-    for (int i = 0; i < 5; ++i) {
-      const int q = 5 * tn + i;
-      if (q < NDX) {
-#pragma unroll
-        for (int s = 0; s < 4; ++s) XR[4 * tm + s][q] = dx[s][i];
-      }
+    for (int s = 0; s < 4; ++s) {
+      *reinterpret_cast<float4*>(&XR[tm + 32 * s][4 * tn]) = make_float4(dx[s][0], dx[s][1], dx[s][2], dx[s][3]);
+      if (tn < 3) XR[tm + 32 * s][32 + tn] = dn[s];
     }
     __syncthreads();
-    for (int e = tid; e < TM * 32; e += blockDim.x) {
-      const int m = e >> 5, k = e & 31;
-      if (m0 + m < P) d_hash[(m0 + m) * 32 + k] = XR[m][k];
+    for (int e = tid; e < TM * 8; e += blockDim.x) {
+      const int m = e >> 3, c = e & 7;
+      if (m0 + m < P)
+        reinterpret_cast<float4*>(d_hash + (m0 + m) * 32)[c] = *reinterpret_cast<const float4*>(&XR[m][4 * c]);
     }
     for (int e = tid; e < TM * 3; e += blockDim.x) {
       const int m = e / 3, c = e % 3;
@@ -386,18 +439,19 @@ __global__ void __launch_bounds__(256, 2) k_mlp_bwd(const float* __restrict__ X,
   }
   // per-block weight-gradient partials: [dW0 (64 x 52) | dW1 (3 x 64) | db0 (64) | db1 (3)]
   float* pb = partials + (int64_t)blockIdx.x * WG;
+  if (wtile) {
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
-    const int n = 8 * tn + j;
-    pb[n * KP + tm] = gW0[j][0];
-    if (tm + 32 < KP) pb[n * KP + tm + 32] = gW0[j][1];
+    for (int j = 0; j < 4; ++j) {
+      const int n = 4 * n4 + j;
+#pragma unroll
+      for (int i = 0; i < 4; ++i) pb[n * KP + 4 * k4 + i] = gW0[j][i];
+      if (k4 == KP / 4 - 1) pb[NH * KP + NO * NH + n] = gW0[j][3];
+    }
   }
 #pragma unroll
-  for (int j = 0; j < 8; ++j) {
+  for (int j = 0; j < 8; ++j)
 #pragma unroll
     for (int c = 0; c < NO; ++c) gW1[c][j] = warp_sum(gW1[c][j]);
-    gB0[j] = warp_sum(gB0[j]);
-  }
 #pragma unroll
   for (int c = 0; c < NO; ++c) gB1[c] = warp_sum(gB1[c]);
   if (tm == 0) {
@@ -406,7 +460,6 @@ __global__ void __launch_bounds__(256, 2) k_mlp_bwd(const float* __restrict__ X,
       const int n = 8 * tn + j;
 #pragma unroll
       for (int c = 0; c < NO; ++c) pb[NH * KP + c * NH + n] = gW1[c][j];
-      pb[NH * KP + NO * NH + n] = gB0[j];
     }
     if (tn == 0) {
 #pragma unroll
@@ -436,7 +489,7 @@ __global__ void k_mlp_wgrad_reduce(const float* __restrict__ partials, int nbloc
 }
 
 constexpr size_t kBwdSmem =
-    sizeof(float) * (KP * TM + TM * XRS + NH * DZS + KP * NH + NH + NO * NH + 4 + TM * NO);
+    sizeof(float) * (TM * XRS + NH * DZS + KP * NH + NH + NO * NH + 4 + TM * NO);
 
 }  // namespace vx
 
@@ -507,6 +560,7 @@ int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int 
   VX_REQUIRE(n_points >= 0 && ldx >= KIN, "bad sizes");
   VX_REQUIRE(x && W0 && b0 && W1 && b1 && d_colors && d_hash && d_normal && dW0 && db0 && dW1 && db1 && partials,
              "null pointer");
+  VX_REQUIRE((reinterpret_cast<uintptr_t>(d_hash) & 15) == 0, "d_hash must be 16-byte aligned");
   const int nb = vx_mlp_blocks(n_points);
   VX_REQUIRE(n_partial_floats >= (int64_t)nb * WG, "partials buffer holds %lld floats, need %lld",
              (long long)n_partial_floats, (long long)nb * WG);

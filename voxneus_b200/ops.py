@@ -542,7 +542,8 @@ class AppearanceMLPFn(torch.autograd.Function):
         if width != 51:
             raise RuntimeError("the fused appearance path needs 16 hash levels x 2 features")
         ld = MLP_LD
-        need_rows = any(ctx.needs_input_grad[:6])
+        # needs_input_grad stays True under no_grad: inference (serving) must not write the rows
+        need_rows = torch.is_grad_enabled() and any(ctx.needs_input_grad[:6])
         rows = torch.empty(p, ld, device=mid.device) if need_rows else None
         nrm = normals.detach().contiguous()
         colors = torch.empty(p, 3, device=mid.device)
