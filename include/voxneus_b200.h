@@ -219,6 +219,12 @@ int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, i
 int vx_mlp_blocks(int64_t n_points);
 int vx_mlp_partial_floats(void);
 
+/* The three MLP kernels run on the tcgen05 tensor cores (kind::tf32, hi/lo split for FP32-level
+ * accuracy) and wait on the tensor core with bounded mbarrier polls. Returns how many blocks gave
+ * up on such a wait since the last call (their outputs are invalid) and resets the count; -1 on
+ * a CUDA error. Synchronises the device (diagnostic only). No counterpart in the reference. */
+int vx_tensor_core_timeouts(void);
+
 /* Adjoint of vx_radiance_mlp_forward (recomputes the hidden layer): d_colors (n,3) -> d_hash (n,32)
  * (gradient of input columns 0..31), d_normal (n,3) (columns 48..50), and the weight gradients
  * dW0, db0, dW1, db1 (written, not accumulated; summed over blocks in a fixed order).

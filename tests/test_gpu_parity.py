@@ -404,14 +404,28 @@ def test_hash_and_sh_golden(golden):
     assert_close(enc.encoder.embeddings.grad, emb.grad, GRAD_TOL, "hash grad")
 
 
-def test_fused_mlp_matches_oracle():
-    """51-64-3 MLP forward (1e-5) and adjoint (input and weight gradients, 1e-4) vs torch fp32 autograd."""
-    from voxneus_b200 import ops
+@pytest.mark.parametrize("p", [3000, 50000])
+def test_fused_mlp_matches_oracle(p):
+    """51-64-3 MLP forward (1e-5) and adjoint (input and weight gradients, 1e-4) vs torch fp32 autograd.
+
+    3000 rows: one partial tile per block; 50000 rows: blocks accumulate several tiles of the
+    weight gradient in tensor memory. Neither is a multiple of the 128-sample tile.
+
+    Rows with a hidden pre-activation within 1e-6 of the largest |z| of zero (FP64) sit on a ReLU
+    kink, where any two FP32 evaluation orders can disagree on the unit's sign (and move that
+    sample's input gradient and its share of dW0 by ~|dz x|); they are dropped from the inputs
+    (a handful: at most one in 2000) so every output is compared in full."""
+    from voxneus_b200 import _lib, ops
 
     torch.manual_seed(13)
-    p = 3000  # not a multiple of the 128-sample tile
     rows = torch.randn(p, 52)
     l0, l1 = torch.nn.Linear(51, 64), torch.nn.Linear(64, 3)
+    with torch.no_grad():
+        z64 = rows[:, :51].double() @ l0.weight.double().T + l0.bias.double()
+        smooth = (z64.abs() > 1e-6 * float(z64.abs().max())).all(dim=1)
+    assert int((~smooth).sum()) <= max(2, p // 2000), int((~smooth).sum())
+    rows = rows[smooth].contiguous()
+    p = rows.shape[0]
     x = rows[:, :51].clone().requires_grad_(True)
     ws = [t.detach().clone().requires_grad_(True) for t in (l0.weight, l0.bias, l1.weight, l1.bias)]
     ref = O.radiance_mlp(x[:, :32], x[:, 32:48], x[:, 48:51], *ws)
@@ -427,6 +441,7 @@ def test_fused_mlp_matches_oracle():
     assert_close(xd.grad[:, 48:51], x.grad[:, 48:51], GRAD_TOL, "d normal")
     for a, b, nm in zip(wd, ws, ("W0", "b0", "W1", "b1")):
         assert_close(a.grad, b.grad, GRAD_TOL, nm)
+    assert _lib.query("vx_tensor_core_timeouts") == 0
 
 
 def test_fused_appearance_render_matches_cublas_path(golden):

@@ -1,24 +1,42 @@
 // Radiance MLP [hash 32 | SH 16 | normal 3] -> 64 ReLU -> 3 Sigmoid (models/radiance_mlp.py:42-53,
-// 81-98) as two fused FP32 kernels: the forward writes only the colours; the adjoint recomputes
-// the hidden layer, writes dL/d(hash features) and dL/d(normal), and reduces the weight gradients
-// into per-block partials that a second kernel sums in a fixed order (deterministic).
+// 81-98) on the 5th-generation tensor cores (tcgen05, kind::tf32, accumulators in TMEM).
 //
-// Both kernels stage a 128-sample tile of input rows in shared memory and run the 51 -> 64 layer
-// as a register-tiled SIMT GEMM: thread (lane, warp) owns samples 4*lane..4*lane+3 and hidden
-// units 8*warp..8*warp+7, reading the inputs as 16-byte shared loads and the weights as
-// warp-broadcast loads. FP32 throughout (the parity bar of the colours is 1e-5 relative).
+// Accuracy: every product runs as a 3-term split x = hi + lo (hi, lo tf32), a*b ~ ah*bh + ah*bl +
+// al*bh, accumulated in f32 — about 21 bits per product, the FP32 parity bar (colours 1e-5, weight
+// gradients 1e-4 of their scale) holds where a single tf32 pass (11 bits) would not.
+//
+// Operands are K-major canonical no-swizzle layouts (tc.cuh; kind::tf32 with an MN-major operand
+// writes nothing on this part, so every operand is staged with its contraction dimension
+// contiguous). A 16-byte chunk holds 4 consecutive K elements of one row:
+//   X    (128 sample rows, K = features): chunk (m, 4f..4f+3) at (f*16 + m/8)*128 + (m%8)*16
+//   W0   (64 hidden rows,  K = features): element (n, k) at ((k/4)*8 + n/8)*128 + (n%8)*16 + (k%4)*4
+//   W0^T (64 feature rows, K = hidden), DZ (128 sample rows, K = hidden), and X^T / DZ^T (feature /
+//   hidden rows, K = the tile's samples) likewise.
+// GEMMs (M = 128 rows in TMEM lanes, N = 64 f32 columns):
+//   Z   = X W0^T         A = X,                  B = W0     (K = 56 features, 7 steps)
+//   dX  = DZ W0          A = DZ,                 B = W0^T   (K = 64 hidden, 8 steps)
+//   dW0 = [DZh;DZl]^T X  A = [DZ_hi^T; DZ_lo^T], B = X^T    (K = 128 samples, 16 steps)
+// The forward writes the colours (and, for the adjoint, the 52-float input rows); the adjoint
+// recomputes Z with the identical MMA sequence, writes dL/d(hash) and dL/d(normal), accumulates
+// dW0 (and db0 through a ones column) in TMEM across its tiles and dW1/db1 in registers, and
+// writes per-block partials that k_mlp_wgrad_reduce sums in block order (deterministic).
 #include "hashgrid.cuh"
+#include "tc.cuh"
 
 namespace vx {
 
-constexpr int KIN = 51;   // input features
-constexpr int KP = 52;    // padded
-constexpr int NH = 64;    // hidden units
-constexpr int NO = 3;     // colours
-constexpr int TM = 128;   // samples per tile
-constexpr int DZS = TM;   // row stride of the transposed dL/dz tile
-constexpr int XRS = KP;   // row stride of the row-major input tile (16-byte rows)
+constexpr int KIN = 51;  // input features
+constexpr int KP = 52;   // row width of the input rows (column 51 is padding)
+constexpr int NH = 64;   // hidden units
+constexpr int NO = 3;    // colours
+constexpr int TM = 128;  // samples per tile (TMEM lanes)
 constexpr int WG = NH * KP + NO * NH + NH + NO;  // per-block weight-gradient partial size
+constexpr uint32_t kWaitLimit = 1u << 22;       // mbarrier polls before a tile gives up
+
+constexpr uint32_t kXBytes = 16 * 16 * 128;  // one tf32 part of X (or DZ)
+constexpr uint32_t kWBytes = 16 * 8 * 128;   // one tf32 part of W0
+
+__device__ int g_tc_timeouts = 0;
 
 struct MlpW {
   const float* W0;  // (64, 51)
@@ -27,123 +45,136 @@ struct MlpW {
   const float* b1;  // (3)
 };
 
-__device__ __forceinline__ void load_weights(const MlpW& w, float (*W0T)[NH], float* B0, float (*W1s)[NH], float* B1,
-                                             int tid, int nthreads) {
-  for (int i = tid; i < KP * NH; i += nthreads) {
-    const int k = i / NH, n = i % NH;
-    W0T[k][n] = (k < KIN) ? w.W0[n * KIN + k] : 0.0f;
+__device__ __forceinline__ uint32_t x_off(int f, int m) { return (uint32_t)((f * 16 + (m >> 3)) * 128 + (m & 7) * 16); }
+__device__ __forceinline__ uint32_t w_off(int n, int k) {
+  return (uint32_t)(((k >> 2) * 8 + (n >> 3)) * 128 + (n & 7) * 16 + (k & 3) * 4);
+}
+
+__device__ __forceinline__ void st_split4(uint8_t* hi, uint8_t* lo, uint32_t off, float a, float b, float c, float d) {
+  float4 h, l;
+  tc::split_tf32(a, h.x, l.x);
+  tc::split_tf32(b, h.y, l.y);
+  tc::split_tf32(c, h.z, l.z);
+  tc::split_tf32(d, h.w, l.w);
+  *reinterpret_cast<float4*>(hi + off) = h;
+  *reinterpret_cast<float4*>(lo + off) = l;
+}
+
+// W0 as hi/lo tf32 (features 51..63 zero), b0, W1, b1; X feature chunks 13..15 (columns 52..63,
+// never written by the tiles) zeroed.
+__device__ void stage_weights(const MlpW& w, uint8_t* WH, uint8_t* WL, uint8_t* XH, uint8_t* XL, float* B0,
+                              float* W1s, float* B1, int tid, int nt) {
+  for (int e = tid; e < NH * 64; e += nt) {
+    const int n = e >> 6, k = e & 63;
+    float h, l;
+    tc::split_tf32(k < KIN ? w.W0[n * KIN + k] : 0.0f, h, l);
+    *reinterpret_cast<float*>(WH + w_off(n, k)) = h;
+    *reinterpret_cast<float*>(WL + w_off(n, k)) = l;
   }
-  for (int i = tid; i < NH; i += nthreads) B0[i] = w.b0[i];
-  for (int i = tid; i < NO * NH; i += nthreads) W1s[i / NH][i % NH] = w.W1[i];
+  for (int e = tid; e < 3 * TM; e += nt) {
+    const uint32_t off = x_off(13 + e / TM, e % TM);
+    *reinterpret_cast<float4*>(XH + off) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    *reinterpret_cast<float4*>(XL + off) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
+  for (int i = tid; i < NH; i += nt) B0[i] = w.b0[i];
+  for (int i = tid; i < NO * NH; i += nt) W1s[i] = w.W1[i];
   if (tid < NO) B1[tid] = w.b1[tid];
 }
 
-// hidden pre-activations z[s][j] for samples 4*tm+s, units 8*tn+j
-__device__ __forceinline__ void layer0(const float (*XT)[TM], const float (*W0T)[NH], const float* B0, int tm, int tn,
-                                       float z[4][8]) {
-#pragma unroll
-  for (int s = 0; s < 4; ++s)
-#pragma unroll
-    for (int j = 0; j < 8; ++j) z[s][j] = B0[8 * tn + j];
-#pragma unroll 4
-  for (int k = 0; k < KIN; ++k) {
-    const float4 a = *reinterpret_cast<const float4*>(&XT[k][4 * tm]);
-    const float4 w0 = *reinterpret_cast<const float4*>(&W0T[k][8 * tn]);
-    const float4 w1 = *reinterpret_cast<const float4*>(&W0T[k][8 * tn + 4]);
-    const float av[4] = {a.x, a.y, a.z, a.w};
-    const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) z[s][j] = fmaf(av[s], wv[j], z[s][j]);
+// Rows m0..m0+127 of X (row stride ldx) into the X buffers; thread (m, hh) takes the 16-byte
+// chunks 0..6 (hh = 0) or 7..12 (hh = 1). Column 51 becomes `one` on real rows; rows past P are 0.
+__device__ __forceinline__ void stage_rows(const float* __restrict__ X, int64_t ldx, bool vec, int64_t P, int64_t m0,
+                                           uint8_t* XH, uint8_t* XL, int m, int hh, float one) {
+  const bool ok = m0 + m < P;
+  const float* row = X + (m0 + m) * ldx;
+  const int c0 = hh ? 7 : 0, c1 = hh ? 13 : 7;
+  for (int c = c0; c < c1; ++c) {
+    float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (ok) {
+      if (vec) {
+        v = __ldg(reinterpret_cast<const float4*>(row) + c);
+      } else {
+        v.x = __ldg(row + 4 * c);
+        v.y = __ldg(row + 4 * c + 1);
+        v.z = __ldg(row + 4 * c + 2);
+        v.w = 4 * c + 3 < KIN ? __ldg(row + 4 * c + 3) : 0.0f;
+      }
+      if (c == 12) v.w = one;
+    }
+    st_split4(XH, XL, x_off(c, m), v.x, v.y, v.z, v.w);
   }
 }
 
-// Stage rows m0..m0+127 (row stride ldx) as XT[k][m].
-__device__ __forceinline__ void load_tile(const float* __restrict__ X, int64_t ldx, int64_t P, int64_t m0,
-                                          float (*XT)[TM], int tid) {
-  if (tid < TM) {
-    const int64_t m = m0 + tid;
-    const bool ok = m < P;
-    const float* row = X + m * ldx;
-#pragma unroll 4
-    for (int k = 0; k < KP; ++k) XT[k][tid] = (ok && k < KIN) ? __ldg(row + k) : 0.0f;
+// Z = X W0^T into TMEM columns [tz, tz + 64), issued by one thread (same sequence in both passes).
+__device__ __forceinline__ void issue_z(uint32_t tz, uint32_t xh, uint32_t xl, uint32_t wh, uint32_t wl) {
+  constexpr uint32_t id = tc::idesc_tf32(TM, NH, false, false);
+#pragma unroll 1
+  for (int ks = 0; ks < 7; ++ks) {
+    const uint64_t ah = tc::sdesc(xh + ks * 4096, 2048, 128), al = tc::sdesc(xl + ks * 4096, 2048, 128);
+    const uint64_t bh = tc::sdesc(wh + ks * 2048, 1024, 128), bl = tc::sdesc(wl + ks * 2048, 1024, 128);
+    tc::mma_tf32(tz, ah, bh, id, ks > 0);
+    tc::mma_tf32(tz, ah, bl, id, true);
+    tc::mma_tf32(tz, al, bh, id, true);
   }
 }
 
-__global__ void __launch_bounds__(256) k_mlp_fwd(const float* __restrict__ X, int64_t ldx, int64_t P, MlpW w,
-                                                 float* __restrict__ out) {
-  __shared__ __align__(16) float XT[KP][TM];
-  __shared__ __align__(16) float W0T[KP][NH];
-  __shared__ float B0[NH], W1s[NO][NH], B1[NO];
-  const int tid = threadIdx.x, tm = tid & 31, tn = tid >> 5;
-  load_weights(w, W0T, B0, W1s, B1, tid, blockDim.x);
+// This thread's half of the colour pre-activation: hidden units 32*hh..32*hh+31 of sample lane.
+__device__ __forceinline__ void colour_partial(const float z[32], int hh, const float* B0, const float* W1s,
+                                               float& p0, float& p1, float& p2) {
+  p0 = p1 = p2 = 0.0f;
+#pragma unroll
+  for (int j = 0; j < 32; ++j) {
+    const int n = 32 * hh + j;
+    const float h = fmaxf(z[j] + B0[n], 0.0f);
+    p0 = fmaf(W1s[n], h, p0);
+    p1 = fmaf(W1s[NH + n], h, p1);
+    p2 = fmaf(W1s[2 * NH + n], h, p2);
+  }
+}
+
+// Forward. kHashIn: the 51 features of a tile are built in place (two threads per sample, 8 hash
+// levels each; SH of the view direction; the normal); else they are read from rows X. kRowsOut
+// also writes the rows for the adjoint. 256 threads: warp w reads TMEM lanes 32*(w%4).. and
+// hidden columns 32*(w/4)..; the two column halves meet in shared memory.
+template <bool kHashIn, bool kRowsOut>
+__global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* __restrict__ X, int64_t ldx, int xvec,
+                                                       int64_t P, MlpW w, float* __restrict__ colors) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* XH = smem;
+  uint8_t* XL = XH + kXBytes;
+  uint8_t* WH = XL + kXBytes;
+  uint8_t* WL = WH + kWBytes;
+  float* B0 = reinterpret_cast<float*>(WL + kWBytes);
+  float* W1s = B0 + NH;
+  float* B1 = W1s + NO * NH;
+  float* RED = B1 + 4;  // [2][TM][4]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(RED + 2 * TM * 4);
+  uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31, q = wid & 3, hh = wid >> 2;
+  stage_weights(w, WH, WL, XH, XL, B0, W1s, B1, tid, blockDim.x);
+  if (tid == 0) tc::mbar_init(bar, 1);
+  if (wid == 0) tc::tmem_alloc(s_taddr, 64);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = *s_taddr;
+  const uint32_t xh = tc::smem_u32(XH), xl = tc::smem_u32(XL), wh = tc::smem_u32(WH), wl = tc::smem_u32(WL);
+  const uint32_t mask = (1u << a.log2T) - 1u;
+  const size_t T = (size_t)1 << a.log2T;
+  uint32_t phase = 0;
   const int64_t ntiles = (P + TM - 1) / TM;
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t m0 = t * TM;
-    __syncthreads();
-    load_tile(X, ldx, P, m0, XT, tid);
-    __syncthreads();
-    float z[4][8];
-    layer0(XT, W0T, B0, tm, tn, z);
-    float part[4][NO];
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-#pragma unroll
-      for (int c = 0; c < NO; ++c) {
-        float acc = 0.0f;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc = fmaf(W1s[c][8 * tn + j], fmaxf(z[s][j], 0.0f), acc);
-        part[s][c] = acc;
-      }
-    __syncthreads();  // XT reads done: reuse it for the layer-1 partial sums
-    float* red = &XT[0][0];
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-#pragma unroll
-      for (int c = 0; c < NO; ++c) red[(tn * TM + 4 * tm + s) * NO + c] = part[s][c];
-    __syncthreads();
-    if (tid < TM && m0 + tid < P) {
-#pragma unroll
-      for (int c = 0; c < NO; ++c) {
-        float o = B1[c];
-#pragma unroll
-        for (int g = 0; g < 8; ++g) o += red[(g * TM + tid) * NO + c];
-        out[(m0 + tid) * NO + c] = sigmoidf_ref(o);
-      }
-    }
-  }
-}
-
-// Appearance + MLP forward for (rays, midpoints): the 51 input features of a 128-sample tile
-// are built straight into the shared tile — two threads per sample, each gathering 8 hash
-// levels (float2 corner features); SH of the view direction and the normal complete the row
-// — then the MLP runs on the tile. kRows also writes the rows (the adjoint's input), as
-// 16-byte stores of each thread's columns.
-template <bool kRows>
-__global__ void __launch_bounds__(256) k_appearance_mlp_fwd(HashArgs a, MlpW w, float* __restrict__ colors) {
-  __shared__ __align__(16) float XT[KP][TM];
-  __shared__ __align__(16) float W0T[KP][NH];
-  __shared__ float B0[NH], W1s[NO][NH], B1[NO];
-  const int tid = threadIdx.x, tm = tid & 31, tn = tid >> 5;
-  load_weights(w, W0T, B0, W1s, B1, tid, blockDim.x);
-  const uint32_t mask = (1u << a.log2T) - 1u;
-  const size_t T = (size_t)1 << a.log2T;
-  const int64_t ntiles = (a.P + TM - 1) / TM;
-  for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
-    const int64_t m0 = t * TM;
-    __syncthreads();
-    {
+    if (kHashIn) {
       const int m = tid & (TM - 1), half = tid >> 7;
       const int64_t i = m0 + m;
-      float feat[16];
-      float extra[16];
-      if (i < a.P) {
+      float feat[16], extra[16];
+      if (i < P) {
         float x[3];
         sample_pos(a, i, x);
 #pragma unroll
-        for (int q = 0; q < 8; ++q) {
-          const int l = 8 * half + q;
+        for (int qq = 0; qq < 8; ++qq) {
+          const int l = 8 * half + qq;
           const float lw = a.lw[l];
           float f0 = 0.0f, f1 = 0.0f;
           if (lw != 0.0f) {
@@ -161,8 +192,8 @@ __global__ void __launch_bounds__(256) k_appearance_mlp_fwd(HashArgs a, MlpW w, 
               f1 *= lw;
             }
           }
-          feat[2 * q] = f0;
-          feat[2 * q + 1] = f1;
+          feat[2 * qq] = f0;
+          feat[2 * qq + 1] = f1;
         }
         if (half == 0) {
           const int64_t r = i / a.S;
@@ -175,298 +206,382 @@ __global__ void __launch_bounds__(256) k_appearance_mlp_fwd(HashArgs a, MlpW w, 
         }
       } else {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) feat[q] = extra[q] = 0.0f;
+        for (int qq = 0; qq < 16; ++qq) feat[qq] = extra[qq] = 0.0f;
       }
 #pragma unroll
-      for (int q = 0; q < 16; ++q) XT[16 * half + q][m] = feat[q];
+      for (int c = 0; c < 4; ++c)
+        st_split4(XH, XL, x_off(4 * half + c, m), feat[4 * c], feat[4 * c + 1], feat[4 * c + 2], feat[4 * c + 3]);
       if (half == 0) {
 #pragma unroll
-        for (int q = 0; q < 16; ++q) XT[32 + q][m] = extra[q];
+        for (int c = 0; c < 4; ++c)
+          st_split4(XH, XL, x_off(8 + c, m), extra[4 * c], extra[4 * c + 1], extra[4 * c + 2], extra[4 * c + 3]);
       } else {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) XT[48 + q][m] = extra[q];
+        st_split4(XH, XL, x_off(12, m), extra[0], extra[1], extra[2], extra[3]);
       }
-      if (kRows && i < a.P) {
+      if (kRowsOut && i < P) {
         float4* row = reinterpret_cast<float4*>(a.out + i * a.ld);
 #pragma unroll
-        for (int q = 0; q < 4; ++q)
-          row[4 * half + q] = make_float4(feat[4 * q], feat[4 * q + 1], feat[4 * q + 2], feat[4 * q + 3]);
+        for (int c = 0; c < 4; ++c)
+          row[4 * half + c] = make_float4(feat[4 * c], feat[4 * c + 1], feat[4 * c + 2], feat[4 * c + 3]);
         if (half == 0) {
 #pragma unroll
-          for (int q = 0; q < 4; ++q)
-            row[8 + q] = make_float4(extra[4 * q], extra[4 * q + 1], extra[4 * q + 2], extra[4 * q + 3]);
+          for (int c = 0; c < 4; ++c)
+            row[8 + c] = make_float4(extra[4 * c], extra[4 * c + 1], extra[4 * c + 2], extra[4 * c + 3]);
         } else {
           row[12] = make_float4(extra[0], extra[1], extra[2], extra[3]);
         }
       }
+    } else {
+      stage_rows(X, ldx, xvec != 0, P, m0, XH, XL, tid & (TM - 1), tid >> 7, 0.0f);
     }
+    tc::fence_smem_to_async();
     __syncthreads();
-    float z[4][8];
-    layer0(XT, W0T, B0, tm, tn, z);
-    float part[4][NO];
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
+    if (tid == 0) {
+      tc::fence_after_sync();
+      issue_z(tbase, xh, xl, wh, wl);
+      tc::commit(bar);
+    }
+    const bool ok = tc::mbar_wait(bar, phase, kWaitLimit);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {
+      if (tid == 0) atomicAdd(&g_tc_timeouts, 1);
+      break;
+    }
+    tc::fence_after_sync();
+    float z[32];
+    tc::tmem_ld32(tbase + ((uint32_t)(32 * q) << 16) + 32 * hh, z);
+    tc::tmem_wait_ld();
+    float p0, p1, p2;
+    colour_partial(z, hh, B0, W1s, p0, p1, p2);
+    float* r = RED + (hh * TM + 32 * q + lane) * 4;
+    r[0] = p0;
+    r[1] = p1;
+    r[2] = p2;
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid < TM && m0 + tid < P) {
 #pragma unroll
       for (int c = 0; c < NO; ++c) {
-        float acc = 0.0f;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc = fmaf(W1s[c][8 * tn + j], fmaxf(z[s][j], 0.0f), acc);
-        part[s][c] = acc;
-      }
-    __syncthreads();
-    float* red = &XT[0][0];
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-#pragma unroll
-      for (int c = 0; c < NO; ++c) red[(tn * TM + 4 * tm + s) * NO + c] = part[s][c];
-    __syncthreads();
-    if (tid < TM && m0 + tid < a.P) {
-#pragma unroll
-      for (int c = 0; c < NO; ++c) {
-        float o = B1[c];
-#pragma unroll
-        for (int g = 0; g < 8; ++g) o += red[(g * TM + tid) * NO + c];
+        const float o = (B1[c] + RED[tid * 4 + c]) + RED[(TM + tid) * 4 + c];
         colors[(m0 + tid) * NO + c] = sigmoidf_ref(o);
       }
     }
   }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (wid == 0) tc::tmem_dealloc(tbase, 64);
 }
 
-// Stage rows m0..m0+127 of X as XR[m][0..51] with column 51 = 1 on real rows and whole rows of
-// zeros past P (the ones column turns the dW0 reduction's last column into db0; W0T's row 51 is
-// zero, so the column adds nothing to the hidden layer).
-__device__ __forceinline__ void load_rows(const float* __restrict__ X, int64_t ldx, int64_t P, int64_t m0,
-                                          float (*XR)[XRS], int tid, int nthreads) {
-  const int64_t nrows = P - m0 < TM ? P - m0 : TM;
-  if ((ldx & 3) == 0 && (reinterpret_cast<uintptr_t>(X) & 15) == 0) {
-    for (int e = tid; e < TM * (KP / 4); e += nthreads) {
-      const int m = e / (KP / 4), c = e - (KP / 4) * m;
-      float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-      if (m < nrows) {
-        v = __ldg(reinterpret_cast<const float4*>(X + (m0 + m) * ldx) + c);
-        if (c == KP / 4 - 1) v.w = 1.0f;
-      }
-      *reinterpret_cast<float4*>(&XR[m][4 * c]) = v;
-    }
-  } else {
-    for (int e = tid; e < TM * KP; e += nthreads) {
-      const int m = e / KP, k = e - KP * m;
-      XR[m][k] = m < nrows ? (k < KIN ? __ldg(X + (m0 + m) * ldx + k) : 1.0f) : 0.0f;
-    }
+constexpr size_t kFwdSmem = 2 * kXBytes + 2 * kWBytes + sizeof(float) * (NH + NO * NH + 4 + 2 * TM * 4) + 16;
+
+// Adjoint. d_out (P,3) -> d_hash (P,32), d_normal (P,3), per-block weight-gradient partials
+// [dW0 (64 x 52) | dW1 (3 x 64) | db0 (64) | db1 (3)]. tcgen05 kind::tf32 takes K-major operands
+// only here, so the sample contraction of dW0 reads transposed copies: X^T (written as the rows
+// are staged) and DZ^T, whose scalar stores are bank-conflict free because their 16-byte K chunks
+// of 4 samples sit 1040 / 2064 bytes apart (one 16-byte pad per chunk slab).
+// Per tile: stage rows -> Z MMA -> epilogue (colours, dO, dW1 in registers, DZ) -> dX MMA ->
+// DZ^T -> dW0 MMA (overlapping the dX readout). TMEM columns: Z [0,64), dX [64,128),
+// dW0 = [DZ_hi | DZ_lo]^T X_hi in [128,192) and x X_lo in [192,256).
+constexpr uint32_t kXtSlab = 8 * 128 + 16;    // X^T: 4 samples x 64 feature rows
+constexpr uint32_t kDztSlab = 16 * 128 + 16;  // DZ^T: 4 samples x 128 rows (hidden hi | hidden lo)
+constexpr uint32_t kXtBytes = 32 * kXtSlab;
+constexpr uint32_t kR1Bytes = 66560;          // X (hi, lo) -> DZ (hi, lo) -> DZ^T, one at a time
+
+__device__ __forceinline__ uint32_t xt_off(int f, int m) {
+  return (uint32_t)((m >> 2) * kXtSlab + (f >> 3) * 128 + (f & 7) * 16 + (m & 3) * 4);
+}
+__device__ __forceinline__ uint32_t dzt_off(int r, int m) {
+  return (uint32_t)((m >> 2) * kDztSlab + (r >> 3) * 128 + (r & 7) * 16 + (m & 3) * 4);
+}
+// W0^T (feature rows f, hidden K): element (f, n) at (n/4)*1024 + (f/8)*128 + (f%8)*16 + (n%4)*4
+__device__ __forceinline__ uint32_t wt_off(int f, int n) {
+  return (uint32_t)((n >> 2) * 1024 + (f >> 3) * 128 + (f & 7) * 16 + (n & 3) * 4);
+}
+
+__global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__ X, int64_t ldx, int xvec, int64_t P,
+                                                      MlpW w, const float* __restrict__ d_out,
+                                                      float* __restrict__ d_hash, float* __restrict__ d_normal,
+                                                      float* __restrict__ partials) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* WH = smem;
+  uint8_t* WL = WH + kWBytes;
+  uint8_t* WTH = WL + kWBytes;
+  uint8_t* WTL = WTH + kWBytes;
+  uint8_t* XTH = WTL + kWBytes;
+  uint8_t* XTL = XTH + kXtBytes;
+  uint8_t* R1 = XTL + kXtBytes;
+  float* RED = reinterpret_cast<float*>(R1 + kR1Bytes);  // [2][TM][4]
+  float* W1s = RED + 2 * TM * 4;
+  float* B0 = W1s + NO * NH;
+  float* B1 = B0 + NH;
+  uint64_t* bar = reinterpret_cast<uint64_t*>(B1 + 4);
+  uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bar + 1);
+  const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31, q = wid & 3, hh = wid >> 2;
+  const int m = 32 * q + lane;  // this thread's sample in the tile (its TMEM lane)
+  // W0 (hidden rows) for Z, W0^T (feature rows) for dX, b0, W1, b1; X^T rows 52..63 zero
+  for (int e = tid; e < NH * 64; e += blockDim.x) {
+    const int n = e >> 6, k = e & 63;
+    float h, l;
+    tc::split_tf32(k < KIN ? w.W0[n * KIN + k] : 0.0f, h, l);
+    *reinterpret_cast<float*>(WH + w_off(n, k)) = h;
+    *reinterpret_cast<float*>(WL + w_off(n, k)) = l;
+    *reinterpret_cast<float*>(WTH + wt_off(k, n)) = h;
+    *reinterpret_cast<float*>(WTL + wt_off(k, n)) = l;
   }
-}
-
-// Adjoint. d_out (P,3) -> d_hash (P,32), d_normal (P,3), per-block weight-gradient partials.
-// Thread (lane, warp) owns samples lane + 32 s (s = 0..3), so row-major 16-byte tile reads are
-// bank-conflict free (rows 208 bytes apart); dL/dz is staged as DZT[n][4 lane + s]. The weight
-// gradient runs on 4x4 micro-tiles (threads 0..207: units 4*(t/13).., columns 4*(t%13)..).
-__global__ void __launch_bounds__(256, 2) k_mlp_bwd(const float* __restrict__ X, int64_t ldx, int64_t P, MlpW w,
-                                                 const float* __restrict__ d_out, float* __restrict__ d_hash,
-                                                 float* __restrict__ d_normal, float* __restrict__ partials) {
-  extern __shared__ __align__(16) float smem[];
-  float(*XR)[XRS] = reinterpret_cast<float(*)[XRS]>(smem);                   // TM x XRS
-  float(*DZT)[DZS] = reinterpret_cast<float(*)[DZS]>(smem + TM * XRS);       // NH x DZS
-  float(*W0T)[NH] = reinterpret_cast<float(*)[NH]>(smem + TM * XRS + NH * DZS);
-  float* B0 = smem + TM * XRS + NH * DZS + KP * NH;
-  float(*W1s)[NH] = reinterpret_cast<float(*)[NH]>(B0 + NH);
-  float* B1 = B0 + NH + NO * NH;
-  float(*DO)[NO] = reinterpret_cast<float(*)[NO]>(B1 + 4);
-  const int tid = threadIdx.x, tm = tid & 31, tn = tid >> 5;
-  load_weights(w, W0T, B0, W1s, B1, tid, blockDim.x);
-  const bool wtile = tid < 16 * (KP / 4);
-  const int n4 = tid / (KP / 4), k4 = tid - (KP / 4) * n4;
-  float gW0[4][4];  // units 4*n4+j, columns 4*k4+i (column 51 accumulates db0)
+  for (int e = tid; e < 12 * TM; e += blockDim.x) {
+    const uint32_t off = xt_off(52 + e / TM, e % TM);
+    *reinterpret_cast<float*>(XTH + off) = 0.0f;
+    *reinterpret_cast<float*>(XTL + off) = 0.0f;
+  }
+  for (int i = tid; i < NH; i += blockDim.x) B0[i] = w.b0[i];
+  for (int i = tid; i < NO * NH; i += blockDim.x) W1s[i] = w.W1[i];
+  if (tid < NO) B1[tid] = w.b1[tid];
+  if (tid == 0) tc::mbar_init(bar, 1);
+  if (wid == 0) tc::tmem_alloc(s_taddr, 256);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tbase = *s_taddr;
+  const uint32_t lane_base = (uint32_t)(32 * q) << 16;
+  const uint32_t wh = tc::smem_u32(WH), wl = tc::smem_u32(WL), wth = tc::smem_u32(WTH), wtl = tc::smem_u32(WTL);
+  const uint32_t xth = tc::smem_u32(XTH), xtl = tc::smem_u32(XTL), r1 = tc::smem_u32(R1);
+  constexpr uint32_t idN = tc::idesc_tf32(TM, 64, false, false);
+  float g1[NO][32];  // dW1 of hidden units 32*hh+j, summed over this thread's samples
 #pragma unroll
-  for (int j = 0; j < 4; ++j)
-#pragma unroll
-    for (int i = 0; i < 4; ++i) gW0[j][i] = 0.0f;
-  float gW1[NO][8], gB1[NO];
-#pragma unroll
-  for (int j = 0; j < 8; ++j)
-#pragma unroll
-    for (int c = 0; c < NO; ++c) gW1[c][j] = 0.0f;
-#pragma unroll
-  for (int c = 0; c < NO; ++c) gB1[c] = 0.0f;
+  for (int j = 0; j < 32; ++j) g1[0][j] = g1[1][j] = g1[2][j] = 0.0f;
+  float sb[NO] = {0.0f, 0.0f, 0.0f};
+  bool first_w = true, failed = false;
+  uint32_t phase = 0;
   const int64_t ntiles = (P + TM - 1) / TM;
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t m0 = t * TM;
-    __syncthreads();
-    load_rows(X, ldx, P, m0, XR, tid, blockDim.x);
-    if (tid < TM) {
+    const bool valid = m0 + m < P;
+    // rows -> X (sample rows, R1) and X^T (feature rows); column 51 = 1 on real rows (db0)
+    {
+      const float* row = X + (m0 + m) * ldx;
+      const int c0 = hh ? 7 : 0, c1 = hh ? 13 : 7;
+      for (int c = c0; c < c1; ++c) {
+        float v[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+        if (valid) {
+          if (xvec) {
+            const float4 u = __ldg(reinterpret_cast<const float4*>(row) + c);
+            v[0] = u.x;
+            v[1] = u.y;
+            v[2] = u.z;
+            v[3] = u.w;
+          } else {
 #pragma unroll
-      for (int c = 0; c < NO; ++c) DO[tid][c] = (m0 + tid < P) ? d_out[(m0 + tid) * NO + c] : 0.0f;
-    }
-    __syncthreads();
-    // hidden pre-activations, k in the same order as the forward kernels (bit-identical z)
-    float z[4][8];
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-#pragma unroll
-      for (int j = 0; j < 8; ++j) z[s][j] = B0[8 * tn + j];
-#pragma unroll 1
-    for (int k = 0; k < KP; k += 4) {
-      float4 xa[4];
-#pragma unroll
-      for (int s = 0; s < 4; ++s) xa[s] = *reinterpret_cast<const float4*>(&XR[tm + 32 * s][k]);
-#pragma unroll
-      for (int i = 0; i < 4; ++i) {
-        const float4 w0 = *reinterpret_cast<const float4*>(&W0T[k + i][8 * tn]);
-        const float4 w1 = *reinterpret_cast<const float4*>(&W0T[k + i][8 * tn + 4]);
-        const float wv[8] = {w0.x, w0.y, w0.z, w0.w, w1.x, w1.y, w1.z, w1.w};
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-          const float xv = i == 0 ? xa[s].x : (i == 1 ? xa[s].y : (i == 2 ? xa[s].z : xa[s].w));
-#pragma unroll
-          for (int j = 0; j < 8; ++j) z[s][j] = fmaf(xv, wv[j], z[s][j]);
-        }
-      }
-    }
-    // recompute the colours for the sigmoid adjoint
-    float* red = &DZT[0][0];
-#pragma unroll
-    for (int s = 0; s < 4; ++s)
-#pragma unroll
-      for (int c = 0; c < NO; ++c) {
-        float acc = 0.0f;
-#pragma unroll
-        for (int j = 0; j < 8; ++j) acc = fmaf(W1s[c][8 * tn + j], fmaxf(z[s][j], 0.0f), acc);
-        red[(tn * TM + tm + 32 * s) * NO + c] = acc;
-      }
-    __syncthreads();
-    if (tid < TM) {
-#pragma unroll
-      for (int c = 0; c < NO; ++c) {
-        float o = B1[c];
-#pragma unroll
-        for (int g = 0; g < 8; ++g) o += red[(g * TM + tid) * NO + c];
-        const float y = sigmoidf_ref(o);
-        DO[tid][c] = DO[tid][c] * ((1.0f - y) * y);  // dL/d(pre-sigmoid)
-      }
-    }
-    __syncthreads();
-    // dL/dh, ReLU adjoint and layer-1 weight gradients; dL/dz staged as DZT[n][4 lane + s]
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      const int m = tm + 32 * s;
-      const float d0 = DO[m][0], d1 = DO[m][1], d2 = DO[m][2];
-      if (tn == 0) {
-        gB1[0] += d0;
-        gB1[1] += d1;
-        gB1[2] += d2;
-      }
-#pragma unroll
-      for (int j = 0; j < 8; ++j) {
-        const int n = 8 * tn + j;
-        const float h = fmaxf(z[s][j], 0.0f);
-        gW1[0][j] = fmaf(d0, h, gW1[0][j]);
-        gW1[1][j] = fmaf(d1, h, gW1[1][j]);
-        gW1[2][j] = fmaf(d2, h, gW1[2][j]);
-        const float dh = d0 * W1s[0][n] + d1 * W1s[1][n] + d2 * W1s[2][n];
-        z[s][j] = (h > 0.0f) ? dh : 0.0f;
-      }
-    }
-#pragma unroll
-    for (int j = 0; j < 8; ++j)
-      *reinterpret_cast<float4*>(&DZT[8 * tn + j][4 * tm]) = make_float4(z[0][j], z[1][j], z[2][j], z[3][j]);
-    __syncthreads();
-    // dW0[n][k] += sum_m dz[m][n] x[m][k]; slot p of DZT holds sample (p >> 2) + 32 (p & 3)
-    if (wtile) {
-#pragma unroll 2
-      for (int p = 0; p < TM; p += 4) {
-        float4 d[4], x[4];
-#pragma unroll
-        for (int j = 0; j < 4; ++j) d[j] = *reinterpret_cast<const float4*>(&DZT[4 * n4 + j][p]);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) x[q] = *reinterpret_cast<const float4*>(&XR[(p >> 2) + 32 * q][4 * k4]);
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-          const float xv[4] = {x[q].x, x[q].y, x[q].z, x[q].w};
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const float dv = q == 0 ? d[j].x : (q == 1 ? d[j].y : (q == 2 ? d[j].z : d[j].w));
-#pragma unroll
-            for (int i = 0; i < 4; ++i) gW0[j][i] = fmaf(dv, xv[i], gW0[j][i]);
+            for (int i = 0; i < 4; ++i) v[i] = 4 * c + i < KIN ? __ldg(row + 4 * c + i) : 0.0f;
           }
+          if (c == 12) v[3] = 1.0f;
         }
+        float hi[4], lo[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          tc::split_tf32(v[i], hi[i], lo[i]);
+          *reinterpret_cast<float*>(XTH + xt_off(4 * c + i, m)) = hi[i];
+          *reinterpret_cast<float*>(XTL + xt_off(4 * c + i, m)) = lo[i];
+        }
+        *reinterpret_cast<float4*>(R1 + x_off(c, m)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+        *reinterpret_cast<float4*>(R1 + kXBytes + x_off(c, m)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+      }
+      if (hh) {  // feature chunk 13 (columns 52..55) is inside the Z contraction: zero it
+        *reinterpret_cast<float4*>(R1 + x_off(13, m)) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        *reinterpret_cast<float4*>(R1 + kXBytes + x_off(13, m)) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       }
     }
-    // dX[m][k] = sum_n dz[m][n] W0[n][k]: hash columns 4*warp..+3, normal column 48+warp (warps 0..2)
-    float dx[4][4], dn[4];
+    float dy[NO];
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      dn[s] = 0.0f;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) dx[s][i] = 0.0f;
+    for (int c = 0; c < NO; ++c) dy[c] = valid ? d_out[(m0 + m) * NO + c] : 0.0f;
+    tc::fence_smem_to_async();
+    __syncthreads();
+    if (tid == 0) {
+      tc::fence_after_sync();
+      issue_z(tbase, r1, r1 + kXBytes, wh, wl);
+      tc::commit(bar);
     }
-#pragma unroll 1
-    for (int n = 0; n < NH; n += 4) {
-      float4 wq[4];
-#pragma unroll
-      for (int i = 0; i < 4; ++i) wq[i] = *reinterpret_cast<const float4*>(&W0T[4 * tn + i][n]);
-      const float4 wn = tn < 3 ? *reinterpret_cast<const float4*>(&W0T[48 + tn][n]) : make_float4(0, 0, 0, 0);
-#pragma unroll
-      for (int jj = 0; jj < 4; ++jj) {
-        const float4 d = *reinterpret_cast<const float4*>(&DZT[n + jj][4 * tm]);
-        const float dv[4] = {d.x, d.y, d.z, d.w};
-        const float wnj = jj == 0 ? wn.x : (jj == 1 ? wn.y : (jj == 2 ? wn.z : wn.w));
-#pragma unroll
-        for (int s = 0; s < 4; ++s) {
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const float wv = jj == 0 ? wq[i].x : (jj == 1 ? wq[i].y : (jj == 2 ? wq[i].z : wq[i].w));
-            dx[s][i] = fmaf(dv[s], wv, dx[s][i]);
-          }
-          dn[s] = fmaf(dv[s], wnj, dn[s]);
-        }
-      }
+    bool ok = tc::mbar_wait(bar, phase, kWaitLimit);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
     }
-    __syncthreads();  // XR reads (dW0) done: stage dX rows in XR
-#pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      *reinterpret_cast<float4*>(&XR[tm + 32 * s][4 * tn]) = make_float4(dx[s][0], dx[s][1], dx[s][2], dx[s][3]);
-      if (tn < 3) XR[tm + 32 * s][32 + tn] = dn[s];
+    tc::fence_after_sync();
+    float z[32];
+    tc::tmem_ld32(tbase + lane_base + 32 * hh, z);
+    tc::tmem_wait_ld();
+    {
+      float p0, p1, p2;
+      colour_partial(z, hh, B0, W1s, p0, p1, p2);
+      float* r = RED + (hh * TM + m) * 4;
+      r[0] = p0;
+      r[1] = p1;
+      r[2] = p2;
     }
     __syncthreads();
-    for (int e = tid; e < TM * 8; e += blockDim.x) {
-      const int m = e >> 3, c = e & 7;
-      if (m0 + m < P)
-        reinterpret_cast<float4*>(d_hash + (m0 + m) * 32)[c] = *reinterpret_cast<const float4*>(&XR[m][4 * c]);
+    float d[NO];
+#pragma unroll
+    for (int c = 0; c < NO; ++c) {
+      const float o = (B1[c] + RED[m * 4 + c]) + RED[(TM + m) * 4 + c];
+      const float y = sigmoidf_ref(o);
+      d[c] = dy[c] * ((1.0f - y) * y);  // dL/d(pre-sigmoid); 0 on rows past P
     }
-    for (int e = tid; e < TM * 3; e += blockDim.x) {
-      const int m = e / 3, c = e % 3;
-      if (m0 + m < P) d_normal[(m0 + m) * 3 + c] = XR[m][32 + c];
+    if (hh == 0) {
+#pragma unroll
+      for (int c = 0; c < NO; ++c) sb[c] += d[c];
     }
+    // dW1 (registers), dL/dz (kept in z), DZ (sample rows) into R1: the Z MMA has read X
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const int n = 32 * hh + j;
+      const float zz = z[j] + B0[n];
+      const float h = fmaxf(zz, 0.0f);
+#pragma unroll
+      for (int c = 0; c < NO; ++c) g1[c][j] = fmaf(d[c], h, g1[c][j]);
+      const float dhid = d[0] * W1s[n] + d[1] * W1s[NH + n] + d[2] * W1s[2 * NH + n];
+      z[j] = zz > 0.0f ? dhid : 0.0f;
+    }
+#pragma unroll
+    for (int j4 = 0; j4 < 8; ++j4)
+      st_split4(R1, R1 + kXBytes, x_off(8 * hh + j4, m), z[4 * j4], z[4 * j4 + 1], z[4 * j4 + 2], z[4 * j4 + 3]);
+    tc::fence_smem_to_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {  // dX = DZ W0 (B = W0^T, feature rows)
+      tc::fence_after_sync();
+#pragma unroll 1
+      for (int ks = 0; ks < 8; ++ks) {
+        const uint64_t ah = tc::sdesc(r1 + ks * 4096, 2048, 128), al = tc::sdesc(r1 + kXBytes + ks * 4096, 2048, 128);
+        const uint64_t bh = tc::sdesc(wth + ks * 2048, 1024, 128), bl = tc::sdesc(wtl + ks * 2048, 1024, 128);
+        tc::mma_tf32(tbase + 64, ah, bh, idN, ks > 0);
+        tc::mma_tf32(tbase + 64, ah, bl, idN, true);
+        tc::mma_tf32(tbase + 64, al, bh, idN, true);
+      }
+      tc::commit(bar);
+    }
+    ok = tc::mbar_wait(bar, phase, kWaitLimit);
+    phase ^= 1u;
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    tc::fence_after_sync();
+    // DZ^T into R1 (the dX MMA has read DZ): rows 0..63 hi, 64..127 lo
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const int n = 32 * hh + j;
+      float h, l;
+      tc::split_tf32(z[j], h, l);
+      *reinterpret_cast<float*>(R1 + dzt_off(n, m)) = h;
+      *reinterpret_cast<float*>(R1 + dzt_off(NH + n, m)) = l;
+    }
+    tc::fence_smem_to_async();
+    tc::fence_before_sync();
+    __syncthreads();
+    if (tid == 0) {  // dW0 (+db0) += [DZ_hi | DZ_lo]^T X, K = the tile's samples
+      tc::fence_after_sync();
+#pragma unroll 1
+      for (int s = 0; s < 16; ++s) {
+        const uint64_t ad = tc::sdesc(r1 + s * 2 * kDztSlab, kDztSlab, 128);
+        const uint64_t bh = tc::sdesc(xth + s * 2 * kXtSlab, kXtSlab, 128);
+        const uint64_t bl = tc::sdesc(xtl + s * 2 * kXtSlab, kXtSlab, 128);
+        tc::mma_tf32(tbase + 128, ad, bh, idN, !first_w);
+        tc::mma_tf32(tbase + 192, ad, bl, idN, !first_w);
+        first_w = false;
+      }
+      tc::commit(bar);
+    }
+    // dX readout while the dW0 MMAs run
+    if (hh == 0) {
+      float v[32];
+      tc::tmem_ld32(tbase + lane_base + 64, v);
+      tc::tmem_wait_ld();
+      if (valid) {
+        float4* o = reinterpret_cast<float4*>(d_hash + (m0 + m) * 32);
+#pragma unroll
+        for (int c = 0; c < 8; ++c) o[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
+      }
+    } else {
+      float v[4];
+      tc::tmem_ld4(tbase + lane_base + 64 + 48, v);
+      tc::tmem_wait_ld();
+      if (valid) {
+        d_normal[(m0 + m) * 3] = v[0];
+        d_normal[(m0 + m) * 3 + 1] = v[1];
+        d_normal[(m0 + m) * 3 + 2] = v[2];
+      }
+    }
+    ok = tc::mbar_wait(bar, phase, kWaitLimit);  // R1 and X^T are rewritten by the next tile
+    phase ^= 1u;
+    tc::fence_before_sync();
+    if (__syncthreads_or(!ok)) {
+      failed = true;
+      break;
+    }
+    tc::fence_after_sync();
   }
-  // per-block weight-gradient partials: [dW0 (64 x 52) | dW1 (3 x 64) | db0 (64) | db1 (3)]
+  if (failed && tid == 0) atomicAdd(&g_tc_timeouts, 1);
+  // weight-gradient partials of this block
+  const bool have = blockIdx.x < ntiles && !failed;  // every block with a tile issued the dW0 MMAs
   float* pb = partials + (int64_t)blockIdx.x * WG;
-  if (wtile) {
+  float* R2 = reinterpret_cast<float*>(R1);           // [64][64]: dW0 rows of DZ_lo x X_hi
+  float* RW1 = R2 + 64 * 64;                          // [4 q][2 hh][3][32] dW1, then [4][3] db1
+  __syncthreads();
+  if (q >= 2) {
+    float v[32];
+    tc::tmem_ld32(tbase + lane_base + 128 + 32 * hh, v);
+    tc::tmem_wait_ld();
 #pragma unroll
-    for (int j = 0; j < 4; ++j) {
-      const int n = 4 * n4 + j;
-#pragma unroll
-      for (int i = 0; i < 4; ++i) pb[n * KP + 4 * k4 + i] = gW0[j][i];
-      if (k4 == KP / 4 - 1) pb[NH * KP + NO * NH + n] = gW0[j][3];
-    }
+    for (int j = 0; j < 32; ++j) R2[(m - 64) * 64 + 32 * hh + j] = have ? v[j] : 0.0f;
   }
 #pragma unroll
-  for (int j = 0; j < 8; ++j)
+  for (int c = 0; c < NO; ++c) {
 #pragma unroll
-    for (int c = 0; c < NO; ++c) gW1[c][j] = warp_sum(gW1[c][j]);
+    for (int j = 0; j < 32; ++j) g1[c][j] = warp_sum(g1[c][j]);
+    sb[c] = warp_sum(sb[c]);
+  }
+  if (lane == 0) {
 #pragma unroll
-  for (int c = 0; c < NO; ++c) gB1[c] = warp_sum(gB1[c]);
-  if (tm == 0) {
+    for (int c = 0; c < NO; ++c) {
 #pragma unroll
-    for (int j = 0; j < 8; ++j) {
-      const int n = 8 * tn + j;
-#pragma unroll
-      for (int c = 0; c < NO; ++c) pb[NH * KP + c * NH + n] = gW1[c][j];
-    }
-    if (tn == 0) {
-#pragma unroll
-      for (int c = 0; c < NO; ++c) pb[NH * KP + NO * NH + NH + c] = gB1[c];
+      for (int j = 0; j < 32; ++j) RW1[((q * 2 + hh) * 3 + c) * 32 + j] = g1[c][j];
+      if (hh == 0) RW1[4 * 2 * 3 * 32 + q * 3 + c] = sb[c];
     }
   }
+  __syncthreads();
+  if (q < 2) {
+    float v1[32], v2[32];
+    tc::tmem_ld32(tbase + lane_base + 128 + 32 * hh, v1);
+    tc::tmem_ld32(tbase + lane_base + 192 + 32 * hh, v2);
+    tc::tmem_wait_ld();
+#pragma unroll
+    for (int j = 0; j < 32; ++j) {
+      const int col = 32 * hh + j;
+      const float val = have ? (v1[j] + v2[j]) + R2[m * 64 + col] : 0.0f;
+      if (col < KP) pb[m * KP + col] = val;
+      if (col == KIN) pb[NH * KP + NO * NH + m] = val;  // ones column: db0
+    }
+  }
+  if (tid < NO * NH) {
+    const int c = tid / NH, n = tid % NH, h2 = n >> 5, j = n & 31;
+    float s = 0.0f;
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq) s += RW1[((qq * 2 + h2) * 3 + c) * 32 + j];
+    pb[NH * KP + c * NH + n] = have ? s : 0.0f;
+  }
+  if (tid < NO) {
+    float s = 0.0f;
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq) s += RW1[4 * 2 * 3 * 32 + qq * 3 + tid];
+    pb[NH * KP + NO * NH + NH + tid] = have ? s : 0.0f;
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (wid == 0) tc::tmem_dealloc(tbase, 256);
 }
+
+constexpr size_t kBwdSmem = 4 * kWBytes + 2 * kXtBytes + kR1Bytes + sizeof(float) * (2 * TM * 4 + NO * NH + NH + 4) + 16;
+
 
 // Sum the per-block partials in block order into dW0 (64,51), dW1 (3,64), db0 (64), db1 (3).
 __global__ void k_mlp_wgrad_reduce(const float* __restrict__ partials, int nblocks, float* __restrict__ dW0,
@@ -488,8 +603,69 @@ __global__ void k_mlp_wgrad_reduce(const float* __restrict__ partials, int nbloc
   }
 }
 
-constexpr size_t kBwdSmem =
-    sizeof(float) * (TM * XRS + NH * DZS + KP * NH + NH + NO * NH + 4 + TM * NO);
+// MLP input rows [hash 32 | SH 16 | normal 3 | 0] of (rays, midpoints), four threads per sample:
+// thread (i, g) gathers hash levels 4g..4g+3 (columns 8g..8g+7) and writes SH coefficients
+// 4g..4g+3 (columns 32+4g..); g = 3 also the normal. Few registers and no shared memory, so many
+// warps keep the table gathers in flight; the arithmetic per level is the fused kernel's.
+__global__ void __launch_bounds__(256) k_hash_rows(HashArgs a) {
+  const uint32_t mask = (1u << a.log2T) - 1u;
+  const size_t T = (size_t)1 << a.log2T;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.P * 4;
+       e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e >> 2;
+    const int g = (int)(e & 3);
+    float x[3];
+    sample_pos(a, i, x);
+    float f[8];
+#pragma unroll
+    for (int qq = 0; qq < 4; ++qq) {
+      const int l = 4 * g + qq;
+      const float lw = a.lw[l];
+      float f0 = 0.0f, f1 = 0.0f;
+      if (lw != 0.0f) {
+        LevelCell c;
+        level_cell(x, a.res[l], mask, c);
+        const float2* tab = reinterpret_cast<const float2*>(a.table) + (size_t)l * T;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          const float2 v = __ldg(tab + c.h[k]);
+          f0 = fmaf(c.w[k], v.x, f0);
+          f1 = fmaf(c.w[k], v.y, f1);
+        }
+        if (lw < 1.0f) {
+          f0 *= lw;
+          f1 *= lw;
+        }
+      }
+      f[2 * qq] = f0;
+      f[2 * qq + 1] = f1;
+    }
+    float4* row = reinterpret_cast<float4*>(a.out + i * a.ld);
+    row[2 * g] = make_float4(f[0], f[1], f[2], f[3]);
+    row[2 * g + 1] = make_float4(f[4], f[5], f[6], f[7]);
+    const int64_t r = i / a.S;
+    float o[16];
+    sh16(__ldg(a.rays_d + 3 * r), __ldg(a.rays_d + 3 * r + 1), __ldg(a.rays_d + 3 * r + 2), o);
+    row[8 + g] = g == 0 ? make_float4(o[0], o[1], o[2], o[3])
+                 : g == 1 ? make_float4(o[4], o[5], o[6], o[7])
+                 : g == 2 ? make_float4(o[8], o[9], o[10], o[11])
+                          : make_float4(o[12], o[13], o[14], o[15]);
+    if (g == 3) row[12] = make_float4(a.normals[3 * i], a.normals[3 * i + 1], a.normals[3 * i + 2], 0.0f);
+  }
+}
+
+template <bool kHashIn, bool kRowsOut>
+int launch_fwd(const HashArgs& a, const float* X, int64_t ldx, int64_t P, const MlpW& w, float* colors,
+               cudaStream_t st) {
+  auto kern = k_mlp_fwd_tc<kHashIn, kRowsOut>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem);
+  if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "mlp forward: %s", cudaGetErrorString(e));
+  const int64_t tiles = (P + TM - 1) / TM;
+  const unsigned blocks = (unsigned)(tiles < (int64_t)kSMs * 2 ? tiles : (int64_t)kSMs * 2);
+  const int xvec = X && (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
+  kern<<<blocks, 256, kFwdSmem, st>>>(a, X, ldx, xvec, P, w, colors);
+  return VX_OK;
+}
 
 }  // namespace vx
 
@@ -518,23 +694,33 @@ int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, i
   a.ld = ld_rows;
   a.normals = normals;
   MlpW w{W0, b0, W1, b1};
-  const int64_t tiles = (n_points + TM - 1) / TM;
-  const unsigned blocks = (unsigned)(tiles < (int64_t)kSMs * 4 ? tiles : (int64_t)kSMs * 4);
-  if (rows)
-    k_appearance_mlp_fwd<true><<<blocks, 256, 0, (cudaStream_t)stream>>>(a, w, colors);
-  else
-    k_appearance_mlp_fwd<false><<<blocks, 256, 0, (cudaStream_t)stream>>>(a, w, colors);
-  count_launches(1);
+  cudaStream_t st = (cudaStream_t)stream;
+  if (rows) {  // training: rows gathered at high occupancy, then the MLP on the rows
+    k_hash_rows<<<grid_for(n_points * 4, 256), 256, 0, st>>>(a);
+    if (int s = launch_fwd<false, false>(a, rows, ld_rows, n_points, w, colors, st)) return s;
+    count_launches(2);
+  } else {  // inference: features built in shared memory, nothing else written
+    if (int s = launch_fwd<true, false>(a, nullptr, 0, n_points, w, colors, st)) return s;
+    count_launches(1);
+  }
   return check_launch("appearance_mlp_forward");
 }
 
 int vx_mlp_blocks(int64_t n_points) {
   const int64_t tiles = (n_points + TM - 1) / TM;
-  const int64_t cap = (int64_t)kSMs * 2;
+  const int64_t cap = (int64_t)kSMs;
   return (int)(tiles < 1 ? 1 : (tiles < cap ? tiles : cap));
 }
 
 int vx_mlp_partial_floats(void) { return WG; }
+
+int vx_tensor_core_timeouts(void) {
+  int h = 0;
+  const int zero = 0;
+  if (cudaMemcpyFromSymbol(&h, g_tc_timeouts, sizeof(int)) != cudaSuccess) return -1;
+  if (cudaMemcpyToSymbol(g_tc_timeouts, &zero, sizeof(int)) != cudaSuccess) return -1;
+  return h;
+}
 
 int vx_radiance_mlp_forward(const float* x, int64_t ldx, int64_t n_points, int in_dim, int hidden, int out_dim,
                             const float* W0, const float* b0, const float* W1, const float* b1, float* colors,
@@ -545,9 +731,8 @@ int vx_radiance_mlp_forward(const float* x, int64_t ldx, int64_t n_points, int i
   if (n_points == 0) return VX_OK;
   VX_REQUIRE(x && W0 && b0 && W1 && b1 && colors, "null pointer");
   MlpW w{W0, b0, W1, b1};
-  const int64_t tiles = (n_points + TM - 1) / TM;
-  const unsigned blocks = (unsigned)(tiles < (int64_t)kSMs * 4 ? tiles : (int64_t)kSMs * 4);
-  k_mlp_fwd<<<blocks, 256, 0, (cudaStream_t)stream>>>(x, ldx, n_points, w, colors);
+  HashArgs a{};
+  if (int s = launch_fwd<false, false>(a, x, ldx, n_points, w, colors, (cudaStream_t)stream)) return s;
   count_launches(1);
   return check_launch("radiance_mlp_forward");
 }
@@ -566,10 +751,11 @@ int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int 
              (long long)n_partial_floats, (long long)nb * WG);
   MlpW w{W0, b0, W1, b1};
   cudaStream_t st = (cudaStream_t)stream;
-  cudaError_t e = cudaFuncSetAttribute(k_mlp_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmem);
-  if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "radiance_mlp_backward: %s", cudaGetErrorString(e));
   if (n_points > 0) {
-    k_mlp_bwd<<<nb, 256, kBwdSmem, st>>>(x, ldx, n_points, w, d_colors, d_hash, d_normal, partials);
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_bwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmem);
+    if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "radiance_mlp_backward: %s", cudaGetErrorString(e));
+    const int xvec = (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+    k_mlp_bwd_tc<<<nb, 256, kBwdSmem, st>>>(x, ldx, xvec, n_points, w, d_colors, d_hash, d_normal, partials);
   } else {
     cudaMemsetAsync(partials, 0, sizeof(float) * WG, st);
   }

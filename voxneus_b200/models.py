@@ -307,7 +307,7 @@ class VoxNeuS(nn.Module):
             l0, l1 = self.radiance_mlp.net[0], self.radiance_mlp.net[2]
             colors = ops.AppearanceMLPFn.apply(self.radiance_hash.encoder.embeddings, normal, l0.weight, l0.bias,
                                                l1.weight, l1.bias, o, d, mid, lo, hi, self.radiance_hash.encoder.cfg,
-                                               active_levels)
+                                               active_levels, torch.is_grad_enabled())
         else:
             x = ops.AppearanceInputFn.apply(self.radiance_hash.encoder.embeddings, normal, o, d, mid, lo, hi,
                                             self.radiance_hash.encoder.cfg, active_levels)

@@ -535,15 +535,17 @@ class AppearanceMLPFn(torch.autograd.Function):
     """
 
     @staticmethod
-    def forward(ctx, embeddings, normals, W0, b0, W1, b1, rays_o, rays_d, mid, xyz_min, xyz_max, cfg, active_levels):
+    def forward(ctx, embeddings, normals, W0, b0, W1, b1, rays_o, rays_d, mid, xyz_min, xyz_max, cfg, active_levels,
+                keep_rows=True):
         nr, ns = mid.shape
         p = nr * ns
         width = 2 * cfg.n_levels + 16 + 3
         if width != 51:
             raise RuntimeError("the fused appearance path needs 16 hash levels x 2 features")
         ld = MLP_LD
-        # needs_input_grad stays True under no_grad: inference (serving) must not write the rows
-        need_rows = torch.is_grad_enabled() and any(ctx.needs_input_grad[:6])
+        # keep_rows: the caller's grad mode (forward itself always runs with grad disabled, and
+        # needs_input_grad stays True under no_grad), so inference does not write the rows
+        need_rows = bool(keep_rows) and any(ctx.needs_input_grad[:6])
         rows = torch.empty(p, ld, device=mid.device) if need_rows else None
         nrm = normals.detach().contiguous()
         colors = torch.empty(p, 3, device=mid.device)
@@ -565,13 +567,15 @@ class AppearanceMLPFn(torch.autograd.Function):
         nr, ns = mid.shape
         rows = ctx.rows
         ctx.rows = None
+        if rows is None:
+            raise RuntimeError("AppearanceMLPFn: forward ran with keep_rows=False; no adjoint input kept")
         d_hash, d_normal, dW0, db0, dW1, db1 = mlp_backward(rows, W0, b0, W1, b1, g.reshape(-1, 3))
         d_emb = None
         if ctx.needs_input_grad[0]:
             d_emb = torch.zeros(eshape, device=g.device)
             hash_backward(d_emb, cfg, active_levels, None, rays_o, rays_d, mid, ns, xyz_min, xyz_max, nr * ns, d_hash,
                           32)
-        return (d_emb, d_normal.reshape(nshape), dW0, db0, dW1, db1, None, None, None, None, None, None, None)
+        return (d_emb, d_normal.reshape(nshape), dW0, db0, dW1, db1, None, None, None, None, None, None, None, None)
 
 
 class HashEncodeFn(torch.autograd.Function):
