@@ -32,12 +32,7 @@ __global__ void __launch_bounds__(256) k_appearance_fwd(HashArgs a) {
         level_cell(x, a.res[l], mask, c);
         const float2* tab = reinterpret_cast<const float2*>(a.table) + (size_t)l * T;
         float f0 = 0.0f, f1 = 0.0f;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const float2 e = __ldg(tab + c.h[k]);
-          f0 = fmaf(c.w[k], e.x, f0);
-          f1 = fmaf(c.w[k], e.y, f1);
-        }
+        gather_level(tab, c, f0, f1);
         if (lw < 1.0f) {
           f0 *= lw;
           f1 *= lw;
@@ -92,8 +87,7 @@ __global__ void __launch_bounds__(256) k_hash_bwd(HashArgs a) {
       LevelCell c;
       level_cell(x, a.res[l], mask, c);
       float2* tab = reinterpret_cast<float2*>(a.table_grad) + (size_t)l * T;
-#pragma unroll
-      for (int k = 0; k < 8; ++k) atomicAdd(tab + c.h[k], make_float2(c.w[k] * g0, c.w[k] * g1));
+      scatter_level(tab, c, g0, g1);
     }
   }
 }

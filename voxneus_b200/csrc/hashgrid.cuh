@@ -60,6 +60,7 @@ __device__ __forceinline__ uint32_t hash3(uint32_t x, uint32_t y, uint32_t z, ui
 struct LevelCell {
   uint32_t h[8];
   float w[8];
+  bool xpair;  // the cell's x index is even: corners k and k+4 (x, x+1) are entries h[k], h[k]^1
 };
 
 __device__ __forceinline__ void level_cell(const float x[3], int res, uint32_t mask, LevelCell& c) {
@@ -73,6 +74,7 @@ __device__ __forceinline__ void level_cell(const float x[3], int res, uint32_t m
     c0[k] = (int)fl;
     d[k] = s - fl;
   }
+  c.xpair = (c0[0] & 1) == 0;
   const float ox = 1.0f - d[0], oy = 1.0f - d[1], oz = 1.0f - d[2];
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
@@ -81,6 +83,47 @@ __device__ __forceinline__ void level_cell(const float x[3], int res, uint32_t m
     const uint32_t cz = (uint32_t)(c0[2] + (k & 1));
     c.h[k] = hash3(cx, cy, cz, mask);
     c.w[k] = ((k & 4) ? d[0] : ox) * ((k & 2) ? d[1] : oy) * ((k & 1) ? d[2] : oz);
+  }
+}
+
+// Trilinear blend of one level's 2 features, corners in the order 0..7. Corners k < 4 are read
+// as the aligned 16-byte pair holding h[k]; when the cell's x index is even that pair also holds
+// corner k+4 (hash bit 0 is x's bit 0), else corner k+4 is a separate 8-byte load. Same sums,
+// same order as eight 8-byte loads; about a quarter fewer sectors touched.
+__device__ __forceinline__ void gather_level(const float2* __restrict__ tab, const LevelCell& c, float& f0,
+                                             float& f1) {
+  float2 e[8];
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float4 v = __ldg(reinterpret_cast<const float4*>(tab) + (c.h[k] >> 1));
+    const bool odd = c.h[k] & 1u;
+    e[k] = odd ? make_float2(v.z, v.w) : make_float2(v.x, v.y);
+    e[k + 4] = odd ? make_float2(v.x, v.y) : make_float2(v.z, v.w);
+  }
+  if (!c.xpair) {
+#pragma unroll
+    for (int k = 4; k < 8; ++k) e[k] = __ldg(tab + c.h[k]);
+  }
+#pragma unroll
+  for (int k = 0; k < 8; ++k) {
+    f0 = fmaf(c.w[k], e[k].x, f0);
+    f1 = fmaf(c.w[k], e[k].y, f1);
+  }
+}
+
+// Adjoint of gather_level: one 16-byte atomic per x-pair when the cell's x index is even.
+__device__ __forceinline__ void scatter_level(float2* __restrict__ tab, const LevelCell& c, float g0, float g1) {
+  if (c.xpair) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const float a0 = c.w[k] * g0, a1 = c.w[k] * g1, b0 = c.w[k + 4] * g0, b1 = c.w[k + 4] * g1;
+      const bool odd = c.h[k] & 1u;
+      atomicAdd(reinterpret_cast<float4*>(tab) + (c.h[k] >> 1),
+                odd ? make_float4(b0, b1, a0, a1) : make_float4(a0, a1, b0, b1));
+    }
+  } else {
+#pragma unroll
+    for (int k = 0; k < 8; ++k) atomicAdd(tab + c.h[k], make_float2(c.w[k] * g0, c.w[k] * g1));
   }
 }
 

@@ -81,27 +81,43 @@ __device__ void stage_weights(const MlpW& w, uint8_t* WH, uint8_t* WL, uint8_t* 
   if (tid < NO) B1[tid] = w.b1[tid];
 }
 
-// Rows m0..m0+127 of X (row stride ldx) into the X buffers; thread (m, hh) takes the 16-byte
-// chunks 0..6 (hh = 0) or 7..12 (hh = 1). Column 51 becomes `one` on real rows; rows past P are 0.
-__device__ __forceinline__ void stage_rows(const float* __restrict__ X, int64_t ldx, bool vec, int64_t P, int64_t m0,
-                                           uint8_t* XH, uint8_t* XL, int m, int hh, float one) {
+// Row chunks of sample m of the tile at m0 into registers: thread (m, hh) takes the 16-byte
+// chunks 0..6 (hh = 0) or 7..12 (hh = 1, v[6] unused). Rows past P read as 0.
+__device__ __forceinline__ void load_row_chunks(const float* __restrict__ X, int64_t ldx, bool vec, int64_t P,
+                                                int64_t m0, int m, int hh, float4 v[7]) {
   const bool ok = m0 + m < P;
   const float* row = X + (m0 + m) * ldx;
-  const int c0 = hh ? 7 : 0, c1 = hh ? 13 : 7;
-  for (int c = c0; c < c1; ++c) {
-    float4 v = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    if (ok) {
+  const int c0 = hh ? 7 : 0;
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    const int c = c0 + j;
+    v[j] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    if (ok && c < 13) {
       if (vec) {
-        v = __ldg(reinterpret_cast<const float4*>(row) + c);
+        v[j] = __ldg(reinterpret_cast<const float4*>(row) + c);
       } else {
-        v.x = __ldg(row + 4 * c);
-        v.y = __ldg(row + 4 * c + 1);
-        v.z = __ldg(row + 4 * c + 2);
-        v.w = 4 * c + 3 < KIN ? __ldg(row + 4 * c + 3) : 0.0f;
+        v[j].x = __ldg(row + 4 * c);
+        v[j].y = __ldg(row + 4 * c + 1);
+        v[j].z = __ldg(row + 4 * c + 2);
+        v[j].w = 4 * c + 3 < KIN ? __ldg(row + 4 * c + 3) : 0.0f;
       }
-      if (c == 12) v.w = one;
     }
-    st_split4(XH, XL, x_off(c, m), v.x, v.y, v.z, v.w);
+  }
+}
+
+// The chunks of load_row_chunks into the X buffers (hi/lo tf32); column 51 becomes `one` on
+// real rows.
+__device__ __forceinline__ void store_row_chunks(const float4 v[7], bool valid, uint8_t* XH, uint8_t* XL, int m,
+                                                 int hh, float one) {
+  const int c0 = hh ? 7 : 0;
+#pragma unroll
+  for (int j = 0; j < 7; ++j) {
+    const int c = c0 + j;
+    if (c < 13) {
+      float4 u = v[j];
+      if (c == 12 && valid) u.w = one;
+      st_split4(XH, XL, x_off(c, m), u.x, u.y, u.z, u.w);
+    }
   }
 }
 
@@ -163,6 +179,9 @@ __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* 
   const size_t T = (size_t)1 << a.log2T;
   uint32_t phase = 0;
   const int64_t ntiles = (P + TM - 1) / TM;
+  float4 pre[7];
+  if (!kHashIn && (int64_t)blockIdx.x < ntiles)
+    load_row_chunks(X, ldx, xvec != 0, P, (int64_t)blockIdx.x * TM, tid & (TM - 1), tid >> 7, pre);
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t m0 = t * TM;
     if (kHashIn) {
@@ -181,12 +200,7 @@ __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* 
             LevelCell c;
             level_cell(x, a.res[l], mask, c);
             const float2* tab = reinterpret_cast<const float2*>(a.table) + (size_t)l * T;
-#pragma unroll
-            for (int k = 0; k < 8; ++k) {
-              const float2 e = __ldg(tab + c.h[k]);
-              f0 = fmaf(c.w[k], e.x, f0);
-              f1 = fmaf(c.w[k], e.y, f1);
-            }
+            gather_level(tab, c, f0, f1);
             if (lw < 1.0f) {
               f0 *= lw;
               f1 *= lw;
@@ -232,7 +246,7 @@ __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* 
         }
       }
     } else {
-      stage_rows(X, ldx, xvec != 0, P, m0, XH, XL, tid & (TM - 1), tid >> 7, 0.0f);
+      store_row_chunks(pre, m0 + (tid & (TM - 1)) < P, XH, XL, tid & (TM - 1), tid >> 7, 0.0f);
     }
     tc::fence_smem_to_async();
     __syncthreads();
@@ -241,6 +255,8 @@ __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* 
       issue_z(tbase, xh, xl, wh, wl);
       tc::commit(bar);
     }
+    if (!kHashIn && t + gridDim.x < ntiles)  // next tile's rows fly during the MMA and the epilogue
+      load_row_chunks(X, ldx, xvec != 0, P, (t + gridDim.x) * TM, tid & (TM - 1), tid >> 7, pre);
     const bool ok = tc::mbar_wait(bar, phase, kWaitLimit);
     phase ^= 1u;
     if (__syncthreads_or(!ok)) {
@@ -337,7 +353,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   for (int i = tid; i < NO * NH; i += blockDim.x) W1s[i] = w.W1[i];
   if (tid < NO) B1[tid] = w.b1[tid];
   if (tid == 0) tc::mbar_init(bar, 1);
-  if (wid == 0) tc::tmem_alloc(s_taddr, 256);
+  if (wid == 0) tc::tmem_alloc(s_taddr, 512);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
@@ -346,53 +362,57 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   const uint32_t wh = tc::smem_u32(WH), wl = tc::smem_u32(WL), wth = tc::smem_u32(WTH), wtl = tc::smem_u32(WTL);
   const uint32_t xth = tc::smem_u32(XTH), xtl = tc::smem_u32(XTL), r1 = tc::smem_u32(R1);
   constexpr uint32_t idN = tc::idesc_tf32(TM, 64, false, false);
-  float g1[NO][32];  // dW1 of hidden units 32*hh+j, summed over this thread's samples
+  // dW1 accumulators of hidden units 32*hh+j, colour c, summed over this thread's samples: TMEM
+  // columns 256 + 96*hh + 32*c + j of this thread's lane (registers are spent on the prefetch)
+  const uint32_t g1addr = tbase + lane_base + 256 + 96 * hh;
+  {
+    float zero[32];
 #pragma unroll
-  for (int j = 0; j < 32; ++j) g1[0][j] = g1[1][j] = g1[2][j] = 0.0f;
+    for (int j = 0; j < 32; ++j) zero[j] = 0.0f;
+#pragma unroll
+    for (int c = 0; c < NO; ++c) tc::tmem_st32(g1addr + 32 * c, zero);
+    tc::tmem_wait_st();
+  }
   float sb[NO] = {0.0f, 0.0f, 0.0f};
   bool first_w = true, failed = false;
   uint32_t phase = 0;
   const int64_t ntiles = (P + TM - 1) / TM;
+  float4 pre[7];  // this tile's row chunks, loaded during the previous tile
+  float dy[NO];
+  if ((int64_t)blockIdx.x < ntiles) {
+    const int64_t m0 = (int64_t)blockIdx.x * TM;
+    load_row_chunks(X, ldx, xvec != 0, P, m0, m, hh, pre);
+#pragma unroll
+    for (int c = 0; c < NO; ++c) dy[c] = m0 + m < P ? d_out[(m0 + m) * NO + c] : 0.0f;
+  }
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t m0 = t * TM;
     const bool valid = m0 + m < P;
     // rows -> X (sample rows, R1) and X^T (feature rows); column 51 = 1 on real rows (db0)
     {
-      const float* row = X + (m0 + m) * ldx;
-      const int c0 = hh ? 7 : 0, c1 = hh ? 13 : 7;
-      for (int c = c0; c < c1; ++c) {
-        float v[4] = {0.0f, 0.0f, 0.0f, 0.0f};
-        if (valid) {
-          if (xvec) {
-            const float4 u = __ldg(reinterpret_cast<const float4*>(row) + c);
-            v[0] = u.x;
-            v[1] = u.y;
-            v[2] = u.z;
-            v[3] = u.w;
-          } else {
+      const int c0 = hh ? 7 : 0;
 #pragma unroll
-            for (int i = 0; i < 4; ++i) v[i] = 4 * c + i < KIN ? __ldg(row + 4 * c + i) : 0.0f;
+      for (int jc = 0; jc < 7; ++jc) {
+        const int c = c0 + jc;
+        if (c < 13) {
+          float v[4] = {pre[jc].x, pre[jc].y, pre[jc].z, pre[jc].w};
+          if (c == 12 && valid) v[3] = 1.0f;
+          float hi[4], lo[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) {
+            tc::split_tf32(v[i], hi[i], lo[i]);
+            *reinterpret_cast<float*>(XTH + xt_off(4 * c + i, m)) = hi[i];
+            *reinterpret_cast<float*>(XTL + xt_off(4 * c + i, m)) = lo[i];
           }
-          if (c == 12) v[3] = 1.0f;
+          *reinterpret_cast<float4*>(R1 + x_off(c, m)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
+          *reinterpret_cast<float4*>(R1 + kXBytes + x_off(c, m)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
         }
-        float hi[4], lo[4];
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-          tc::split_tf32(v[i], hi[i], lo[i]);
-          *reinterpret_cast<float*>(XTH + xt_off(4 * c + i, m)) = hi[i];
-          *reinterpret_cast<float*>(XTL + xt_off(4 * c + i, m)) = lo[i];
-        }
-        *reinterpret_cast<float4*>(R1 + x_off(c, m)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
-        *reinterpret_cast<float4*>(R1 + kXBytes + x_off(c, m)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
       }
       if (hh) {  // feature chunk 13 (columns 52..55) is inside the Z contraction: zero it
         *reinterpret_cast<float4*>(R1 + x_off(13, m)) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         *reinterpret_cast<float4*>(R1 + kXBytes + x_off(13, m)) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
       }
     }
-    float dy[NO];
-#pragma unroll
-    for (int c = 0; c < NO; ++c) dy[c] = valid ? d_out[(m0 + m) * NO + c] : 0.0f;
     tc::fence_smem_to_async();
     __syncthreads();
     if (tid == 0) {
@@ -430,16 +450,25 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
 #pragma unroll
       for (int c = 0; c < NO; ++c) sb[c] += d[c];
     }
-    // dW1 (registers), dL/dz (kept in z), DZ (sample rows) into R1: the Z MMA has read X
+    // dW1 (TMEM accumulators), dL/dz (kept in z), DZ (sample rows) into R1: the Z MMA has read X
+#pragma unroll
+    for (int j = 0; j < 32; ++j) z[j] += B0[32 * hh + j];
+#pragma unroll 1
+    for (int c = 0; c < NO; ++c) {
+      float acc[32];
+      tc::tmem_ld32(g1addr + 32 * c, acc);
+      tc::tmem_wait_ld();
+      const float dc = c == 0 ? d[0] : (c == 1 ? d[1] : d[2]);
+#pragma unroll
+      for (int j = 0; j < 32; ++j) acc[j] = fmaf(dc, fmaxf(z[j], 0.0f), acc[j]);
+      tc::tmem_st32(g1addr + 32 * c, acc);
+    }
+    tc::tmem_wait_st();
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
       const int n = 32 * hh + j;
-      const float zz = z[j] + B0[n];
-      const float h = fmaxf(zz, 0.0f);
-#pragma unroll
-      for (int c = 0; c < NO; ++c) g1[c][j] = fmaf(d[c], h, g1[c][j]);
       const float dhid = d[0] * W1s[n] + d[1] * W1s[NH + n] + d[2] * W1s[2 * NH + n];
-      z[j] = zz > 0.0f ? dhid : 0.0f;
+      z[j] = z[j] > 0.0f ? dhid : 0.0f;
     }
 #pragma unroll
     for (int j4 = 0; j4 < 8; ++j4)
@@ -491,6 +520,13 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
       }
       tc::commit(bar);
     }
+    // next tile's rows fly during the dW0 MMAs and the dX readout
+    if (t + gridDim.x < ntiles) {
+      const int64_t mn = (t + gridDim.x) * TM;
+      load_row_chunks(X, ldx, xvec != 0, P, mn, m, hh, pre);
+#pragma unroll
+      for (int c = 0; c < NO; ++c) dy[c] = mn + m < P ? d_out[(mn + m) * NO + c] : 0.0f;
+    }
     // dX readout while the dW0 MMAs run
     if (hh == 0) {
       float v[32];
@@ -534,18 +570,18 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
 #pragma unroll
     for (int j = 0; j < 32; ++j) R2[(m - 64) * 64 + 32 * hh + j] = have ? v[j] : 0.0f;
   }
-#pragma unroll
+#pragma unroll 1
   for (int c = 0; c < NO; ++c) {
+    float acc[32];
+    tc::tmem_ld32(g1addr + 32 * c, acc);
+    tc::tmem_wait_ld();
 #pragma unroll
-    for (int j = 0; j < 32; ++j) g1[c][j] = warp_sum(g1[c][j]);
-    sb[c] = warp_sum(sb[c]);
-  }
-  if (lane == 0) {
+    for (int j = 0; j < 32; ++j) acc[j] = warp_sum(acc[j]);
+    const float sbc = warp_sum(c == 0 ? sb[0] : (c == 1 ? sb[1] : sb[2]));
+    if (lane == 0) {
 #pragma unroll
-    for (int c = 0; c < NO; ++c) {
-#pragma unroll
-      for (int j = 0; j < 32; ++j) RW1[((q * 2 + hh) * 3 + c) * 32 + j] = g1[c][j];
-      if (hh == 0) RW1[4 * 2 * 3 * 32 + q * 3 + c] = sb[c];
+      for (int j = 0; j < 32; ++j) RW1[((q * 2 + hh) * 3 + c) * 32 + j] = acc[j];
+      if (hh == 0) RW1[4 * 2 * 3 * 32 + q * 3 + c] = sbc;
     }
   }
   __syncthreads();
@@ -577,7 +613,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   }
   tc::fence_before_sync();
   __syncthreads();
-  if (wid == 0) tc::tmem_dealloc(tbase, 256);
+  if (wid == 0) tc::tmem_dealloc(tbase, 512);
 }
 
 constexpr size_t kBwdSmem = 4 * kWBytes + 2 * kXtBytes + kR1Bytes + sizeof(float) * (2 * TM * 4 + NO * NH + NH + 4) + 16;
@@ -607,7 +643,7 @@ __global__ void k_mlp_wgrad_reduce(const float* __restrict__ partials, int nbloc
 // thread (i, g) gathers hash levels 4g..4g+3 (columns 8g..8g+7) and writes SH coefficients
 // 4g..4g+3 (columns 32+4g..); g = 3 also the normal. Few registers and no shared memory, so many
 // warps keep the table gathers in flight; the arithmetic per level is the fused kernel's.
-__global__ void __launch_bounds__(256) k_hash_rows(HashArgs a) {
+__global__ void __launch_bounds__(256, 6) k_hash_rows(HashArgs a) {
   const uint32_t mask = (1u << a.log2T) - 1u;
   const size_t T = (size_t)1 << a.log2T;
   for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.P * 4;
@@ -626,12 +662,7 @@ __global__ void __launch_bounds__(256) k_hash_rows(HashArgs a) {
         LevelCell c;
         level_cell(x, a.res[l], mask, c);
         const float2* tab = reinterpret_cast<const float2*>(a.table) + (size_t)l * T;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-          const float2 v = __ldg(tab + c.h[k]);
-          f0 = fmaf(c.w[k], v.x, f0);
-          f1 = fmaf(c.w[k], v.y, f1);
-        }
+        gather_level(tab, c, f0, f1);
         if (lw < 1.0f) {
           f0 *= lw;
           f1 *= lw;
