@@ -282,6 +282,17 @@ int vx_neus_alpha(const float* sdf, const float* normals, const float* dirs, int
 int vx_composite_weights(const float* alpha, int64_t n_rays, int n_samples, float* weights, float* transmittance,
                          const float* d_weights, const float* d_transmittance, float* d_alpha, void* stream);
 
+/* ------------------------------------------------------------------ colour loss ----------- */
+
+/* Blocks of vx_huber_loss (one double partial each). */
+int vx_huber_loss_blocks(int64_t n);
+
+/* NeuS2 Huber colour loss (rendering/volume_render.py:43-54, compute_huber_color_loss): *loss =
+ * mean over n elements of (d < delta ? 0.5 d^2 / delta : d - 0.5 delta), d = |pred - target|;
+ * grad (optional, n floats) = d(loss)/d(pred). partials: >= vx_huber_loss_blocks(n) doubles. */
+int vx_huber_loss(const float* pred, const float* target, int64_t n, float delta, float* loss, float* grad,
+                  double* partials, int64_t n_partials, void* stream);
+
 /* ------------------------------------------------ active vertices and regularizers -------- */
 
 /* 32-bit words of a V_R bitmap for the grid; blocks of block scratch vx_vr_compact needs. */

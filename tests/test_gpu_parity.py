@@ -444,6 +444,25 @@ def test_fused_mlp_matches_oracle(p):
     assert _lib.query("vx_tensor_core_timeouts") == 0
 
 
+def test_huber_loss_and_gradient():
+    """Fused Huber colour loss (value 1e-5, gradient 1e-4) vs the oracle's torch ops; both branches,
+    exact ties and a size that is not a multiple of the block."""
+    from voxneus_b200.rendering import compute_huber_color_loss
+
+    torch.manual_seed(21)
+    pred = torch.rand(10007, 3)
+    tgt = pred + (torch.rand(10007, 3) - 0.5) * 0.5  # |d| spans both sides of delta = 0.1
+    tgt[:5] = pred[:5]  # d = 0
+    pr = pred.clone().requires_grad_(True)
+    ref = O.huber(pr, tgt, 0.1)
+    ref.backward()
+    pd = to(pred).requires_grad_(True)
+    loss = compute_huber_color_loss(pd, to(tgt), 0.1)
+    assert_close(loss, ref.detach(), VAL_TOL, "huber loss")
+    (loss * 3.0).backward()
+    assert_close(pd.grad, 3.0 * pr.grad, GRAD_TOL, "huber grad")
+
+
 def test_fused_appearance_render_matches_cublas_path(golden):
     """Fused hash+MLP render gives the same values and gradients as the cuBLAS MLP path."""
     from voxneus_b200.rendering import RaySampler, compute_huber_color_loss

@@ -139,12 +139,21 @@ __device__ __forceinline__ void colour_partial(const float z[32], int hh, const 
                                                float& p0, float& p1, float& p2) {
   p0 = p1 = p2 = 0.0f;
 #pragma unroll
-  for (int j = 0; j < 32; ++j) {
-    const int n = 32 * hh + j;
-    const float h = fmaxf(z[j] + B0[n], 0.0f);
-    p0 = fmaf(W1s[n], h, p0);
-    p1 = fmaf(W1s[NH + n], h, p1);
-    p2 = fmaf(W1s[2 * NH + n], h, p2);
+  for (int j4 = 0; j4 < 8; ++j4) {
+    const int n = 32 * hh + 4 * j4;
+    const float4 b = *reinterpret_cast<const float4*>(B0 + n);
+    const float4 u0 = *reinterpret_cast<const float4*>(W1s + n);
+    const float4 u1 = *reinterpret_cast<const float4*>(W1s + NH + n);
+    const float4 u2 = *reinterpret_cast<const float4*>(W1s + 2 * NH + n);
+    const float bb[4] = {b.x, b.y, b.z, b.w}, w0[4] = {u0.x, u0.y, u0.z, u0.w};
+    const float w1[4] = {u1.x, u1.y, u1.z, u1.w}, w2[4] = {u2.x, u2.y, u2.z, u2.w};
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const float h = fmaxf(z[4 * j4 + i] + bb[i], 0.0f);
+      p0 = fmaf(w0[i], h, p0);
+      p1 = fmaf(w1[i], h, p1);
+      p2 = fmaf(w2[i], h, p2);
+    }
   }
 }
 
@@ -452,7 +461,13 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     }
     // dW1 (TMEM accumulators), dL/dz (kept in z), DZ (sample rows) into R1: the Z MMA has read X
 #pragma unroll
-    for (int j = 0; j < 32; ++j) z[j] += B0[32 * hh + j];
+    for (int j4 = 0; j4 < 8; ++j4) {
+      const float4 b = *reinterpret_cast<const float4*>(B0 + 32 * hh + 4 * j4);
+      z[4 * j4] += b.x;
+      z[4 * j4 + 1] += b.y;
+      z[4 * j4 + 2] += b.z;
+      z[4 * j4 + 3] += b.w;
+    }
 #pragma unroll 1
     for (int c = 0; c < NO; ++c) {
       float acc[32];
@@ -465,14 +480,32 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     }
     tc::tmem_wait_st();
 #pragma unroll
+    for (int j4 = 0; j4 < 8; ++j4) {
+      const int n = 32 * hh + 4 * j4;
+      const float4 u0 = *reinterpret_cast<const float4*>(W1s + n);
+      const float4 u1 = *reinterpret_cast<const float4*>(W1s + NH + n);
+      const float4 u2 = *reinterpret_cast<const float4*>(W1s + 2 * NH + n);
+      const float w0[4] = {u0.x, u0.y, u0.z, u0.w}, w1[4] = {u1.x, u1.y, u1.z, u1.w};
+      const float w2[4] = {u2.x, u2.y, u2.z, u2.w};
+#pragma unroll
+      for (int i = 0; i < 4; ++i) {
+        const float dhid = d[0] * w0[i] + d[1] * w1[i] + d[2] * w2[i];
+        z[4 * j4 + i] = z[4 * j4 + i] > 0.0f ? dhid : 0.0f;
+      }
+    }
+    float zl[32];  // dL/dz split once: hi in z, lo in zl (stored as DZ now and as DZ^T below)
+#pragma unroll
     for (int j = 0; j < 32; ++j) {
-      const int n = 32 * hh + j;
-      const float dhid = d[0] * W1s[n] + d[1] * W1s[NH + n] + d[2] * W1s[2 * NH + n];
-      z[j] = z[j] > 0.0f ? dhid : 0.0f;
+      const float v = z[j];
+      tc::split_tf32(v, z[j], zl[j]);
     }
 #pragma unroll
-    for (int j4 = 0; j4 < 8; ++j4)
-      st_split4(R1, R1 + kXBytes, x_off(8 * hh + j4, m), z[4 * j4], z[4 * j4 + 1], z[4 * j4 + 2], z[4 * j4 + 3]);
+    for (int j4 = 0; j4 < 8; ++j4) {
+      const uint32_t off = x_off(8 * hh + j4, m);
+      *reinterpret_cast<float4*>(R1 + off) = make_float4(z[4 * j4], z[4 * j4 + 1], z[4 * j4 + 2], z[4 * j4 + 3]);
+      *reinterpret_cast<float4*>(R1 + kXBytes + off) =
+          make_float4(zl[4 * j4], zl[4 * j4 + 1], zl[4 * j4 + 2], zl[4 * j4 + 3]);
+    }
     tc::fence_smem_to_async();
     tc::fence_before_sync();
     __syncthreads();
@@ -499,10 +532,8 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
 #pragma unroll
     for (int j = 0; j < 32; ++j) {
       const int n = 32 * hh + j;
-      float h, l;
-      tc::split_tf32(z[j], h, l);
-      *reinterpret_cast<float*>(R1 + dzt_off(n, m)) = h;
-      *reinterpret_cast<float*>(R1 + dzt_off(NH + n, m)) = l;
+      *reinterpret_cast<float*>(R1 + dzt_off(n, m)) = z[j];
+      *reinterpret_cast<float*>(R1 + dzt_off(NH + n, m)) = zl[j];
     }
     tc::fence_smem_to_async();
     tc::fence_before_sync();

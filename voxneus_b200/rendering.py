@@ -106,9 +106,8 @@ def composite_weights(alpha: torch.Tensor, eps: float = 1e-7) -> Tuple[torch.Ten
 
 
 def compute_huber_color_loss(pred_rgb, target_rgb, delta: float = 0.1):
-    """NeuS2 Huber loss (rendering/volume_render.py:43-54); elementwise plumbing."""
-    diff = torch.abs(pred_rgb - target_rgb)
-    return torch.mean(torch.where(diff < delta, 0.5 * diff ** 2 / delta, diff - 0.5 * delta))
+    """NeuS2 Huber loss (rendering/volume_render.py:43-54): one fused loss + gradient kernel."""
+    return ops.HuberLossFn.apply(pred_rgb, target_rgb, delta)
 
 
 def volume_render_from_samples(colors, sdf, normals, ray_dirs, z_vals, dists, s, pts=None, sphere_radius=1.0,
