@@ -67,18 +67,35 @@ __global__ void __launch_bounds__(256) k_appearance_fwd(HashArgs a) {
   }
 }
 
+// Adjoint of the hash encoding, four threads per sample: thread (i, g) scatters levels
+// [g*lpt, (g+1)*lpt), lpt = ceil(L/4), loading its d_out values before the first atomic so the
+// loads overlap; float4 atomics for the x-pairs of even cells (scatter_level).
 __global__ void __launch_bounds__(256) k_hash_bwd(HashArgs a) {
   const uint32_t mask = (1u << a.log2T) - 1u;
   const size_t T = (size_t)1 << a.log2T;
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < a.P; i += (int64_t)gridDim.x * blockDim.x) {
+  const int lpt = (a.L + 3) >> 2;
+  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.P * 4; e += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t i = e >> 2;
+    const int l0 = (int)(e & 3) * lpt;
+    const int l1 = min(l0 + lpt, a.L);
+    if (l0 >= l1) continue;
     const float* drow = a.d_out + i * a.ld_d;
+    float g[16];  // lpt <= 8 (L <= 32)
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int l = l0 + q;
+      g[2 * q] = l < l1 ? drow[2 * l] : 0.0f;
+      g[2 * q + 1] = l < l1 ? drow[2 * l + 1] : 0.0f;
+    }
     float x[3];
     sample_pos(a, i, x);
-#pragma unroll 1
-    for (int l = 0; l < a.L; ++l) {
+#pragma unroll
+    for (int q = 0; q < 8; ++q) {
+      const int l = l0 + q;
+      if (l >= l1) break;
       const float lw = a.lw[l];
       if (lw == 0.0f) continue;
-      float g0 = drow[2 * l], g1 = drow[2 * l + 1];
+      float g0 = g[2 * q], g1 = g[2 * q + 1];
       if (lw < 1.0f) {
         g0 *= lw;
         g1 *= lw;
@@ -152,7 +169,7 @@ int vx_hash_encode_backward(float* table_grad, int n_levels, int log2_size, int 
   a.P = n_points;
   a.d_out = d_out;
   a.ld_d = ld_d;
-  k_hash_bwd<<<grid_for(n_points, 256), 256, 0, (cudaStream_t)stream>>>(a);
+  k_hash_bwd<<<grid_for(n_points * 4, 256), 256, 0, (cudaStream_t)stream>>>(a);
   count_launches(1);
   return check_launch("hash_encode_backward");
 }
