@@ -333,14 +333,17 @@ int vx_vr_compact_noalloc(const uint32_t* bitmap, const float* grid, const int32
                           const float xyz_max[3], float relax_radius, float band, const unsigned long long* counts,
                           int64_t* verts_out, int64_t* linear_out, int64_t capacity, void* stream);
 
-/* Blocks of the fused regularizer; partials hold 3 doubles per block. */
+/* Blocks of the fused regularizer, and the doubles of its workspace (3 loss partials per block,
+ * then one flag byte per 32x4x4 tile). */
 int64_t vx_reg_stencil_blocks(const int32_t res[3]);
+int64_t vx_reg_stencil_workspace(const int32_t res[3]);
 
 /* Fused eikonal + curvature closed forms (regularization/eikonal.py:13-171 and curvature.py:13-165 as
  * called by training/trainer.py:268-319), gather form (deterministic, no atomics), accumulated into
  * grad_grid with weights w_eik and w_curv and scale 2/|V_R|. bitmap is the filtered pair written by
  * vx_vr_count; counts selects its relax half (the reference applies the relax filter only when a
- * vertex passes it) and gives |V_R|. band is unused (applied by vx_vr_count); counter may be NULL.
+ * vertex passes it) and gives |V_R|. band is unused (applied by vx_vr_count); counter is unused
+ * (may be NULL). partials: >= vx_reg_stencil_workspace(res) doubles.
  * losses (device float[2], nullable) receives the monitoring losses. */
 int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[3], const float xyz_min[3],
                    const float xyz_max[3], float relax_radius, float band, const unsigned long long* counts,

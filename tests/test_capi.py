@@ -39,6 +39,9 @@ def test_size_queries_without_gpu():
     # persistent stencil grid: min(tiles / 8, 4 blocks per SM on 148 SMs)
     assert _lib.query("vx_reg_stencil_blocks", _lib.i3([256, 256, 256])) == 148 * 4
     assert _lib.query("vx_reg_stencil_blocks", _lib.i3([8, 8, 32])) == 1
+    # 3 loss doubles per block + one flag byte per 32x4x4 tile
+    assert _lib.query("vx_reg_stencil_workspace", _lib.i3([256, 256, 256])) == 3 * 148 * 4 + 8 * 64 * 64 // 8
+    assert _lib.query("vx_reg_stencil_workspace", _lib.i3([8, 8, 32])) == 3 + 1
     assert _lib.query("vx_composite_workspace_blocks", 8192) >= 1
     lib = _lib.load(require_cuda=False)
     assert lib.vx_version().startswith(b"voxneus_b200")

@@ -74,6 +74,7 @@ _PROTOS = {
     "vx_vr_compact": [P, P, HI3, HF3, HF3, F32, F32, P, P, I64, P, P, I64, P],
     "vx_vr_compact_noalloc": [P, P, HI3, HF3, HF3, F32, F32, P, P, P, I64, P],
     "vx_reg_stencil_blocks": [HI3],
+    "vx_reg_stencil_workspace": [HI3],
     "vx_reg_stencil": [P, P, HI3, HF3, HF3, F32, F32, P, F32, F32, P, P, I64, P, P, P],
     "vx_grid_upsample": [P, HI3, P, HI3, P],
 }
@@ -84,6 +85,7 @@ _RESTYPES = {
     "vx_vr_bitmap_words": I64,
     "vx_vr_compact_blocks": I64,
     "vx_reg_stencil_blocks": I64,
+    "vx_reg_stencil_workspace": I64,
     "vx_geometry_backward_det_workspace": ctypes.c_size_t,
     "vx_hash_backward_det_workspace": ctypes.c_size_t,
 }

@@ -159,9 +159,7 @@ __global__ void __launch_bounds__(256) k_curvature_list(const float* __restrict_
 // ------------------------------------ gather form ------------------------------------------
 
 constexpr int TZ = 32, TY = 4, TX = 4;  // output tile (z fastest)
-constexpr int HZ = TZ + 4, HY = TY + 4, HX = TX + 4;  // SDF box, halo 2
-constexpr int MZ = TZ + 2, MY = TY + 2, MX = TX + 2;  // vertex box, halo 1
-constexpr int NVB = MX * MY * MZ;                      // vertices in the halo-1 box
+constexpr int MY = TY + 2, MX = TX + 2;  // halo-1 box extents in y and x
 
 struct StencilArgs {
   const float* f;
@@ -172,7 +170,7 @@ struct StencilArgs {
   float relax_r;
   float w_eik, w_curv;
   float* gg;
-  int tiles_z, tiles_y;
+  int tiles_z, tiles_y, tiles_x;
 };
 
 __device__ __forceinline__ void tile_origin(const StencilArgs& a, int t, int& x0, int& y0, int& z0) {
@@ -205,127 +203,213 @@ __device__ __forceinline__ bool tile_has_bits_warp(const StencilArgs& a, const u
   return __any_sync(0xffffffffu, hit);
 }
 
-// Persistent grid over 32x4x4 tiles taken 8 at a time; blockDim = (32, 4, 2). Each warp tests one
-// tile of the batch against the filtered bitmap, so an empty tile costs one load per lane. For
-// an active tile: stage the SDF box (halo 2); evaluate every active interior vertex of the halo-1
-// box once, storing the contribution it makes to itself (curvature centre) and to each face
-// neighbour (eikonal +-dL/dn_a / 2eps_a plus curvature L_a/eps_a^2, scaled); then every output
-// voxel sums the <= 7 terms that land on it. Per-block loss partials; k_reg_finalize reduces them.
-__global__ void __launch_bounds__(256) k_reg_stencil(StencilArgs a, double* __restrict__ partials, int ntiles) {
-  __shared__ float F[HX][HY][HZ];
-  __shared__ float T[7][NVB];  // [0] centre, [1+2a] to v+e_a, [2+2a] to v-e_a
-  __shared__ double red[3][8];
-  __shared__ int active[8];
-  const int tid = threadIdx.x + 32 * (threadIdx.y + 4 * threadIdx.z);
-  const bool relax_on = a.relax_r > 0.0f && a.counts[1] > 0;
-  const bool band_on = a.counts[2] != a.counts[0] || a.counts[3] != a.counts[1];
-  (void)band_on;
-  const uint32_t* bm = a.fb + (relax_on ? a.nwords : 0);
-  // |V_R| after the filters: counts[1 or 3] (relax) / counts[0 or 2] (no relax); the filtered
-  // bitmaps already carry the band, so the band count is the one to use
-  const unsigned long long nv = relax_on ? a.counts[3] : a.counts[2];
-  const float inv_nv = nv > 0 ? 2.0f / (float)nv : 0.0f;
-  const float dx = 2.0f * a.g.eps[0], dy = 2.0f * a.g.eps[1], dz = 2.0f * a.g.eps[2];
-  const float ex2 = a.g.eps[0] * a.g.eps[0], ey2 = a.g.eps[1] * a.g.eps[1], ez2 = a.g.eps[2] * a.g.eps[2];
-  const float sc = inv_nv * a.w_curv;
-  double le = 0, lc = 0, ln = 0;
-  for (int tb = blockIdx.x * 8; tb < ntiles; tb += gridDim.x * 8) {
-    {
-      const int w = tid >> 5;
-      const bool hit = (tb + w < ntiles) ? tile_has_bits_warp(a, bm, tb + w, tid & 31) : false;
-      if ((tid & 31) == 0) active[w] = hit;
-    }
-    __syncthreads();
-    for (int wt = 0; wt < 8; ++wt) {
-      if (!active[wt]) continue;
-      int x0, y0, z0;
-      tile_origin(a, tb + wt, x0, y0, z0);
-      for (int q = tid; q < HX * HY * HZ; q += 256) {
-        const int hz = q % HZ, hy = (q / HZ) % HY, hx = q / (HZ * HY);
-        const int x = x0 - 2 + hx, y = y0 - 2 + hy, z = z0 - 2 + hz;
-        float v = 0.0f;
-        if (x >= 0 && x < a.g.rx && y >= 0 && y < a.g.ry && z >= 0 && z < a.g.rz)
-          v = __ldg(a.f + lin3(a.g, x, y, z));
-        F[hx][hy][hz] = v;
-      }
-      __syncthreads();
-      // per-vertex terms of the halo-1 box
-      for (int q = tid; q < NVB; q += 256) {
-        const int mz = q % MZ, my = (q / MZ) % MY, mx = q / (MZ * MY);
-        const int x = x0 - 1 + mx, y = y0 - 1 + my, z = z0 - 1 + mz;
-        bool on = x >= 1 && x <= a.g.rx - 2 && y >= 1 && y <= a.g.ry - 2 && z >= 1 && z <= a.g.rz - 2;
-        if (on) {
-          const int idx = lin3(a.g, x, y, z);
-          on = (__ldg(bm + (idx >> 5)) >> (idx & 31)) & 1u;
-        }
-        float t0 = 0.f, tpx = 0.f, tmx = 0.f, tpy = 0.f, tmy = 0.f, tpz = 0.f, tmz = 0.f;
-        if (on) {
-          const int hx = mx + 1, hy = my + 1, hz = mz + 1;
-          const float fc = F[hx][hy][hz];
-          const float fxp = F[hx + 1][hy][hz], fxm = F[hx - 1][hy][hz];
-          const float fyp = F[hx][hy + 1][hz], fym = F[hx][hy - 1][hz];
-          const float fzp = F[hx][hy][hz + 1], fzm = F[hx][hy][hz - 1];
-          const float Lx = (fxp + fxm - 2.0f * fc) / ex2;
-          const float Ly = (fyp + fym - 2.0f * fc) / ey2;
-          const float Lz = (fzp + fzm - 2.0f * fc) / ez2;
-          const float nx = (fxp - fxm) / dx, ny = (fyp - fym) / dy, nz = (fzp - fzm) / dz;
-          const float len = sqrtf(nx * nx + ny * ny + nz * nz);
-          // eikonal_grad.cu: scale = 2/|V_R| (1 - 1/(|n| + 1e-8)) w; +-scale*n_a / (2 eps_a)
-          const float se = inv_nv * (1.0f - 1.0f / (len + 1e-8f)) * a.w_eik;
-          const float ex = (se * nx) / dx, ey = (se * ny) / dy, ez = (se * nz) / dz;
-          // curvature_grad.cu: centre scale*(-2 Lx/ex^2 - 2 Ly/ey^2 - 2 Lz/ez^2), neighbours scale*L_a/eps_a^2
-          const float cx = sc * (Lx / ex2), cy = sc * (Ly / ey2), cz = sc * (Lz / ez2);
-          t0 = sc * (-2.0f * Lx / ex2 - 2.0f * Ly / ey2 - 2.0f * Lz / ez2);
-          tpx = ex + cx;
-          tmx = -ex + cx;
-          tpy = ey + cy;
-          tmy = -ey + cy;
-          tpz = ez + cz;
-          tmz = -ez + cz;
-          if (mx >= 1 && mx <= TX && my >= 1 && my <= TY && mz >= 1 && mz <= TZ) {  // owned by this tile
-            const double l = sqrt((double)nx * nx + (double)ny * ny + (double)nz * nz + 1e-16);
-            le += (l - 1.0) * (l - 1.0);
-            lc += (double)Lx * Lx + (double)Ly * Ly + (double)Lz * Lz;
-            ln += 1.0;
-          }
-        }
-        T[0][q] = t0;
-        T[1][q] = tpx;
-        T[2][q] = tmx;
-        T[3][q] = tpy;
-        T[4][q] = tmy;
-        T[5][q] = tpz;
-        T[6][q] = tmz;
-      }
-      __syncthreads();
-      const int lz = threadIdx.x, ly = threadIdx.y;
-#pragma unroll
-      for (int rep = 0; rep < 2; ++rep) {
-        const int lx = threadIdx.z + 2 * rep;
-        const int x = x0 + lx, y = y0 + ly, z = z0 + lz;
-        if (x >= a.g.rx || y >= a.g.ry || z >= a.g.rz) continue;
-        const int c = ((lx + 1) * MY + (ly + 1)) * MZ + (lz + 1);  // this voxel in the vertex box
-        float acc = T[0][c];
-        acc += T[1][c - MY * MZ] + T[2][c + MY * MZ];  // from v - e_x (to v + e_x) and v + e_x (to v - e_x)
-        acc += T[3][c - MZ] + T[4][c + MZ];
-        acc += T[5][c - 1] + T[6][c + 1];
-        if (acc != 0.0f) {
-          float* p = a.gg + lin3(a.g, x, y, z);
-          *p += acc;
-        }
-      }
-      __syncthreads();  // F and T are rewritten by the next tile
-    }
-    __syncthreads();  // active[] is rewritten by the next batch
+struct StencilConsts {
+  float inv_nv, dx, dy, dz, ex2, ey2, ez2, sc, w_eik;
+};
+
+// What active vertex (x, y, z) adds to itself (t0: curvature centre) and to its face neighbours
+// (tp[a] to v + e_a, tm[a] to v - e_a: eikonal +-scale n_a / (2 eps_a) plus curvature scale L_a /
+// eps_a^2), with scale = 2/|V_R| (1 - 1/(|n| + 1e-8)) w_eik and sc = 2/|V_R| w_curv
+// (eikonal_grad.cu, curvature_grad.cu); also its two loss terms.
+__device__ __forceinline__ void vertex_terms(const StencilArgs& a, const StencilConsts& k, int x, int y, int z,
+                                             float& t0, float tp[3], float tm[3], double* loss) {
+  const float* f = a.f;
+  const int c = lin3(a.g, x, y, z);
+  const int sx = a.g.ry * a.g.rz, sy = a.g.rz;
+  const float fc = __ldg(f + c);
+  const float fxp = __ldg(f + c + sx), fxm = __ldg(f + c - sx);
+  const float fyp = __ldg(f + c + sy), fym = __ldg(f + c - sy);
+  const float fzp = __ldg(f + c + 1), fzm = __ldg(f + c - 1);
+  const float Lx = (fxp + fxm - 2.0f * fc) / k.ex2;
+  const float Ly = (fyp + fym - 2.0f * fc) / k.ey2;
+  const float Lz = (fzp + fzm - 2.0f * fc) / k.ez2;
+  const float nx = (fxp - fxm) / k.dx, ny = (fyp - fym) / k.dy, nz = (fzp - fzm) / k.dz;
+  const float len = sqrtf(nx * nx + ny * ny + nz * nz);
+  const float se = k.inv_nv * (1.0f - 1.0f / (len + 1e-8f)) * k.w_eik;
+  const float ex = (se * nx) / k.dx, ey = (se * ny) / k.dy, ez = (se * nz) / k.dz;
+  const float cx = k.sc * (Lx / k.ex2), cy = k.sc * (Ly / k.ey2), cz = k.sc * (Lz / k.ez2);
+  t0 = k.sc * (-2.0f * Lx / k.ex2 - 2.0f * Ly / k.ey2 - 2.0f * Lz / k.ez2);
+  tp[0] = ex + cx;
+  tm[0] = -ex + cx;
+  tp[1] = ey + cy;
+  tm[1] = -ey + cy;
+  tp[2] = ez + cz;
+  tm[2] = -ez + cz;
+  if (loss) {
+    const double l = sqrt((double)nx * nx + (double)ny * ny + (double)nz * nz + 1e-16);
+    loss[0] += (l - 1.0) * (l - 1.0);
+    loss[1] += (double)Lx * Lx + (double)Ly * Ly + (double)Lz * Lz;
+    loss[2] += 1.0;
   }
-  le = warp_sum_d(le);
-  lc = warp_sum_d(lc);
-  ln = warp_sum_d(ln);
-  const int wl = tid & 31, ww = tid >> 5;
-  if (wl == 0) {
-    red[0][ww] = le;
-    red[1][ww] = lc;
-    red[2][ww] = ln;
+}
+
+// V_R bits of the vertices (x, y, z0 - 1 .. z0 + 32) of one grid column as bits 0..33 of a word
+// pair (vertices outside the interior read 0).
+__device__ __forceinline__ uint64_t column_window(const StencilArgs& a, const uint32_t* __restrict__ bm, int x, int y,
+                                                  int z0) {
+  if (x < 1 || x > a.g.rx - 2 || y < 1 || y > a.g.ry - 2) return 0ull;
+  const int64_t b = (int64_t)lin3(a.g, x, y, z0) - 1;  // bit of vertex z0 - 1 (may precede the column)
+  const int64_t w0 = b >> 5;
+  const int s = (int)(b & 31);
+  const uint32_t u0 = (w0 >= 0 && w0 < a.nwords) ? __ldg(bm + w0) : 0u;
+  const uint32_t u1 = (w0 + 1 < a.nwords) ? __ldg(bm + w0 + 1) : 0u;
+  const uint32_t u2 = (s > 0 && w0 + 2 < a.nwords) ? __ldg(bm + w0 + 2) : 0u;
+  uint64_t v = ((uint64_t)u1 << 32 | u0) >> s;
+  if (s > 0) v |= (uint64_t)u2 << (64 - s);
+  // keep interior z only: z = z0 - 1 + k in [1, rz - 2]
+  const int klo = max(0, 2 - z0), khi = min(33, a.g.rz - 1 - z0);
+  if (khi < klo) return 0ull;
+  const uint64_t keep = ((khi >= 63 ? ~0ull : ((1ull << (khi + 1)) - 1ull))) & ~((1ull << klo) - 1ull);
+  return v & keep;
+}
+
+__device__ __forceinline__ uint64_t shfl_u64(uint64_t v, int src) {
+  const uint32_t lo = __shfl_sync(0xffffffffu, (uint32_t)v, src);
+  const uint32_t hi = __shfl_sync(0xffffffffu, (uint32_t)(v >> 32), src);
+  return (uint64_t)hi << 32 | lo;
+}
+
+// Does tile t own a vertex of the filtered V_R set? One thread per tile (its own voxels, no halo).
+__global__ void __launch_bounds__(256) k_tile_flags(StencilArgs a, int ntiles, uint8_t* __restrict__ flags) {
+  const bool relax_on = a.relax_r > 0.0f && a.counts[1] > 0;
+  const uint32_t* bm = a.fb + (relax_on ? a.nwords : 0);
+  for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < ntiles; t += gridDim.x * blockDim.x) {
+    int x0, y0, z0;
+    tile_origin(a, t, x0, y0, z0);
+    bool hit = false;
+    const int z1 = min(z0 + TZ, a.g.rz) - 1;
+    for (int q = 0; q < TX * TY && !hit; ++q) {
+      const int x = x0 + q / TY, y = y0 + q % TY;
+      if (x >= a.g.rx || y >= a.g.ry) continue;
+      const int b0 = lin3(a.g, x, y, z0), b1 = lin3(a.g, x, y, z1);
+      for (int w = b0 >> 5; w <= (b1 >> 5); ++w) {
+        uint32_t m = 0xffffffffu;
+        if (w == (b0 >> 5)) m &= 0xffffffffu << (b0 & 31);
+        if (w == (b1 >> 5)) m &= 0xffffffffu >> (31 - (b1 & 31));
+        hit |= (__ldg(bm + w) & m) != 0u;
+      }
+    }
+    flags[t] = hit ? 1 : 0;
+  }
+}
+
+// Fused eikonal + curvature gradient in gather form over 32x4x4 tiles. Warp w of the grid owns
+// tiles w, w + W, w + 2W, ... (W warps); its lanes test 32 of them at once against the flags of the
+// 3x3x3 tiles around each (a tile's outputs need the vertices of its halo), and the warp then
+// works through the tiles that need it, one at a time, lane = z offset. Lane c < 36 loads the V_R
+// window of column (x0 - 1 + c / 6, y0 - 1 + c % 6) of the tile's halo; each output voxel reads its
+// 7 neighbour bits from those windows (warp shuffles of a uniform column) and sums, in a fixed
+// order, the terms of the active ones, each evaluated from the SDF through L1 — V_R is a thin
+// band, so few vertices are active. No atomics, no shared staging; per-block loss partials
+// (fixed assignment and order) for k_reg_finalize.
+__global__ void __launch_bounds__(256) k_reg_stencil(StencilArgs a, const uint8_t* __restrict__ flags,
+                                                     double* __restrict__ partials, int ntiles) {
+  __shared__ double red[3][8];
+  __shared__ uint16_t vlist_all[8][MX * MY * (TZ + 2)];  // per warp: active vertices of the halo box
+  __shared__ float acc_all[8][TX * TY * TZ];             // per warp: the tile's output sums
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  uint16_t* vlist = vlist_all[warp];
+  float* acc_s = acc_all[warp];
+  for (int o = lane; o < TX * TY * TZ; o += 32) acc_s[o] = 0.0f;
+  __syncwarp();
+  const bool relax_on = a.relax_r > 0.0f && a.counts[1] > 0;
+  const uint32_t* bm = a.fb + (relax_on ? a.nwords : 0);
+  // |V_R| after the filters: counts[3] (relax) / counts[2] (no relax); the filtered bitmaps
+  // already carry the band, so the band count is the one to use
+  const unsigned long long nv = relax_on ? a.counts[3] : a.counts[2];
+  StencilConsts k;
+  k.inv_nv = nv > 0 ? 2.0f / (float)nv : 0.0f;
+  k.dx = 2.0f * a.g.eps[0];
+  k.dy = 2.0f * a.g.eps[1];
+  k.dz = 2.0f * a.g.eps[2];
+  k.ex2 = a.g.eps[0] * a.g.eps[0];
+  k.ey2 = a.g.eps[1] * a.g.eps[1];
+  k.ez2 = a.g.eps[2] * a.g.eps[2];
+  k.sc = k.inv_nv * a.w_curv;
+  k.w_eik = a.w_eik;
+  double loss[3] = {0.0, 0.0, 0.0};
+  const int gw = blockIdx.x * 8 + warp, nw = gridDim.x * 8;
+  for (int base = 0; gw + base * nw < ntiles; base += 32) {
+    const int tl = gw + (base + lane) * nw;
+    bool need = false;
+    if (tl < ntiles) {
+      const int tz = tl % a.tiles_z, ty = (tl / a.tiles_z) % a.tiles_y, tx = tl / (a.tiles_z * a.tiles_y);
+      for (int dx = -1; dx <= 1; ++dx)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dz = -1; dz <= 1; ++dz) {
+            const int nx = tx + dx, ny = ty + dy, nz = tz + dz;
+            if (nx < 0 || nx >= a.tiles_x || ny < 0 || ny >= a.tiles_y || nz < 0 || nz >= a.tiles_z) continue;
+            need |= __ldg(flags + ((int64_t)nx * a.tiles_y + ny) * a.tiles_z + nz) != 0;
+          }
+    }
+    unsigned todo = __ballot_sync(0xffffffffu, need);
+    while (todo) {
+      const int b = __ffs(todo) - 1;
+      todo &= todo - 1;
+      const int t = gw + (base + b) * nw;
+      int x0, y0, z0;
+      tile_origin(a, t, x0, y0, z0);
+      const uint64_t w0 = column_window(a, bm, x0 - 1 + lane / 6, y0 - 1 + lane % 6, z0);
+      const uint64_t w1 =
+          lane < 4 ? column_window(a, bm, x0 - 1 + (lane + 32) / 6, y0 - 1 + (lane + 32) % 6, z0) : 0ull;
+      const int cnt0 = __popcll(w0), cnt1 = __popcll(w1);
+      int incl = cnt0 + cnt1;  // inclusive warp prefix of the vertex counts (column order)
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int total = __shfl_sync(0xffffffffu, incl, 31);
+      if (total == 0) continue;
+      // compact the active vertices of the halo box: code = column * 34 + window bit
+      int pos = incl - cnt0 - cnt1;
+      for (uint64_t m = w0; m; m &= m - 1) vlist[pos++] = (uint16_t)(lane * 34 + __ffsll((long long)m) - 1);
+      for (uint64_t m = w1; m; m &= m - 1) vlist[pos++] = (uint16_t)((lane + 32) * 34 + __ffsll((long long)m) - 1);
+      __syncwarp();
+      // evaluate each vertex once and add its 7 terms into the tile's accumulators in 7 ordered
+      // passes (two vertices never share a target within a pass)
+      for (int base = 0; base < total; base += 32) {
+        const int idx = base + lane;
+        float t0 = 0.0f, tp[3] = {0.0f, 0.0f, 0.0f}, tm[3] = {0.0f, 0.0f, 0.0f};
+        int vx = 0, vy = 0, vz = 0;
+        const bool mine = idx < total;
+        if (mine) {
+          const int code = vlist[idx], col = code / 34, kb = code - 34 * col;
+          vx = x0 - 1 + col / MY;
+          vy = y0 - 1 + col % MY;
+          vz = z0 - 1 + kb;
+          const bool owned = vx >= x0 && vx < x0 + TX && vy >= y0 && vy < y0 + TY && vz >= z0 && vz < z0 + TZ;
+          vertex_terms(a, k, vx, vy, vz, t0, tp, tm, owned ? loss : nullptr);
+        }
+#pragma unroll
+        for (int p = 0; p < 7; ++p) {
+          const int ax = p == 1 ? 1 : (p == 2 ? -1 : 0), ay = p == 3 ? 1 : (p == 4 ? -1 : 0);
+          const int az = p == 5 ? 1 : (p == 6 ? -1 : 0);
+          const float term = p == 0 ? t0 : (p & 1) ? tp[(p - 1) >> 1] : tm[(p - 1) >> 1];
+          const int ox = vx + ax - x0, oy = vy + ay - y0, oz = vz + az - z0;
+          if (mine && ox >= 0 && ox < TX && oy >= 0 && oy < TY && oz >= 0 && oz < TZ)
+            acc_s[(ox * TY + oy) * TZ + oz] += term;
+          __syncwarp();
+        }
+      }
+      // add the tile's sums to the gradient (z-contiguous lanes) and clear the accumulators
+#pragma unroll 1
+      for (int o = lane; o < TX * TY * TZ; o += 32) {
+        const float v = acc_s[o];
+        if (v != 0.0f) {
+          const int ox = o / (TY * TZ), oy = (o / TZ) % TY, oz = o % TZ;
+          a.gg[lin3(a.g, x0 + ox, y0 + oy, z0 + oz)] += v;
+          acc_s[o] = 0.0f;
+        }
+      }
+      __syncwarp();
+    }
+  }
+  double le = warp_sum_d(loss[0]), lc = warp_sum_d(loss[1]), ln = warp_sum_d(loss[2]);
+  if (lane == 0) {
+    red[0][warp] = le;
+    red[1][warp] = lc;
+    red[2][warp] = ln;
   }
   __syncthreads();
   if (tid == 0) {
@@ -430,9 +514,14 @@ static int64_t stencil_tiles(const int32_t res[3]) {
 }
 
 int64_t vx_reg_stencil_blocks(const int32_t res[3]) {
-  const int64_t t = (stencil_tiles(res) + 7) / 8;  // tiles are taken 8 per block iteration
+  const int64_t t = (stencil_tiles(res) + 7) / 8;  // at least one tile per warp
   const int64_t cap = (int64_t)kSMs * 4;
   return t < cap ? t : cap;
+}
+
+int64_t vx_reg_stencil_workspace(const int32_t res[3]) {
+  // 3 loss doubles per block, then one flag byte per tile
+  return 3 * vx_reg_stencil_blocks(res) + (stencil_tiles(res) + 7) / 8;
 }
 
 int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[3], const float xyz_min[3],
@@ -442,9 +531,9 @@ int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[
   if (int s = check_reg(res)) return s;
   VX_REQUIRE(grid && bitmap && counts && grad_grid && partials && xyz_min && xyz_max, "null pointer");
   const int64_t nb = vx_reg_stencil_blocks(res);
-  VX_REQUIRE(nb < (int64_t(1) << 31), "grid too large");
-  VX_REQUIRE(n_partials >= 3 * nb, "partials buffer too small (%lld < %lld)", (long long)n_partials,
-             (long long)(3 * nb));
+  const int64_t need = vx_reg_stencil_workspace(res);
+  VX_REQUIRE(n_partials >= need, "workspace too small (%lld < %lld doubles)", (long long)n_partials,
+             (long long)need);
   StencilArgs a;
   a.f = grid;
   a.fb = bitmap;
@@ -458,11 +547,15 @@ int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[
   a.gg = grad_grid;
   a.tiles_z = (res[2] + TZ - 1) / TZ;
   a.tiles_y = (res[1] + TY - 1) / TY;
+  a.tiles_x = (res[0] + TX - 1) / TX;
   (void)counter;
   const int64_t ntiles = stencil_tiles(res);
-  k_reg_stencil<<<(unsigned)nb, dim3(32, 4, 2), 0, (cudaStream_t)stream>>>(a, partials, (int)ntiles);
-  if (losses) k_reg_finalize<<<1, 256, 0, (cudaStream_t)stream>>>(partials, (int)nb, losses);
-  count_launches(losses ? 2 : 1);
+  uint8_t* flags = reinterpret_cast<uint8_t*>(partials + 3 * nb);
+  cudaStream_t st = (cudaStream_t)stream;
+  k_tile_flags<<<grid_for(ntiles, 256), 256, 0, st>>>(a, (int)ntiles, flags);
+  k_reg_stencil<<<(unsigned)nb, 256, 0, st>>>(a, flags, partials, (int)ntiles);
+  if (losses) k_reg_finalize<<<1, 256, 0, st>>>(partials, (int)nb, losses);
+  count_launches(losses ? 3 : 2);
   return check_launch("reg_stencil");
 }
 

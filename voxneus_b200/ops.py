@@ -851,8 +851,7 @@ def reg_stencil(grid, filtered, res, xyz_min, xyz_max, relax_radius, band, count
     dev = grid.device
     bitmap = filtered
     sc = Scratch.get(dev)
-    nblk = int(L.query("vx_reg_stencil_blocks", i3(res)))
-    partials = sc.partials_for(3 * nblk)
+    partials = sc.partials_for(int(L.query("vx_reg_stencil_workspace", i3(res))))
     if losses is None:
         losses = torch.zeros(2, device=dev)
     call("vx_reg_stencil", ptr(grid), ptr(bitmap), i3(res), f3(xyz_min), f3(xyz_max), float(relax_radius),
