@@ -15,7 +15,10 @@ Design:
   budget (a fraction of the free HBM measured at start), then each iteration takes one chunk
   from every active request in turn (round robin), so requests that arrive while others are
   running start at the next iteration and their chunks interleave with the older ones on the
-  device; input copies run on a separate copy stream ahead of the compute stream.
+  device; input copies run on a separate copy stream ahead of the compute stream. Results for
+  host requests come back through a fixed ring of pinned staging blocks on the copy stream and
+  are copied into ordinary host tensors by the engine thread as each block lands (allocating
+  pinned memory per request would cost milliseconds and synchronise the device).
 * A result is the same alone and in any mix: every ray and point is computed independently,
   with the same kernels and launch shapes, whatever chunk it falls in.
 * Failures stay on the host: malformed requests are rejected at submission, a request larger
@@ -25,6 +28,7 @@ Design:
 
 from __future__ import annotations
 
+import collections
 import math
 import queue
 import threading
@@ -62,6 +66,8 @@ class Request:
     _next: int = 0
     _reserved: int = 0
     _copy_evt: Optional[torch.cuda.Event] = None
+    _out_evt: Optional[torch.cuda.Event] = None
+    _pieces_left: int = 0
 
     @property
     def latency(self) -> float:
@@ -136,6 +142,8 @@ class _GraphBucket:
 class ServingEngine:
     RENDER_BUCKETS = (4096, 16384, 65536)
     QUERY_BUCKETS = (65536, 262144, 1048576)
+    STAGE_BYTES = 16 << 20  # pinned staging block
+    STAGE_BLOCKS = 8
 
     def __init__(self, store: SceneStore, memory_fraction: float = 0.5, n_samples: int = 64,
                  n_importance: int = 64, budget_bytes: Optional[int] = None, fault_injector=None,
@@ -168,6 +176,14 @@ class ServingEngine:
         self.waiting: List[Request] = []
         self.active: List[Request] = []
         self._inflight: List[Tuple[torch.cuda.Event, Request]] = []
+        # device -> host results go through a fixed ring of pinned staging blocks (allocating pinned
+        # memory per request is slow and synchronising); the engine thread copies each landed block
+        # into the request's ordinary host tensor
+        self._stage = [torch.empty(self.STAGE_BYTES, dtype=torch.uint8, pin_memory=True)
+                       for _ in range(self.STAGE_BLOCKS)]
+        self._free_stage: List[int] = list(range(self.STAGE_BLOCKS))
+        self._pieces: "collections.deque" = collections.deque()  # (req, src flat view, dst flat view)
+        self._pieces_inflight: List[Tuple[torch.cuda.Event, int, Request, torch.Tensor, int]] = []
         self._rid = 0
         self._stop = threading.Event()
         self._failed: Optional[str] = None
@@ -195,7 +211,8 @@ class ServingEngine:
         for t in req.inputs:
             if t.dim() != 2 or t.shape[1] != 3 or t.shape[0] != n or t.dtype != torch.float32:
                 raise RequestError("inputs must be float32 (n, 3) tensors of equal length")
-            if not bool(torch.isfinite(t).all()):
+            # one float64 reduction: finite iff every element is (float32 magnitudes cannot overflow it)
+            if not math.isfinite(float(t.sum(dtype=torch.float64))):
                 raise RequestError("inputs contain NaN or Inf")
         if n == 0:
             raise RequestError("empty request")
@@ -263,31 +280,67 @@ class ServingEngine:
         req._next = start + cnt
 
     def _finish(self, req: Request):
-        host = req.inputs[0].device.type == "cpu"
-        with torch.cuda.stream(self.compute):
-            if host:
-                req.outputs = {}
-                for k, v in req._dev_out.items():
-                    h = torch.empty(v.shape, dtype=v.dtype, pin_memory=True)
-                    h.copy_(v, non_blocking=True)
-                    req.outputs[k] = h
-            else:
-                req.outputs = dict(req._dev_out)
-            evt = torch.cuda.Event()
-            evt.record(self.compute)
-        self._inflight.append((evt, req))
+        """All chunks of req are queued on the compute stream: queue its results for the host."""
+        evt = torch.cuda.Event()
+        evt.record(self.compute)
+        if req.inputs[0].device.type != "cpu":
+            req.outputs = dict(req._dev_out)
+            self._inflight.append((evt, req))
+            return
+        req._out_evt = evt
+        req.outputs = {}
+        req._pieces_left = 0
+        for k, v in req._dev_out.items():
+            h = torch.empty(v.shape, dtype=v.dtype)
+            req.outputs[k] = h
+            src, dst = v.reshape(-1).view(torch.uint8), h.reshape(-1).view(torch.uint8)
+            for a in range(0, src.numel(), self.STAGE_BYTES):
+                b = min(a + self.STAGE_BYTES, src.numel())
+                self._pieces.append((req, src[a:b], dst[a:b]))
+                req._pieces_left += 1
+        self._issue_pieces()
+
+    def _issue_pieces(self):
+        while self._pieces and self._free_stage:
+            req, src, dst = self._pieces.popleft()
+            i = self._free_stage.pop()
+            n = src.numel()
+            with torch.cuda.stream(self.copy):
+                self.copy.wait_event(req._out_evt)
+                self._stage[i][:n].copy_(src, non_blocking=True)
+                evt = torch.cuda.Event()
+                evt.record(self.copy)
+            self._pieces_inflight.append((evt, i, req, dst, n))
+
+    def _complete(self, req: Request):
+        req.finished = time.perf_counter()
+        self.reserved -= req._reserved
+        req._dev_in, req._dev_out = (), {}
+        req.done.set()
 
     def _poll(self):
         keep = []
         for evt, req in self._inflight:
             if evt.query():
-                req.finished = time.perf_counter()
-                self.reserved -= req._reserved
-                req._dev_in, req._dev_out = (), {}
-                req.done.set()
+                self._complete(req)
             else:
                 keep.append((evt, req))
         self._inflight = keep
+        keep_p = []
+        for evt, i, req, dst, n in self._pieces_inflight:
+            if evt.query():
+                dst.copy_(self._stage[i][:n])
+                self._free_stage.append(i)
+                req._pieces_left -= 1
+                if req._pieces_left == 0:
+                    self._complete(req)
+            else:
+                keep_p.append((evt, i, req, dst, n))
+        self._pieces_inflight = keep_p
+        self._issue_pieces()
+
+    def _busy(self) -> bool:
+        return bool(self.active or self._inflight or self._pieces or self._pieces_inflight)
 
     def _loop(self):
         try:
@@ -296,7 +349,7 @@ class ServingEngine:
                 self._admit()
                 self._poll()
                 if not self.active:
-                    if not self._inflight:
+                    if not self._busy():
                         time.sleep(0.0002)
                     continue
                 for req in list(self.active):
@@ -308,7 +361,8 @@ class ServingEngine:
                         self._finish(req)
         except Exception as e:  # host-side failure: fail every request and stop
             self._failed = f"{type(e).__name__}: {e}"
-            for req in self.active + self.waiting + [r for _, r in self._inflight]:
+            in_copy = [p[0] for p in self._pieces] + [p[2] for p in self._pieces_inflight]
+            for req in self.active + self.waiting + [r for _, r in self._inflight] + in_copy:
                 req.error = self._failed
                 req.done.set()
             while True:
