@@ -80,15 +80,52 @@ def make_scene(res, device, seed=0):
 
 
 class ClockSampler:
+    """SM clock, max clock, power and clock-event reasons sampled during the timed region: NVML
+    read every 5 ms from a thread (one sample taken on entry and one on exit, so a region shorter
+    than the period still has samples); `nvidia-smi -lms 50` when NVML is not importable."""
+
     FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
               "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
               "clocks_event_reasons.sw_power_cap")
+    NAMES = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, period_s: float = 0.005):
         self.index = index
+        self.period = period_s
         self.proc = None
+        self.nvml = None
+        self.samples = []  # (sm_mhz, max_mhz, reasons set)
+
+    def _nvml_sample(self):
+        nv, h = self.nvml, self.handle
+        sm = nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)
+        mx = nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM)
+        bits = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+        masks = (nv.nvmlClocksEventReasonHwSlowdown, nv.nvmlClocksEventReasonHwThermalSlowdown,
+                 nv.nvmlClocksEventReasonSwThermalSlowdown, nv.nvmlClocksEventReasonSwPowerCap)
+        self.samples.append((float(sm), float(mx), {nm for nm, m in zip(self.NAMES, masks) if bits & m}))
+
+    def _loop(self):
+        while not self._stop.wait(self.period):
+            try:
+                self._nvml_sample()
+            except Exception:  # a failed read only loses that sample
+                pass
 
     def __enter__(self):
+        try:
+            import pynvml
+
+            pynvml.nvmlInit()
+            self.nvml = pynvml
+            self.handle = self._nvml_handle(pynvml)
+            self._nvml_sample()
+            self._stop = threading.Event()
+            self._thread = threading.Thread(target=self._loop, daemon=True)
+            self._thread.start()
+            return self
+        except Exception:
+            self.nvml = None
         try:
             self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}",
                                           "--format=csv,noheader,nounits", "-lms", "50"],
@@ -97,8 +134,22 @@ class ClockSampler:
             self.proc = None
         return self
 
+    def _nvml_handle(self, nv):
+        """NVML enumerates every GPU of the machine: find this process's CUDA device by PCI address."""
+        pr = torch.cuda.get_device_properties(self.index)
+        bus = f"{pr.pci_domain_id:08X}:{pr.pci_bus_id:02X}:{pr.pci_device_id:02X}.0"
+        return nv.nvmlDeviceGetHandleByPciBusId(bus)
+
     def __exit__(self, *exc):
-        self.lines = []
+        if self.nvml is not None:
+            self._stop.set()
+            self._thread.join(timeout=2)
+            try:
+                self._nvml_sample()
+                self.nvml.nvmlShutdown()
+            except Exception:
+                pass
+            return
         if self.proc is not None:
             self.proc.terminate()
             try:
@@ -106,25 +157,23 @@ class ClockSampler:
             except subprocess.TimeoutExpired:
                 self.proc.kill()
                 out, _ = self.proc.communicate()
-            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+            for ln in out.splitlines():
+                parts = [p.strip() for p in ln.split(",")]
+                if len(parts) < 8:
+                    continue
+                try:
+                    sm, mx = float(parts[0]), float(parts[1])
+                except ValueError:
+                    continue
+                self.samples.append((sm, mx, {nm for nm, v in zip(self.NAMES, parts[4:8])
+                                              if v.lower().startswith("active")}))
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
-        for ln in getattr(self, "lines", []):
-            parts = [p.strip() for p in ln.split(",")]
-            if len(parts) < 8:
-                continue
-            try:
-                sm.append(float(parts[0]))
-                mx = float(parts[1])
-            except ValueError:
-                continue
-            for nm, v in zip(names, parts[4:8]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
+        sm = [x[0] for x in self.samples]
+        mx = self.samples[-1][1] if self.samples else None
+        reasons = set().union(*[x[2] for x in self.samples]) if self.samples else set()
         return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx, "reasons": sorted(reasons),
-                "samples": len(sm)}
+                "samples": len(sm), "source": "nvml" if self.nvml is not None else "nvidia-smi"}
 
 
 def peak_hbm():

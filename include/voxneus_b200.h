@@ -76,6 +76,22 @@ int vx_adam_upd(float* param, const float* grad, float* exp_avg, float* exp_avg_
 int vx_masked_adam_upd(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, int step,
                        float beta1, float beta2, float lr, float eps, void* stream);
 
+/* torch.optim.Adam's update (no counterpart in the reference extension: the reference steps its
+ * network parameters, training/optimizer.py:119-154, with torch.optim.Adam):
+ * m = b1 m + (1-b1) g, v = b2 v + (1-b2) g^2, p -= (lr / (1 - b1^t)) m / (sqrt(v) / sqrt(1 - b2^t) + eps),
+ * over several tensors, each with its own step count t and learning rate (its parameter group's),
+ * one launch per 8 tensors. All segments are updated in place. */
+typedef struct vx_adam_segment {
+  float* param;
+  const float* grad;
+  float* exp_avg;
+  float* exp_avg_sq;
+  int64_t n;
+  int64_t step;
+  float lr;
+} vx_adam_segment;
+int vx_adam_torch(const vx_adam_segment* segs, int n_segs, float beta1, float beta2, float eps, void* stream);
+
 /* ------------------------------------------------------------ field queries --------------- */
 
 /* DenseSDFGrid.query_sdf (models/sdf_grid.py:90-120) and query_normals (:122-160) in one pass over
@@ -349,6 +365,41 @@ int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[
                    const float xyz_max[3], float relax_radius, float band, const unsigned long long* counts,
                    float w_eik, float w_curv, float* grad_grid, double* partials, int64_t n_partials,
                    unsigned int* counter, float* losses, void* stream);
+
+/* ------------------------------------------------------------ occupancy grid ------------- */
+
+/* Bytes of the workspace vx_occupancy_update needs for n drawn cells (8 per cell, 16-byte padded). */
+int64_t vx_occupancy_workspace(int64_t n);
+
+/* World-space centres of the drawn cells (n,3) of an occ_res^3 grid spanning [occ_min, occ_max]:
+ * xyz_min + ((idx + 0.5) / res) * (xyz_max - xyz_min) (rendering/occupancy_grid.py:85-98), for a
+ * caller that evaluates its own SDF function at them. */
+int vx_occupancy_points(int32_t occ_res, const float occ_min[3], const float occ_max[3], const int64_t* idx_x,
+                        const int64_t* idx_y, const int64_t* idx_z, int64_t n, float* pts, void* stream);
+
+/* OccupancyGrid.is_occupied (rendering/occupancy_grid.py:121-147) for world points pts (n,3):
+ * occupied_out[i] = 1 when the point lies inside [occ_min, occ_max] and its cell of the occ_res^3
+ * mask is set (the lookup the sampler applies to interval midpoints), else 0. */
+int vx_occupancy_query(const uint8_t* mask, int32_t occ_res, const float occ_min[3], const float occ_max[3],
+                       const float* pts, int64_t n, uint8_t* occupied_out, void* stream);
+
+/* OccupancyGrid.update_from_sdf (rendering/occupancy_grid.py:62-119) at caller-drawn cells
+ * (idx_x, idx_y, idx_z: n int64 each, as torch.randint draws them, :81-83). The SDF comes from the
+ * dense grid (sdf_grid with res / sdf_min / sdf_max, the trilinear query of models/sdf_grid.py:90-120
+ * at the cell centres) or, when sdf_grid is NULL, from sdf_values (n). s (device scalar) is s, or the
+ * variance parameter v when s_is_variance (s = clamp(exp(10 v), 1e-4, s_max)). Density
+ * s*sig*(1-sig), sig = sigmoid(s*sdf); floor 2*threshold where |sdf| < 2*|(xyz_max-xyz_min)/occ_res|;
+ * unless first, max with decay * previous density; density (occ_res^3 float) and mask (occ_res^3
+ * bytes, 0/1; a torch.bool tensor) are written at the drawn cells. A cell drawn several times gets
+ * the value computed from its density before this update. Cells outside [0, occ_res) are skipped and
+ * counted into *n_invalid (device, nullable). workspace: >= vx_occupancy_workspace(n) bytes, 16-byte
+ * aligned. Two launches on stream. */
+int vx_occupancy_update(const float* sdf_grid, const int32_t res[3], const float sdf_min[3], const float sdf_max[3],
+                        const float* sdf_values, int32_t occ_res, const float occ_min[3], const float occ_max[3],
+                        const int64_t* idx_x, const int64_t* idx_y, const int64_t* idx_z, int64_t n,
+                        const float* s, int s_is_variance, float s_max, int first, float decay, float threshold,
+                        float* density, uint8_t* mask, void* workspace, int64_t workspace_bytes,
+                        unsigned int* n_invalid, void* stream);
 
 /* -------------------------------------------------------------- grid upsampling ----------- */
 

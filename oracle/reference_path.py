@@ -189,6 +189,33 @@ def is_occupied(mask: torch.Tensor, pts: torch.Tensor, xyz_min, xyz_max) -> torc
     return occ.reshape(lead)
 
 
+def occupancy_update(density: torch.Tensor, mask: torch.Tensor, idx: torch.Tensor, sdf_fn, s, first: bool,
+                     xyz_min, xyz_max, decay: float = 0.95, threshold: float = 0.01) -> None:
+    """One EMA update of the occupancy grid at the drawn cells idx (3, n), in place.
+
+    rendering/occupancy_grid.py:62-119: cell centres -> world points, SDF query, logistic density
+    s*sig*(1-sig) with sig = sigmoid(s*sdf) (:15-22), near-surface floor 2*threshold where
+    |sdf| < 2*|voxel step|, max with decay*previous after the first update, mask = density > threshold.
+    Cells drawn more than once all read the previous value and write the same result.
+    """
+    r = density.shape[0]
+    lo = torch.as_tensor(xyz_min, dtype=torch.float32)
+    hi = torch.as_tensor(xyz_max, dtype=torch.float32)
+    ix, iy, iz = idx[0], idx[1], idx[2]
+    step = (hi - lo) / float(r)
+    pts = torch.stack([lo[a] + ((i.float() + 0.5) / float(r)) * (hi[a] - lo[a]) for a, i in enumerate((ix, iy, iz))],
+                      dim=-1)
+    sdf = sdf_fn(pts).reshape(-1)
+    s = torch.as_tensor(s, dtype=torch.float32)
+    sig = torch.sigmoid(s * sdf)
+    dens = s * sig * (1.0 - sig)
+    near = (torch.abs(sdf) < 2.0 * torch.linalg.norm(step).item()).float()
+    eff = torch.maximum(dens, near * (threshold * 2.0))
+    upd = eff if first else torch.maximum(density[ix, iy, iz] * decay, eff)
+    density[ix, iy, iz] = upd
+    mask[ix, iy, iz] = upd > threshold
+
+
 def up_sample(o, d, z, sdf, n_importance: int, inv_s: float, det: bool, occ_fn=None, u=None,
               return_detail=False):
     """One NeuS upsampling step.  rendering/sampler.py:243-292."""

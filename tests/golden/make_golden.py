@@ -43,8 +43,9 @@ def _import_reference(path: str):
     from voxneus.rendering import neus_alpha as ralpha
     from voxneus.rendering import volume_render as rvr
     from voxneus.training import scheduler as rsched
+    from voxneus.rendering.occupancy_grid import OccupancyGrid
 
-    return dict(up=up, PyTorchHashGrid=PyTorchHashGrid, SH=SphericalHarmonicsEmbedder, DenseSDFGrid=DenseSDFGrid,
+    return dict(OccupancyGrid=OccupancyGrid, up=up, PyTorchHashGrid=PyTorchHashGrid, SH=SphericalHarmonicsEmbedder, DenseSDFGrid=DenseSDFGrid,
                 VoxNeuS=VoxNeuS, eav=extract_active_vertices, curv=compute_curvature_loss_and_gradient,
                 eik=compute_eikonal_loss_and_gradient, rays=rrays, sampler=rsampler, alpha=ralpha, vr=rvr,
                 sched=rsched)
@@ -224,20 +225,52 @@ def gen_alpha(R):
     save("alpha.npz", sdf=sdf, normals=nrm, dirs=dirs, dists=dists, s=s, alpha=a, acut=acut, wcut=w, tcut=t)
 
 
+def gen_occupancy(R):
+    """OccupancyGrid.update_from_sdf (rendering/occupancy_grid.py:62-119): three EMA updates of a
+    32^3 occupancy grid from a perturbed sphere SDF on a 20^3 grid. The cell draws of each update
+    are replayed from the same seed first so that the fixture carries the indices the reference drew."""
+    torch.manual_seed(11)
+    m = R["DenseSDFGrid"](resolution=20, init_mode="sphere")
+    with torch.no_grad():
+        m.grid.add_(0.03 * torch.randn_like(m.grid))
+    occ = R["OccupancyGrid"](resolution=32)
+    out = dict(grid=m.grid.detach())
+    for k, (s, ratio) in enumerate([(30.0, 0.05), (45.0, 0.05), (80.0, 0.0)]):
+        seed = 100 + k
+        torch.manual_seed(seed)
+        n = max(int(32 ** 3 * ratio), 1024)
+        idx = torch.stack([torch.randint(0, 32, (n,)) for _ in range(3)])
+        torch.manual_seed(seed)
+        occ.update_from_sdf(m.query_sdf, torch.tensor(s), subsample_ratio=ratio)
+        out[f"idx{k}"] = idx
+        out[f"s{k}"] = np.float32(s)
+        out[f"density{k}"] = occ.density_grid.clone()
+        out[f"mask{k}"] = occ.occupancy_mask.clone()
+    save("occupancy.npz", **out)
+
+
+GENERATORS = {
+    "field_query": gen_field_query,
+    "sampler": gen_sampler,
+    "render_det": lambda R: gen_render(R, perturb=False, name="render_det.npz"),
+    "render_perturb": lambda R: gen_render(R, perturb=True, name="render_perturb.npz"),
+    "regularizers": gen_regularizers,
+    "upsample": gen_upsample,
+    "hash": gen_hash,
+    "alpha": gen_alpha,
+    "occupancy": gen_occupancy,
+}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--reference", default="/root/reference/Code")
+    ap.add_argument("--only", nargs="*", choices=sorted(GENERATORS), help="fixtures to write (default: all)")
     args = ap.parse_args()
     torch.set_num_threads(1)
     R = _import_reference(args.reference)
-    gen_field_query(R)
-    gen_sampler(R)
-    gen_render(R, perturb=False, name="render_det.npz")
-    gen_render(R, perturb=True, name="render_perturb.npz")
-    gen_regularizers(R)
-    gen_upsample(R)
-    gen_hash(R)
-    gen_alpha(R)
+    for name in args.only or list(GENERATORS):
+        GENERATORS[name](R)
 
 
 if __name__ == "__main__":

@@ -43,6 +43,10 @@ def test_size_queries_without_gpu():
     assert _lib.query("vx_reg_stencil_workspace", _lib.i3([256, 256, 256])) == 3 * 148 * 4 + 8 * 64 * 64 // 8
     assert _lib.query("vx_reg_stencil_workspace", _lib.i3([8, 8, 32])) == 3 + 1
     assert _lib.query("vx_composite_workspace_blocks", 8192) >= 1
+    # occupancy update: a float value and an int32 cell per draw, each half 16-byte padded
+    assert _lib.query("vx_occupancy_workspace", 524288) == 8 * 524288
+    assert _lib.query("vx_occupancy_workspace", 1) == 32
+    assert _lib.query("vx_occupancy_workspace", 0) == 0
     lib = _lib.load(require_cuda=False)
     assert lib.vx_version().startswith(b"voxneus_b200")
 
@@ -58,6 +62,10 @@ def test_invalid_arguments_are_rejected_before_launch():
                                  None, 4, 16, 200, 4, 0, None, None, None, None, None, 0, None, None, None, None,
                                  None, None)
     assert st == 1 and b"<= 32" in lib.vx_last_error()
+    # occupancy update with neither an SDF grid nor SDF values
+    st = lib.vx_occupancy_update(None, None, None, None, None, 32, _lib.f3([-1] * 3), _lib.f3([1] * 3), None, None,
+                                 None, 0, None, 0, 0.0, 1, 0.95, 0.01, None, None, None, 0, None, None)
+    assert st == 1 and b"exactly one" in lib.vx_last_error()
 
 
 def test_kernel_calls_fail_loudly_without_cuda(monkeypatch):

@@ -516,3 +516,161 @@ def test_masked_adam_leaves_zero_grad_untouched():
     SparseGridAdam([p], lr=0.05).step()
     assert p[0].item() == 1.0 and p[30].item() == 1.0 and p[999].item() == 1.0
     assert p[10].item() < 1.0 and p[50].item() > 1.0
+
+
+def _occ_compare(dens_gpu, mask_gpu, dens_ref, mask_ref, threshold=0.01):
+    """Density within VAL_TOL; the mask bit-exact except where the oracle's value sits within
+    VAL_TOL of the threshold (a comparison that one ulp of SDF can flip)."""
+    assert_close(dens_gpu, dens_ref, VAL_TOL, "occupancy density")
+    m_gpu = mask_gpu.cpu()
+    border = (dens_ref.double() - threshold).abs() <= VAL_TOL * (abs(threshold) + float(dens_ref.abs().max()))
+    assert bool(((m_gpu == mask_ref) | border).all()), int((m_gpu != mask_ref).sum())
+
+
+def test_occupancy_update_golden(golden):
+    """The reference's three EMA updates (its own cell draws) replayed through the kernel."""
+    from voxneus_b200 import ops
+
+    g = golden("occupancy.npz")
+    lo, hi = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
+    grid = to(g["grid"])
+    density = torch.zeros(32, 32, 32, device=DEV)
+    mask = torch.ones(32, 32, 32, dtype=torch.bool, device=DEV)
+    for k in range(3):
+        idx = [to(g[f"idx{k}"][a].contiguous()) for a in range(3)]
+        s = torch.tensor(float(g[f"s{k}"]), device=DEV)
+        ops.occupancy_update(density, mask, idx, lo, hi, s, False, 0.0, k == 0, 0.95, 0.01, grid=grid,
+                             grid_bounds=(lo, hi))
+        torch.cuda.synchronize()
+        _occ_compare(density, mask, g[f"density{k}"], g[f"mask{k}"])
+
+
+def test_occupancy_update_full_size_matches_oracle():
+    """128^3 occupancy grid, a quarter of the cells per update (524,288 draws with repeats), 96^3
+    SDF grid, s from the variance parameter, three updates against the oracle on the same draws."""
+    from voxneus_b200.models import VoxNeuS
+
+    torch.manual_seed(3)
+    m = VoxNeuS(grid_res=96, hash_log2_size=12).to(DEV)
+    with torch.no_grad():
+        m.sdf_grid.grid.add_(0.02 * torch.randn_like(m.sdf_grid.grid))
+    lo, hi = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
+    glo, ghi = torch.tensor(lo), torch.tensor(hi)
+    grid_cpu = m.sdf_grid.grid.detach().cpu()
+    dens = torch.zeros(128, 128, 128)
+    mask = torch.ones(128, 128, 128, dtype=torch.bool)
+    gen = torch.Generator(device=DEV)
+    for k, v in enumerate([0.3, 0.45, 0.6]):
+        with torch.no_grad():
+            m.variance_net.variance.fill_(v)
+        gen.manual_seed(40 + k)
+        m.update_occupancy_grid(0.25, generator=gen)
+        gen.manual_seed(40 + k)
+        idx = torch.stack([torch.randint(0, 128, (128 ** 3 // 4,), device=DEV, generator=gen) for _ in range(3)]).cpu()
+        s = O.variance_s(torch.tensor(v))
+        O.occupancy_update(dens, mask, idx, lambda p: O.query_sdf(grid_cpu, p, glo, ghi), s, k == 0, lo, hi)
+        torch.cuda.synchronize()
+        _occ_compare(m.occupancy_grid.density_grid, m.occupancy_grid.occupancy_mask, dens, mask)
+    assert m.occupancy_grid.total_updates == 3
+    assert 0.0 < m.occupancy_grid.occupied_percentage < 100.0
+
+
+def test_occupancy_repeated_cell_reads_previous_density():
+    """A cell drawn many times in one update decays once (gather before scatter)."""
+    from voxneus_b200 import ops
+
+    lo, hi = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
+    density = torch.full((8, 8, 8), 1.0, device=DEV)
+    mask = torch.ones(8, 8, 8, dtype=torch.bool, device=DEV)
+    idx = [torch.full((5000,), 7, dtype=torch.int64, device=DEV) for _ in range(3)]
+    far = torch.full((5000,), 10.0, device=DEV)  # density ~0, not near the surface
+    ops.occupancy_update(density, mask, idx, lo, hi, torch.tensor(30.0, device=DEV), False, 0.0, False, 0.95, 0.01,
+                         sdf_values=far)
+    torch.cuda.synchronize()
+    assert float(density[7, 7, 7]) == float(torch.tensor(0.95))
+    assert float(density[0, 0, 0]) == 1.0 and bool(mask[7, 7, 7])
+
+
+def test_occupancy_callable_known_answer_and_query():
+    """tests/test_neus2_features.py:30-55 through the module API on the GPU (an analytic SDF
+    callable), and is_occupied bit-exact against the oracle, points outside the box included."""
+    from voxneus_b200.models import OccupancyGrid
+
+    torch.manual_seed(5)
+    occ = OccupancyGrid(resolution=32, threshold=0.01).to(DEV)
+    for _ in range(5):
+        occ.update_from_sdf(lambda p: torch.linalg.norm(p, dim=-1, keepdim=True) - 0.5, torch.tensor(30.0), 1.0)
+    surf = torch.tensor([[0.5, 0.0, 0.0], [0.0, 0.5, 0.0], [0.0, 0.0, 0.5]], device=DEV)
+    far = torch.tensor([[0.95, 0.95, 0.95], [-0.95, -0.95, -0.95]], device=DEV)
+    assert bool(occ.is_occupied(surf).all()) and not bool(occ.is_occupied(far).all())
+    pts = (torch.rand(20000, 3) * 2.4 - 1.2)
+    pts[:5] = torch.tensor([[1.0, 1.0, 1.0], [-1.0, -1.0, -1.0], [1.0000001, 0.0, 0.0], [0.0, -1.0, 0.5],
+                            [0.99999994, 0.99999994, 0.99999994]])
+    got = occ.is_occupied(to(pts.reshape(100, 200, 3))).cpu().reshape(-1)
+    ref = O.is_occupied(occ.occupancy_mask.cpu(), pts, torch.tensor([-1.0] * 3), torch.tensor([1.0] * 3))
+    assert torch.equal(got, ref)
+
+
+def test_fused_adam_matches_torch_adam():
+    """FusedAdam (one multi-tensor launch, torch.optim.Adam's formula) against torch.optim.Adam:
+    three groups with their own learning rates, vector bodies with scalar tails, zero gradients,
+    and a parameter whose grad is None for one step (skipped, its step count held back)."""
+    from voxneus_b200.training import FusedAdam
+
+    torch.manual_seed(7)
+    shapes = [(16, 4099, 2), (64, 51), (64,), (3, 64), (3,), ()]
+    base = [torch.randn(s) for s in shapes]
+    ours = [b.clone().to(DEV).requires_grad_(True) for b in base]
+    ref = [b.clone().to(DEV).requires_grad_(True) for b in base]
+
+    def groups(ps):
+        return [{"params": ps[:1], "lr": 1e-2}, {"params": ps[1:5], "lr": 1e-3}, {"params": ps[5:], "lr": 5e-4}]
+
+    opt = FusedAdam(groups(ours), betas=(0.9, 0.999), eps=1e-8)
+    opt_ref = torch.optim.Adam(groups(ref), betas=(0.9, 0.999), eps=1e-8, foreach=False)
+    for step in range(5):
+        grads = [torch.randn(s) * (torch.rand(s) > 0.3) for s in shapes]
+        for ps in (ours, ref):
+            for k, p in enumerate(ps):
+                p.grad = None if (step == 2 and k == 3) else grads[k].to(DEV)
+        opt.step()
+        opt_ref.step()
+        for a, b in zip(ours, ref):
+            assert_close(a.detach(), b.detach(), 1e-6, "adam param", scale=1.0)
+    for a, b in zip(ours, ref):
+        sa, sb = opt.state[a], opt_ref.state[b]
+        assert sa["step"] == int(sb["step"])
+        assert_close(sa["exp_avg"], sb["exp_avg"], 1e-6, "exp_avg", scale=1.0)
+        assert_close(sa["exp_avg_sq"], sb["exp_avg_sq"], 1e-6, "exp_avg_sq", scale=1.0)
+
+
+@pytest.mark.parametrize("offset", [0, 1])
+def test_masked_adam_reference_formula(offset):
+    """vx_masked_adam_upd / vx_adam_upd against the extension's formula (adam_upd_kernel.cu:40-82)
+    in float64, on a 16-byte aligned buffer (float4 body + tail) and on one offset by 4 bytes
+    (scalar path); gradient-0 elements keep p, m and v bit for bit in the masked form."""
+    from voxneus_b200 import ops
+
+    torch.manual_seed(8)
+    n = 1_000_003
+    bufs = [torch.randn(n + offset) for _ in range(4)]
+    bufs[1][torch.rand(n + offset) < 0.6] = 0.0  # grad
+    bufs[3] = bufs[3].abs()  # exp_avg_sq >= 0
+    for masked in (True, False):
+        p, g, m, v = (b.clone().to(DEV)[offset:] for b in bufs)
+        p0, g0, m0, v0 = (b[offset:].double() for b in bufs)
+        step, b1, b2, lr, eps = 3, 0.9, 0.99, 0.1, 1e-8
+        ops.adam_update(p, g, m, v, step, b1, b2, lr, eps, masked=masked)
+        torch.cuda.synchronize()
+        ss = lr * math.sqrt(1 - b2 ** step) / (1 - b1 ** step)
+        m1 = b1 * m0 + (1 - b1) * g0
+        v1 = b2 * v0 + (1 - b2) * g0 * g0
+        p1 = p0 - ss * m1 / (v1.sqrt() + eps)
+        if masked:
+            keep = g0 == 0
+            m1[keep], v1[keep], p1[keep] = m0[keep], v0[keep], p0[keep]
+            assert torch.equal(p.cpu()[keep], bufs[0][offset:][keep])
+            assert torch.equal(m.cpu()[keep], bufs[2][offset:][keep])
+        assert_close(p, p1, 1e-6, "adam p", scale=1.0)
+        assert_close(m, m1, 1e-6, "adam m", scale=1.0)
+        assert_close(v, v1, 1e-6, "adam v", scale=1.0)

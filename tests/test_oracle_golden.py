@@ -164,3 +164,40 @@ def test_hash_resolutions():
     res = O.hash_level_resolutions(16)
     assert res[0] == 16 and res[-1] == 2048 and all(b >= a for a, b in zip(res, res[1:]))
     assert math.isclose(O.level_weight(5, 5.5), 0.5)
+
+
+def test_occupancy_update(golden):
+    """Three EMA updates replayed at the reference's own cell draws reproduce its grids exactly."""
+    g = golden("occupancy.npz")
+    lo, hi = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
+    glo, ghi = torch.tensor(lo), torch.tensor(hi)
+    density = torch.zeros(32, 32, 32)
+    mask = torch.ones(32, 32, 32, dtype=torch.bool)
+    for k in range(3):
+        O.occupancy_update(density, mask, g[f"idx{k}"], lambda p: O.query_sdf(g["grid"], p, glo, ghi), g[f"s{k}"],
+                           k == 0, lo, hi)
+        assert torch.equal(density, g[f"density{k}"]) and torch.equal(mask, g[f"mask{k}"])
+    # untouched cells keep the initial state: density 0, mask True
+    drawn = torch.zeros(32, 32, 32, dtype=torch.bool)
+    for k in range(3):
+        i = g[f"idx{k}"]
+        drawn[i[0], i[1], i[2]] = True
+    assert bool((density[~drawn] == 0).all()) and bool(mask[~drawn].all())
+    assert bool((~mask[drawn]).any()) and bool(mask[drawn].any())
+
+
+def test_occupancy_sphere_known_answer():
+    """tests/test_neus2_features.py:30-55: sphere r=0.5 on a 32^3 grid, s=30, five full-ratio
+    updates -> the three axis surface points are occupied and two far points are not both occupied."""
+    torch.manual_seed(0)
+    lo, hi = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
+    density = torch.zeros(32, 32, 32)
+    mask = torch.ones(32, 32, 32, dtype=torch.bool)
+    for k in range(5):
+        idx = torch.stack([torch.randint(0, 32, (32 ** 3,)) for _ in range(3)])
+        O.occupancy_update(density, mask, idx, lambda p: torch.linalg.norm(p, dim=-1) - 0.5, 30.0, k == 0, lo, hi)
+    surf = O.is_occupied(mask, torch.tensor([[0.5, 0.0, 0.0], [0.0, 0.5, 0.0], [0.0, 0.0, 0.5]]), torch.tensor(lo),
+                         torch.tensor(hi))
+    far = O.is_occupied(mask, torch.tensor([[0.95, 0.95, 0.95], [-0.95, -0.95, -0.95]]), torch.tensor(lo),
+                        torch.tensor(hi))
+    assert bool(surf.all()) and not bool(far.all())

@@ -77,6 +77,12 @@ _PROTOS = {
     "vx_reg_stencil_workspace": [HI3],
     "vx_reg_stencil": [P, P, HI3, HF3, HF3, F32, F32, P, F32, F32, P, P, I64, P, P, P],
     "vx_grid_upsample": [P, HI3, P, HI3, P],
+    "vx_occupancy_workspace": [I64],
+    "vx_adam_torch": [P, I32, F32, F32, F32, P],
+    "vx_occupancy_points": [I32, HF3, HF3, P, P, P, I64, P, P],
+    "vx_occupancy_query": [P, I32, HF3, HF3, P, I64, P, P],
+    "vx_occupancy_update": [P, HI3, HF3, HF3, P, I32, HF3, HF3, P, P, P, I64, P, I32, F32, I32, F32, F32, P, P, P, I64,
+                            P, P],
 }
 _RESTYPES = {
     "vx_last_error": ctypes.c_char_p,
@@ -86,6 +92,7 @@ _RESTYPES = {
     "vx_vr_compact_blocks": I64,
     "vx_reg_stencil_blocks": I64,
     "vx_reg_stencil_workspace": I64,
+    "vx_occupancy_workspace": I64,
     "vx_geometry_backward_det_workspace": ctypes.c_size_t,
     "vx_hash_backward_det_workspace": ctypes.c_size_t,
 }
@@ -199,6 +206,14 @@ def iarr(v) -> ctypes.Array:
 def farr(v) -> ctypes.Array:
     v = [float(x) for x in v]
     return (ctypes.c_float * max(len(v), 1))(*v)
+
+
+class AdamSegment(ctypes.Structure):
+    """vx_adam_segment of the C header."""
+
+    _fields_ = [("param", ctypes.c_void_p), ("grad", ctypes.c_void_p), ("exp_avg", ctypes.c_void_p),
+                ("exp_avg_sq", ctypes.c_void_p), ("n", ctypes.c_int64), ("step", ctypes.c_int64),
+                ("lr", ctypes.c_float)]
 
 
 def ptr(t: Optional[torch.Tensor]):

@@ -61,6 +61,15 @@ __host__ inline Grid make_grid(const int32_t res[3], const float lo[3], const fl
   return g;
 }
 
+// Host check of a dense grid resolution: >= 2 per axis, fewer than 2^31 voxels (int32 indexing).
+inline int check_grid(const int32_t res[3]) {
+  VX_REQUIRE(res != nullptr, "res is null");
+  VX_REQUIRE(res[0] >= 2 && res[1] >= 2 && res[2] >= 2, "grid resolution must be >= 2 per axis (got %d,%d,%d)",
+             res[0], res[1], res[2]);
+  VX_REQUIRE((int64_t)res[0] * res[1] * res[2] < (int64_t(1) << 31), "grid has 2^31 or more voxels");
+  return VX_OK;
+}
+
 __device__ __forceinline__ int lin3(const Grid& g, int x, int y, int z) { return (x * g.ry + y) * g.rz + z; }
 __device__ __forceinline__ int gdim(const Grid& g, int a) { return a == 0 ? g.rx : (a == 1 ? g.ry : g.rz); }
 
@@ -275,6 +284,44 @@ __device__ __forceinline__ void gs_scatter(float* __restrict__ gg, const Grid& g
 }
 
 // Mark the 8 Eq.7 corners of a sample in a V_R bitmap (bit = linear index), skipping the
+
+// ---------------------------------------------------------------------------------------
+// Occupancy mask lookup, OccupancyGrid.is_occupied (rendering/occupancy_grid.py:122-147):
+// n = (p - min) / (max - min + 1e-8); occupied iff n in [0, 1] on every axis and
+// mask[int(clamp(n * R, 0, R - 1.0001))] is set.
+// ---------------------------------------------------------------------------------------
+struct Occ {
+  const uint8_t* mask;  // (R,R,R) bool, or nullptr for no modulation
+  int r;
+  float lo[3], den[3];
+};
+
+__device__ __forceinline__ bool occupied(const Occ& oc, float px, float py, float pz) {
+  const float p[3] = {px, py, pz};
+  int c[3];
+  bool inb = true;
+  const float hi = (float)((double)oc.r - 1.0001);
+#pragma unroll
+  for (int a = 0; a < 3; ++a) {
+    const float n = __fdiv_rn(__fsub_rn(p[a], oc.lo[a]), oc.den[a]);
+    inb = inb && (n >= 0.0f) && (n <= 1.0f);
+    const float s = fminf(fmaxf(__fmul_rn(n, (float)oc.r), 0.0f), hi);
+    c[a] = (int)s;
+  }
+  return inb && oc.mask[(c[0] * oc.r + c[1]) * oc.r + c[2]] != 0;
+}
+
+inline Occ make_occ(const uint8_t* mask, int r, const float lo[3], const float hi[3]) {
+  Occ oc;
+  oc.mask = mask;
+  oc.r = r;
+  for (int a = 0; a < 3; ++a) {
+    oc.lo[a] = mask ? lo[a] : 0.f;
+    oc.den[a] = mask ? (hi[a] - lo[a]) + 1e-8f : 1.f;
+  }
+  return oc;
+}
+
 // atomic when the bit is already set.
 __device__ __forceinline__ void mark_corners(uint32_t* __restrict__ bm, const Grid& g, const Eq7& e) {
 #pragma unroll

@@ -176,14 +176,6 @@ __global__ void __launch_bounds__(256) k_corners_weights(Grid g, const float* __
   }
 }
 
-static int check_grid(const int32_t res[3]) {
-  VX_REQUIRE(res != nullptr, "res is null");
-  VX_REQUIRE(res[0] >= 2 && res[1] >= 2 && res[2] >= 2, "grid resolution must be >= 2 per axis (got %d,%d,%d)",
-             res[0], res[1], res[2]);
-  VX_REQUIRE((int64_t)res[0] * res[1] * res[2] < (int64_t(1) << 31), "grid has 2^31 or more voxels");
-  return VX_OK;
-}
-
 static Grid grid_from_eps(const int32_t res[3], const float eps[3]) {
   const float lo[3] = {0.f, 0.f, 0.f}, hi[3] = {1.f, 1.f, 1.f};
   Grid g = make_grid(res, lo, hi);

@@ -9,28 +9,6 @@
 
 namespace vx {
 
-struct Occ {
-  const uint8_t* mask;  // (R,R,R) bool, or nullptr for no modulation
-  int r;
-  float lo[3], den[3];
-};
-
-// rendering/occupancy_grid.py:122-147
-__device__ __forceinline__ bool occupied(const Occ& oc, float px, float py, float pz) {
-  const float p[3] = {px, py, pz};
-  int c[3];
-  bool inb = true;
-  const float hi = (float)((double)oc.r - 1.0001);
-#pragma unroll
-  for (int a = 0; a < 3; ++a) {
-    const float n = __fdiv_rn(__fsub_rn(p[a], oc.lo[a]), oc.den[a]);
-    inb = inb && (n >= 0.0f) && (n <= 1.0f);
-    const float s = fminf(fmaxf(__fmul_rn(n, (float)oc.r), 0.0f), hi);
-    c[a] = (int)s;
-  }
-  return inb && oc.mask[(c[0] * oc.r + c[1]) * oc.r + c[2]] != 0;
-}
-
 // rendering/rays.py:102-128
 __device__ __forceinline__ void near_far(float ox, float oy, float oz, float dx, float dy, float dz, float radius,
                                          float& nearv, float& farv) {
@@ -371,17 +349,6 @@ __global__ void k_near_far(const float* __restrict__ o, const float* __restrict_
     nearv[i] = a;
     farv[i] = b;
   }
-}
-
-static Occ make_occ(const uint8_t* mask, int r, const float lo[3], const float hi[3]) {
-  Occ oc;
-  oc.mask = mask;
-  oc.r = r;
-  for (int a = 0; a < 3; ++a) {
-    oc.lo[a] = mask ? lo[a] : 0.f;
-    oc.den[a] = mask ? (hi[a] - lo[a]) + 1e-8f : 1.f;
-  }
-  return oc;
 }
 
 }  // namespace vx

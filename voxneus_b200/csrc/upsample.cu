@@ -1,6 +1,5 @@
 // Trilinear grid upsampling with align_corners=True (geometry/upsample.py:12-39, the
-// F.interpolate call of models/sdf_grid.py:183-195) and the sparse/dense grid Adam updates
-// (training/optimizer.py:32-116; adam_upd_kernel.cu of the reference extension).
+// F.interpolate call of models/sdf_grid.py:183-195).
 //
 // Upsampling is write-bound (a 128^3 -> 256^3 pass reads 8 MiB, L2-resident, and writes
 // 64 MiB): one thread per 4 consecutive z outputs, 16-byte stores when the row allows.
@@ -66,21 +65,6 @@ __global__ void __launch_bounds__(256) k_grid_upsample(const float* __restrict__
   }
 }
 
-template <bool kMasked>
-__global__ void __launch_bounds__(256) k_adam(float* __restrict__ p, const float* __restrict__ g, float* __restrict__ m,
-                                              float* __restrict__ v, int64_t n, float step_size, float b1, float b2,
-                                              float eps) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-    const float gi = g[i];
-    if (kMasked && gi == 0.0f) continue;
-    const float mi = b1 * m[i] + (1.0f - b1) * gi;
-    const float vi = b2 * v[i] + (1.0f - b2) * gi * gi;
-    m[i] = mi;
-    v[i] = vi;
-    p[i] -= step_size * mi / (sqrtf(vi) + eps);
-  }
-}
-
 }  // namespace vx
 
 using namespace vx;
@@ -103,34 +87,6 @@ int vx_grid_upsample(const float* src, const int32_t res_in[3], float* dst, cons
       src, res_in[0], res_in[1], res_in[2], dst, res_out[0], res_out[1], res_out[2], ax[0], ax[1], ax[2]);
   count_launches(1);
   return check_launch("grid_upsample");
-}
-
-static int adam_common(bool masked, float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n,
-                       int step, float beta1, float beta2, float lr, float eps, void* stream) {
-  VX_REQUIRE(n >= 0, "n < 0");
-  VX_REQUIRE(step >= 1, "step must be >= 1");
-  if (n == 0) return VX_OK;
-  VX_REQUIRE(param && grad && exp_avg && exp_avg_sq, "null pointer");
-  // adam_upd_kernel.cu: step_size = lr * sqrt(1 - b2^t) / (1 - b1^t), evaluated on the host
-  const float step_size = lr * sqrtf(1.0f - powf(beta2, (float)step)) / (1.0f - powf(beta1, (float)step));
-  if (masked)
-    k_adam<true><<<grid_for(n, 256, 8), 256, 0, (cudaStream_t)stream>>>(param, grad, exp_avg, exp_avg_sq, n, step_size,
-                                                                        beta1, beta2, eps);
-  else
-    k_adam<false><<<grid_for(n, 256, 8), 256, 0, (cudaStream_t)stream>>>(param, grad, exp_avg, exp_avg_sq, n,
-                                                                         step_size, beta1, beta2, eps);
-  count_launches(1);
-  return check_launch(masked ? "masked_adam_upd" : "adam_upd");
-}
-
-int vx_adam_upd(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, int step, float beta1,
-                float beta2, float lr, float eps, void* stream) {
-  return adam_common(false, param, grad, exp_avg, exp_avg_sq, n, step, beta1, beta2, lr, eps, stream);
-}
-
-int vx_masked_adam_upd(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n, int step,
-                       float beta1, float beta2, float lr, float eps, void* stream) {
-  return adam_common(true, param, grad, exp_avg, exp_avg_sq, n, step, beta1, beta2, lr, eps, stream);
 }
 
 }  // extern "C"

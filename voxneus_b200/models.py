@@ -33,6 +33,16 @@ class GridSDF:
         return self.grid_module.query_sdf(p).squeeze(-1)
 
 
+def _dense_grid_of(fn) -> Optional["DenseSDFGrid"]:
+    """The DenseSDFGrid behind a query_sdf bound method or a GridSDF, else None."""
+    if isinstance(fn, GridSDF):
+        return fn.grid_module
+    owner = getattr(fn, "__self__", None)
+    if isinstance(owner, DenseSDFGrid) and getattr(fn, "__func__", None) is DenseSDFGrid.query_sdf:
+        return owner
+    return None
+
+
 class DenseSDFGrid(nn.Module):
     """Dense FP32 SDF grid (models/sdf_grid.py:24-199)."""
 
@@ -239,6 +249,41 @@ class OccupancyGrid(nn.Module):
     def occupied_percentage(self) -> float:
         return float(self.occupancy_mask.float().mean().item() * 100.0)
 
+    @torch.no_grad()
+    def update_from_sdf(self, query_sdf_fn, s_val, subsample_ratio: float = 0.25, generator=None) -> None:
+        """EMA update with the NeuS2 logistic density (rendering/occupancy_grid.py:62-119).
+
+        Draws max(int(R^3 * subsample_ratio), 1024) cells with three torch.randint calls (x, y, z,
+        the reference's order, from `generator` or the default generator of the grid's device).
+        query_sdf_fn: a DenseSDFGrid's query_sdf (or its GridSDF) is evaluated inside the kernel;
+        any other callable (N,3) -> (N,1) or (N,) is called on the cell centres. s_val: s as a
+        tensor or number, or a SingleVarianceNetwork (s derived from its parameter on the device).
+        """
+        dev = self.density_grid.device
+        res = self.resolution
+        n = max(int(res * res * res * subsample_ratio), 1024)
+        idx = [torch.randint(0, res, (n,), device=dev, generator=generator) for _ in range(3)]
+        lo, hi = self._bounds
+        if isinstance(s_val, SingleVarianceNetwork):
+            s, is_var, s_max = s_val.variance.detach(), True, s_val._s_max
+        else:
+            s, is_var, s_max = torch.as_tensor(s_val).detach().to(device=dev, dtype=torch.float32), False, 0.0
+        grid_mod = _dense_grid_of(query_sdf_fn)
+        if grid_mod is not None:
+            kw = dict(grid=grid_mod.grid.detach(), grid_bounds=grid_mod.bounds())
+        else:
+            pts = ops.occupancy_points(res, lo, hi, idx)
+            kw = dict(sdf_values=query_sdf_fn(pts).detach().reshape(-1).float().contiguous())
+        ops.occupancy_update(self.density_grid, self.occupancy_mask, idx, lo, hi, s, is_var, s_max,
+                             self.total_updates == 0, self.decay, self.threshold, **kw)
+        self.total_updates += 1
+
+    @torch.no_grad()
+    def is_occupied(self, pts_world: torch.Tensor) -> torch.Tensor:
+        """(..., 3) world points -> (...) bool (rendering/occupancy_grid.py:121-147)."""
+        lo, hi = self._bounds
+        return ops.occupancy_query(self.occupancy_mask, lo, hi, pts_world)
+
 
 class VoxNeuS(nn.Module):
     """Assembled model (models/voxneus.py:21-260) with the fused render."""
@@ -265,6 +310,13 @@ class VoxNeuS(nn.Module):
     @property
     def std(self):
         return self.variance_net.std
+
+    @torch.no_grad()
+    def update_occupancy_grid(self, subsample_ratio: float = 0.25, generator=None) -> None:
+        """Periodic occupancy refresh from the SDF grid and the current s (models/voxneus.py:104-113);
+        s is derived from the variance parameter inside the kernel."""
+        self.occupancy_grid.update_from_sdf(self.sdf_grid.query_sdf, self.variance_net, subsample_ratio,
+                                            generator=generator)
 
     def draw_sampler_randoms(self, n_rays: int, n_samples: int, n_importance: int, steps: int, device,
                              generator=None):

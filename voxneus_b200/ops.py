@@ -827,6 +827,63 @@ def vr_compact(bitmap, grid, res, xyz_min, xyz_max, relax_radius, band, counts, 
     return verts, lin
 
 
+def occupancy_points(res: int, xyz_min, xyz_max, idx: Sequence[torch.Tensor]) -> torch.Tensor:
+    """World-space centres (n,3) of the drawn cells of a res^3 occupancy grid."""
+    ix, iy, iz = (check_tensor(t, "idx", dtype=torch.int64) for t in idx)
+    n = ix.numel()
+    if iy.numel() != n or iz.numel() != n:
+        raise RuntimeError("idx_x, idx_y and idx_z must have the same length")
+    pts = torch.empty(n, 3, dtype=torch.float32, device=ix.device)
+    call("vx_occupancy_points", int(res), f3(xyz_min), f3(xyz_max), ptr(ix), ptr(iy), ptr(iz), n, ptr(pts),
+         stream_ptr(ix.device))
+    return pts
+
+
+def occupancy_query(mask: torch.Tensor, xyz_min, xyz_max, pts: torch.Tensor) -> torch.Tensor:
+    """OccupancyGrid.is_occupied: (..., 3) world points -> (...) bool."""
+    check_tensor(mask, "occupancy_mask", dtype=torch.bool)
+    lead = pts.shape[:-1]
+    p = check_tensor(pts.reshape(-1, 3).float().contiguous(), "pts")
+    out = torch.empty(p.shape[0], dtype=torch.bool, device=p.device)
+    call("vx_occupancy_query", ptr(mask), int(mask.shape[0]), f3(xyz_min), f3(xyz_max), ptr(p), p.shape[0], ptr(out),
+         stream_ptr(p.device))
+    return out.reshape(lead)
+
+
+def occupancy_update(density: torch.Tensor, mask: torch.Tensor, idx: Sequence[torch.Tensor], xyz_min, xyz_max,
+                     s: torch.Tensor, s_is_variance: bool, s_max: float, first: bool, decay: float, threshold: float,
+                     grid: Optional[torch.Tensor] = None, grid_bounds=None, sdf_values: Optional[torch.Tensor] = None):
+    """EMA update of density (R,R,R) float32 and mask (R,R,R) bool at the drawn cells, in place."""
+    res = int(density.shape[0])
+    check_tensor(density, "density_grid")
+    check_tensor(mask, "occupancy_mask", dtype=torch.bool)
+    if list(density.shape) != [res] * 3 or list(mask.shape) != [res] * 3:
+        raise RuntimeError("density_grid and occupancy_mask must both be (R, R, R)")
+    ix, iy, iz = (check_tensor(t, "idx", dtype=torch.int64) for t in idx)
+    n = ix.numel()
+    if iy.numel() != n or iz.numel() != n:
+        raise RuntimeError("idx_x, idx_y and idx_z must have the same length")
+    s = check_tensor(s.reshape(1), "s")
+    dev = density.device
+    if grid is not None:
+        gres = _grid3(grid)
+        glo, ghi = grid_bounds
+        gargs = (ptr(grid), i3(gres), f3(glo), f3(ghi), None)
+    else:
+        sdf_values = check_tensor(sdf_values.reshape(-1), "sdf_values")
+        if sdf_values.numel() != n:
+            raise RuntimeError(f"query_sdf_fn returned {sdf_values.numel()} values for {n} points")
+        gargs = (None, None, None, None, ptr(sdf_values))
+    need = int(L.query("vx_occupancy_workspace", n))
+    sc = Scratch.get(dev)
+    ws = getattr(sc, "occ_ws", None)
+    if ws is None or ws.numel() < need:
+        sc.occ_ws = ws = torch.empty(max(need, 16), dtype=torch.uint8, device=dev)
+    call("vx_occupancy_update", *gargs, res, f3(xyz_min), f3(xyz_max), ptr(ix), ptr(iy), ptr(iz), n, ptr(s),
+         int(bool(s_is_variance)), float(s_max), int(bool(first)), float(decay), float(threshold), ptr(density),
+         ptr(mask), ptr(ws), ws.numel(), None, stream_ptr(dev))
+
+
 def reg_list(kind: str, grid3, verts, eps, weight, grad_out):
     """List-form eikonal / curvature (the reference kernels' interface); returns the loss tensor."""
     res = _grid3(grid3)
@@ -871,6 +928,24 @@ def grid_upsample(grid: torch.Tensor, new_res) -> torch.Tensor:
     dst = torch.empty(*lead, *res_out, device=src.device)
     call("vx_grid_upsample", ptr(src), i3(res_in), ptr(dst), i3(res_out), stream_ptr(src.device))
     return dst
+
+
+def adam_torch(segments, beta1: float, beta2: float, eps: float):
+    """torch.optim.Adam's update over [(param, grad, exp_avg, exp_avg_sq, step, lr), ...] in place."""
+    import ctypes
+
+    if not segments:
+        return
+    arr = (L.AdamSegment * len(segments))()
+    dev = segments[0][0].device
+    for k, (p, g, m, v, step, lr) in enumerate(segments):
+        for t, nm in ((p, "param"), (g, "grad"), (m, "exp_avg"), (v, "exp_avg_sq")):
+            check_tensor(t, nm, device=dev)
+            if t.numel() != p.numel():
+                raise RuntimeError(f"{nm} has {t.numel()} elements, param has {p.numel()}")
+        arr[k] = L.AdamSegment(p.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), p.numel(), int(step), float(lr))
+    call("vx_adam_torch", ctypes.cast(arr, ctypes.c_void_p), len(segments), float(beta1), float(beta2), float(eps),
+         stream_ptr(dev))
 
 
 def adam_update(param, grad, exp_avg, exp_avg_sq, step, beta1, beta2, lr, eps, masked):

@@ -4,8 +4,9 @@
 fused render (sampler, geometry, appearance, MLP, compositing), Huber loss, backward through
 the hand-written adjoints (with the k=5 s-gradient rule applied in-kernel), V_R from the
 render's corner bitmap, the fused eikonal + curvature stencil into grid.grad, and the optimizer
-steps (masked grid Adam kernel; torch's fused Adam for the hash table, MLP and variance). No
-host synchronisation unless the s amplification is active (its LR rule needs the flag).
+steps (masked grid Adam kernel; one multi-tensor Adam launch for the hash table, MLP and
+variance). No host synchronisation unless the s amplification is active (its LR rule needs the
+flag).
 """
 
 from __future__ import annotations
@@ -59,15 +60,55 @@ class SparseGridAdam(Optimizer):
         return None
 
 
+class FusedAdam(Optimizer):
+    """torch.optim.Adam (the network optimizer of training/optimizer.py:119-154) with every
+    parameter of every group updated by one kernel launch per 8 tensors (`vx_adam_torch`).
+
+    Same update, hyper-parameters and state names as torch.optim.Adam (step, exp_avg,
+    exp_avg_sq); parameters whose grad is None are skipped, as there. No weight decay or amsgrad.
+    """
+
+    def __init__(self, params, lr: float = 1e-3, betas=(0.9, 0.999), eps: float = 1e-8, weight_decay: float = 0.0,
+                 amsgrad: bool = False):
+        if weight_decay != 0.0 or amsgrad:
+            raise ValueError("weight decay and amsgrad are not on the fused Adam kernel")
+        super().__init__(params, dict(lr=lr, betas=betas, eps=eps, weight_decay=weight_decay, amsgrad=amsgrad))
+
+    @torch.no_grad()
+    def step(self, closure=None):
+        loss = None
+        if closure is not None:
+            with torch.enable_grad():
+                loss = closure()
+        batches: Dict[tuple, list] = {}
+        for group in self.param_groups:
+            b1, b2 = group["betas"]
+            for p in group["params"]:
+                if p.grad is None:
+                    continue
+                if p.grad.is_sparse:
+                    raise RuntimeError("FusedAdam does not support sparse gradients")
+                st = self.state[p]
+                if not st:
+                    st["step"] = 0
+                    st["exp_avg"] = torch.zeros_like(p, memory_format=torch.contiguous_format)
+                    st["exp_avg_sq"] = torch.zeros_like(p, memory_format=torch.contiguous_format)
+                st["step"] += 1
+                batches.setdefault((float(b1), float(b2), float(group["eps"])), []).append(
+                    (p, p.grad.contiguous(), st["exp_avg"], st["exp_avg_sq"], st["step"], group["lr"]))
+        for (b1, b2, eps), segs in batches.items():
+            ops.adam_torch(segs, b1, b2, eps)
+        return loss
+
+
 def create_optimizer(model: VoxNeuS, lr_sdf=0.1, lr_hash=1e-2, lr_mlp=1e-3, lr_variance=1e-2, use_sparse_sdf=True):
     """Optimizer suite (training/optimizer.py:119-154)."""
     sdf_opt = (SparseGridAdam([model.sdf_grid.grid], lr=lr_sdf, betas=(0.9, 0.99)) if use_sparse_sdf
                else torch.optim.Adam([model.sdf_grid.grid], lr=lr_sdf, betas=(0.9, 0.99)))
-    fused = model.sdf_grid.grid.is_cuda
-    net_opt = torch.optim.Adam([{"params": model.radiance_hash.parameters(), "lr": lr_hash},
-                                {"params": model.radiance_mlp.parameters(), "lr": lr_mlp},
-                                {"params": model.variance_net.parameters(), "lr": lr_variance}],
-                               betas=(0.9, 0.999), eps=1e-8, fused=fused)
+    net_opt = FusedAdam([{"params": model.radiance_hash.parameters(), "lr": lr_hash},
+                         {"params": model.radiance_mlp.parameters(), "lr": lr_mlp},
+                         {"params": model.variance_net.parameters(), "lr": lr_variance}],
+                        betas=(0.9, 0.999), eps=1e-8)
     return {"sdf_optimizer": sdf_opt, "net_optimizer": net_opt}
 
 
@@ -78,7 +119,8 @@ class FusedTrainer:
                  w_curv: float = 5e-4, band_voxels: Optional[float] = None, relax_radius: float = 1.2,
                  amplify_k: float = 5.0, s_warmup_steps: int = 5000, total_steps: int = 40000, lr_sdf: float = 0.1,
                  lr_hash: float = 0.01, lr_mlp: float = 0.001, lr_variance: float = 0.0005, up_sample_steps: int = 4,
-                 huber_delta: float = 0.1, optimize: bool = True, exchange=None):
+                 huber_delta: float = 0.1, optimize: bool = True, exchange=None,
+                 occupancy_update_interval: int = 16, occupancy_seed: int = 0):
         self.model = model
         self.exchange = exchange  # dataparallel.GradExchange for world_size > 1
         self.sampler = sampler or RaySampler(64, 64, perturb=True)
@@ -102,6 +144,14 @@ class FusedTrainer:
         self.counts = torch.zeros(4, dtype=torch.int64, device=dev)
         self.reg_losses = torch.zeros(2, device=dev)
         self.amp_flag = torch.zeros(1, dtype=torch.int32, device=dev)
+        # training/trainer.py:171-173: occupancy refresh every `occupancy_update_interval` steps
+        # (0 disables). Data-parallel ranks draw the cells from one shared seed so that their
+        # masks stay identical; a single process draws from the default generator.
+        self.occupancy_update_interval = int(occupancy_update_interval)
+        self.occ_generator = None
+        if exchange is not None:
+            self.occ_generator = torch.Generator(device=dev)
+            self.occ_generator.manual_seed(int(occupancy_seed))
 
     def step(self, rays_o, rays_d, target, step: int = 0, randoms=None) -> Dict[str, torch.Tensor]:
         m = self.model
@@ -112,6 +162,8 @@ class FusedTrainer:
         if not self.optimize:
             for p in m.parameters():
                 p.grad = None
+        if self.occupancy_update_interval > 0 and step % self.occupancy_update_interval == 0:
+            m.update_occupancy_grid(subsample_ratio=0.25, generator=self.occ_generator)
         self.bitmap.zero_()
         self.counts.zero_()
         amp_k = self.amplify_k if step >= self.s_warmup_steps else 0.0
