@@ -6,11 +6,12 @@
 //     masked: elements whose gradient is exactly 0 keep p, m and v.
 //   torch formula (torch.optim.Adam, the network optimizer of training/optimizer.py:119-154):
 //       p -= (lr / (1 - b1^t)) * m / (sqrt(v) / sqrt(1 - b2^t) + eps)
+//     (the division by sqrt(1 - b2^t) is a multiplication by its reciprocal, formed on the host)
 //   both with m = b1 m + (1 - b1) g, v = b2 v + (1 - b2) g^2.
 //
 // HBM-bound streaming: 16 bytes read and 12 written per element (4 read for a masked element
 // whose gradient is 0). Each thread keeps two float4 chunks of every operand in flight (the
-// loads of both are issued before either update), so one wave of 3 blocks per SM covers the
+// loads of both are issued before either update), so one wave of resident blocks covers the
 // HBM latency; a scalar loop takes the tail and any segment whose pointers are not 16-byte
 // aligned. One launch updates up to kMaxSegs tensors, each with its own step size.
 #include "common.cuh"
@@ -27,7 +28,7 @@ struct AdamSeg {
   float* v;
   int64_t n;
   float step_size;
-  float bc2_sqrt;  // sqrt(1 - b2^t), torch formula only
+  float inv_bc2_sqrt;  // 1 / sqrt(1 - b2^t), torch formula only
   int vec;         // all four pointers 16-byte aligned
 };
 
@@ -43,7 +44,7 @@ __device__ __forceinline__ void adam1(float& p, float g, float& m, float& v, con
   m = a.b1 * m + (1.0f - a.b1) * g;
   v = a.b2 * v + (1.0f - a.b2) * g * g;
   if (kTorch)
-    p -= s.step_size * m / (sqrtf(v) / s.bc2_sqrt + a.eps);
+    p -= s.step_size * m / (sqrtf(v) * s.inv_bc2_sqrt + a.eps);
   else
     p -= s.step_size * m / (sqrtf(v) + a.eps);
 }
@@ -125,14 +126,26 @@ __global__ void __launch_bounds__(256) k_adam(const AdamArgs a) {
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
+// One wave: as many blocks as stay resident on the 148 SMs (register-limited), queried once.
+template <bool kMasked, bool kTorch>
+unsigned adam_blocks(int64_t total) {
+  static int per_sm = 0;
+  if (per_sm == 0) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_adam<kMasked, kTorch>, 256, 0) != cudaSuccess || nb < 1)
+      nb = 2;
+    per_sm = nb;
+  }
+  return grid_for((total + 7) / 8, 256, per_sm);
+}
+
 int launch_adam(const AdamArgs& a, bool masked, bool torch_formula, int64_t total, cudaStream_t stream) {
-  const unsigned blocks = grid_for((total + 7) / 8, 256, 3);  // 68 registers: 3 blocks of 256 per SM
   if (torch_formula)
-    k_adam<false, true><<<blocks, 256, 0, stream>>>(a);
+    k_adam<false, true><<<adam_blocks<false, true>(total), 256, 0, stream>>>(a);
   else if (masked)
-    k_adam<true, false><<<blocks, 256, 0, stream>>>(a);
+    k_adam<true, false><<<adam_blocks<true, false>(total), 256, 0, stream>>>(a);
   else
-    k_adam<false, false><<<blocks, 256, 0, stream>>>(a);
+    k_adam<false, false><<<adam_blocks<false, false>(total), 256, 0, stream>>>(a);
   count_launches(1);
   return check_launch(torch_formula ? "adam_torch" : (masked ? "masked_adam_upd" : "adam_upd"));
 }
@@ -205,7 +218,7 @@ int vx_adam_torch(const vx_adam_segment* segs, int n_segs, float beta1, float be
       const double bc1 = 1.0 - pow((double)beta1, (double)in.step);
       const double bc2 = 1.0 - pow((double)beta2, (double)in.step);
       s.step_size = (float)((double)in.lr / bc1);
-      s.bc2_sqrt = (float)sqrt(bc2);
+      s.inv_bc2_sqrt = (float)(1.0 / sqrt(bc2));
       s.vec = aligned16(in.param) && aligned16(in.grad) && aligned16(in.exp_avg) && aligned16(in.exp_avg_sq);
       total += in.n;
     }

@@ -9,13 +9,15 @@
 // writes nothing on this part, so every operand is staged with its contraction dimension
 // contiguous). A 16-byte chunk holds 4 consecutive K elements of one row:
 //   X    (128 sample rows, K = features): chunk (m, 4f..4f+3) at (f*16 + m/8)*128 + (m%8)*16
-//   W0   (64 hidden rows,  K = features): element (n, k) at ((k/4)*8 + n/8)*128 + (n%8)*16 + (k%4)*4
-//   W0^T (64 feature rows, K = hidden), DZ (128 sample rows, K = hidden), and X^T / DZ^T (feature /
-//   hidden rows, K = the tile's samples) likewise.
-// GEMMs (M = 128 rows in TMEM lanes, N = 64 f32 columns):
-//   Z   = X W0^T         A = X,                  B = W0     (K = 56 features, 7 steps)
-//   dX  = DZ W0          A = DZ,                 B = W0^T   (K = 64 hidden, 8 steps)
-//   dW0 = [DZh;DZl]^T X  A = [DZ_hi^T; DZ_lo^T], B = X^T    (K = 128 samples, 16 steps)
+//   W0   [hi; lo] (128 rows: hidden unit n's hi part in row n, its lo part in row 64 + n, K =
+//        features): element (r, k) at ((k/4)*16 + r/8)*128 + (r%8)*16 + (k%4)*4
+//   W0^T [hi; lo] (128 feature rows, K = hidden), DZ (128 sample rows, K = hidden), and X^T [hi; lo]
+//   / DZ^T [hi; lo] (128 rows, K = the tile's samples) likewise.
+// The stacked hi/lo operands let one N = 128 MMA form two of the three products:
+//   Z   = X W0^T   A = X_hi, B = [W_hi; W_lo] (N = 128) + A = X_lo, B = W_hi (N = 64), K = 56 in 7
+//                  steps; Z = columns [0, 64) + [64, 128)
+//   dX  = DZ W0    the same with A = DZ_hi / DZ_lo, B = W0^T [hi; lo], K = 64 in 8 steps
+//   dW0 = [DZh;DZl]^T X   A = DZ^T [hi; lo], B = X^T [hi; lo] (N = 128), K = 128 samples in 16 steps
 // The forward writes the colours (and, for the adjoint, the 52-float input rows); the adjoint
 // recomputes Z with the identical MMA sequence, writes dL/d(hash) and dL/d(normal), accumulates
 // dW0 (and db0 through a ones column) in TMEM across its tiles and dW1/db1 in registers, and
@@ -34,7 +36,7 @@ constexpr int WG = NH * KP + NO * NH + NH + NO;  // per-block weight-gradient pa
 constexpr uint32_t kWaitLimit = 1u << 22;       // mbarrier polls before a tile gives up
 
 constexpr uint32_t kXBytes = 16 * 16 * 128;  // one tf32 part of X (or DZ)
-constexpr uint32_t kWBytes = 16 * 8 * 128;   // one tf32 part of W0
+constexpr uint32_t kWBytes = 16 * 16 * 128;  // W0 (or W0^T) as [hi; lo]
 
 __device__ int g_tc_timeouts = 0;
 
@@ -46,8 +48,9 @@ struct MlpW {
 };
 
 __device__ __forceinline__ uint32_t x_off(int f, int m) { return (uint32_t)((f * 16 + (m >> 3)) * 128 + (m & 7) * 16); }
-__device__ __forceinline__ uint32_t w_off(int n, int k) {
-  return (uint32_t)(((k >> 2) * 8 + (n >> 3)) * 128 + (n & 7) * 16 + (k & 3) * 4);
+// row r of [W_hi; W_lo] (r < 64: hi of hidden unit r, else lo of hidden unit r - 64), feature k
+__device__ __forceinline__ uint32_t w_off(int r, int k) {
+  return (uint32_t)(((k >> 2) * 16 + (r >> 3)) * 128 + (r & 7) * 16 + (k & 3) * 4);
 }
 
 __device__ __forceinline__ void st_split4(uint8_t* hi, uint8_t* lo, uint32_t off, float a, float b, float c, float d) {
@@ -60,16 +63,16 @@ __device__ __forceinline__ void st_split4(uint8_t* hi, uint8_t* lo, uint32_t off
   *reinterpret_cast<float4*>(lo + off) = l;
 }
 
-// W0 as hi/lo tf32 (features 51..63 zero), b0, W1, b1; X feature chunks 13..15 (columns 52..63,
+// W0 as [hi; lo] tf32 (features 51..63 zero), b0, W1, b1; X feature chunks 13..15 (columns 52..63,
 // never written by the tiles) zeroed.
-__device__ void stage_weights(const MlpW& w, uint8_t* WH, uint8_t* WL, uint8_t* XH, uint8_t* XL, float* B0,
-                              float* W1s, float* B1, int tid, int nt) {
+__device__ void stage_weights(const MlpW& w, uint8_t* W2, uint8_t* XH, uint8_t* XL, float* B0, float* W1s, float* B1,
+                              int tid, int nt) {
   for (int e = tid; e < NH * 64; e += nt) {
     const int n = e >> 6, k = e & 63;
     float h, l;
     tc::split_tf32(k < KIN ? w.W0[n * KIN + k] : 0.0f, h, l);
-    *reinterpret_cast<float*>(WH + w_off(n, k)) = h;
-    *reinterpret_cast<float*>(WL + w_off(n, k)) = l;
+    *reinterpret_cast<float*>(W2 + w_off(n, k)) = h;
+    *reinterpret_cast<float*>(W2 + w_off(NH + n, k)) = l;
   }
   for (int e = tid; e < 3 * TM; e += nt) {
     const uint32_t off = x_off(13 + e / TM, e % TM);
@@ -121,17 +124,35 @@ __device__ __forceinline__ void store_row_chunks(const float4 v[7], bool valid, 
   }
 }
 
-// Z = X W0^T into TMEM columns [tz, tz + 64), issued by one thread (same sequence in both passes).
-__device__ __forceinline__ void issue_z(uint32_t tz, uint32_t xh, uint32_t xl, uint32_t wh, uint32_t wl) {
-  constexpr uint32_t id = tc::idesc_tf32(TM, NH, false, false);
+constexpr uint32_t kId128 = tc::idesc_tf32(TM, 2 * NH, false, false);
+constexpr uint32_t kId64 = tc::idesc_tf32(TM, NH, false, false);
+
+// A [hi | lo] K-major operand times a stacked [hi; lo] B: columns [t, t + 64) receive
+// A_hi B_hi + A_lo B_hi and [t + 64, t + 128) receive A_hi B_lo (one N = 128 and one N = 64 MMA per
+// 8-wide K step; the result is the sum of the two column halves). Issued by one thread.
+__device__ __forceinline__ void issue_split(uint32_t t, uint32_t ah0, uint32_t al0, uint32_t b0, int ksteps) {
 #pragma unroll 1
-  for (int ks = 0; ks < 7; ++ks) {
-    const uint64_t ah = tc::sdesc(xh + ks * 4096, 2048, 128), al = tc::sdesc(xl + ks * 4096, 2048, 128);
-    const uint64_t bh = tc::sdesc(wh + ks * 2048, 1024, 128), bl = tc::sdesc(wl + ks * 2048, 1024, 128);
-    tc::mma_tf32(tz, ah, bh, id, ks > 0);
-    tc::mma_tf32(tz, ah, bl, id, true);
-    tc::mma_tf32(tz, al, bh, id, true);
+  for (int ks = 0; ks < ksteps; ++ks) {
+    const uint64_t ah = tc::sdesc(ah0 + ks * 4096, 2048, 128), al = tc::sdesc(al0 + ks * 4096, 2048, 128);
+    const uint64_t b = tc::sdesc(b0 + ks * 4096, 2048, 128);
+    tc::mma_tf32(t, ah, b, kId128, ks > 0);
+    tc::mma_tf32(t, al, b, kId64, true);
   }
+}
+
+// Z = X W0^T into TMEM columns [tz, tz + 128) as two halves to add (same sequence in both passes).
+__device__ __forceinline__ void issue_z(uint32_t tz, uint32_t xh, uint32_t xl, uint32_t w2) {
+  issue_split(tz, xh, xl, w2, 7);
+}
+
+// 32 columns of a split result: TMEM columns [col, col + 32) + [col + 64, col + 96) of this warp's lanes
+__device__ __forceinline__ void tmem_ld_sum32(uint32_t taddr, float v[32]) {
+  float u[32];
+  tc::tmem_ld32(taddr, v);
+  tc::tmem_ld32(taddr + 64, u);
+  tc::tmem_wait_ld();
+#pragma unroll
+  for (int j = 0; j < 32; ++j) v[j] += u[j];
 }
 
 // This thread's half of the colour pre-activation: hidden units 32*hh..32*hh+31 of sample lane.
@@ -167,23 +188,22 @@ __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* 
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* XH = smem;
   uint8_t* XL = XH + kXBytes;
-  uint8_t* WH = XL + kXBytes;
-  uint8_t* WL = WH + kWBytes;
-  float* B0 = reinterpret_cast<float*>(WL + kWBytes);
+  uint8_t* W2 = XL + kXBytes;
+  float* B0 = reinterpret_cast<float*>(W2 + kWBytes);
   float* W1s = B0 + NH;
   float* B1 = W1s + NO * NH;
   float* RED = B1 + 4;  // [2][TM][4]
   uint64_t* bar = reinterpret_cast<uint64_t*>(RED + 2 * TM * 4);
   uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bar + 1);
   const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31, q = wid & 3, hh = wid >> 2;
-  stage_weights(w, WH, WL, XH, XL, B0, W1s, B1, tid, blockDim.x);
+  stage_weights(w, W2, XH, XL, B0, W1s, B1, tid, blockDim.x);
   if (tid == 0) tc::mbar_init(bar, 1);
-  if (wid == 0) tc::tmem_alloc(s_taddr, 64);
+  if (wid == 0) tc::tmem_alloc(s_taddr, 128);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
   const uint32_t tbase = *s_taddr;
-  const uint32_t xh = tc::smem_u32(XH), xl = tc::smem_u32(XL), wh = tc::smem_u32(WH), wl = tc::smem_u32(WL);
+  const uint32_t xh = tc::smem_u32(XH), xl = tc::smem_u32(XL), w2 = tc::smem_u32(W2);
   const uint32_t mask = (1u << a.log2T) - 1u;
   const size_t T = (size_t)1 << a.log2T;
   uint32_t phase = 0;
@@ -261,7 +281,7 @@ __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* 
     __syncthreads();
     if (tid == 0) {
       tc::fence_after_sync();
-      issue_z(tbase, xh, xl, wh, wl);
+      issue_z(tbase, xh, xl, w2);
       tc::commit(bar);
     }
     if (!kHashIn && t + gridDim.x < ntiles)  // next tile's rows fly during the MMA and the epilogue
@@ -274,8 +294,7 @@ __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* 
     }
     tc::fence_after_sync();
     float z[32];
-    tc::tmem_ld32(tbase + ((uint32_t)(32 * q) << 16) + 32 * hh, z);
-    tc::tmem_wait_ld();
+    tmem_ld_sum32(tbase + ((uint32_t)(32 * q) << 16) + 32 * hh, z);
     float p0, p1, p2;
     colour_partial(z, hh, B0, W1s, p0, p1, p2);
     float* r = RED + (hh * TM + 32 * q + lane) * 4;
@@ -294,10 +313,10 @@ __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* 
   }
   tc::fence_before_sync();
   __syncthreads();
-  if (wid == 0) tc::tmem_dealloc(tbase, 64);
+  if (wid == 0) tc::tmem_dealloc(tbase, 128);
 }
 
-constexpr size_t kFwdSmem = 2 * kXBytes + 2 * kWBytes + sizeof(float) * (NH + NO * NH + 4 + 2 * TM * 4) + 16;
+constexpr size_t kFwdSmem = 2 * kXBytes + kWBytes + sizeof(float) * (NH + NO * NH + 4 + 2 * TM * 4) + 16;
 
 // Adjoint. d_out (P,3) -> d_hash (P,32), d_normal (P,3), per-block weight-gradient partials
 // [dW0 (64 x 52) | dW1 (3 x 64) | db0 (64) | db1 (3)]. tcgen05 kind::tf32 takes K-major operands
@@ -305,9 +324,9 @@ constexpr size_t kFwdSmem = 2 * kXBytes + 2 * kWBytes + sizeof(float) * (NH + NO
 // are staged) and DZ^T, whose scalar stores are bank-conflict free because their 16-byte K chunks
 // of 4 samples sit 1040 / 2064 bytes apart (one 16-byte pad per chunk slab).
 // Per tile: stage rows -> Z MMA -> epilogue (colours, dO, dW1 in registers, DZ) -> dX MMA ->
-// DZ^T -> dW0 MMA (overlapping the dX readout). TMEM columns: Z [0,64), dX [64,128),
-// dW0 = [DZ_hi | DZ_lo]^T X_hi in [128,192) and x X_lo in [192,256).
-constexpr uint32_t kXtSlab = 8 * 128 + 16;    // X^T: 4 samples x 64 feature rows
+// DZ^T -> dW0 MMA (overlapping the dX readout). TMEM columns: Z, then dX, in [0,128) (two halves
+// each); dW0 = [DZ_hi | DZ_lo]^T X_hi in [128,192) and x X_lo in [192,256).
+constexpr uint32_t kXtSlab = 16 * 128 + 16;   // X^T: 4 samples x 128 rows (features hi | features lo)
 constexpr uint32_t kDztSlab = 16 * 128 + 16;  // DZ^T: 4 samples x 128 rows (hidden hi | hidden lo)
 constexpr uint32_t kXtBytes = 32 * kXtSlab;
 constexpr uint32_t kR1Bytes = 66560;          // X (hi, lo) -> DZ (hi, lo) -> DZ^T, one at a time
@@ -318,9 +337,10 @@ __device__ __forceinline__ uint32_t xt_off(int f, int m) {
 __device__ __forceinline__ uint32_t dzt_off(int r, int m) {
   return (uint32_t)((m >> 2) * kDztSlab + (r >> 3) * 128 + (r & 7) * 16 + (m & 3) * 4);
 }
-// W0^T (feature rows f, hidden K): element (f, n) at (n/4)*1024 + (f/8)*128 + (f%8)*16 + (n%4)*4
+// W0^T [hi; lo] (row f < 64: hi of feature f, else lo of feature f - 64; hidden K): element (f, n)
+// at (n/4)*2048 + (f/8)*128 + (f%8)*16 + (n%4)*4
 __device__ __forceinline__ uint32_t wt_off(int f, int n) {
-  return (uint32_t)((n >> 2) * 1024 + (f >> 3) * 128 + (f & 7) * 16 + (n & 3) * 4);
+  return (uint32_t)((n >> 2) * 2048 + (f >> 3) * 128 + (f & 7) * 16 + (n & 3) * 4);
 }
 
 __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__ X, int64_t ldx, int xvec, int64_t P,
@@ -328,13 +348,10 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
                                                       float* __restrict__ d_hash, float* __restrict__ d_normal,
                                                       float* __restrict__ partials) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  uint8_t* WH = smem;
-  uint8_t* WL = WH + kWBytes;
-  uint8_t* WTH = WL + kWBytes;
-  uint8_t* WTL = WTH + kWBytes;
-  uint8_t* XTH = WTL + kWBytes;
-  uint8_t* XTL = XTH + kXtBytes;
-  uint8_t* R1 = XTL + kXtBytes;
+  uint8_t* W2 = smem;
+  uint8_t* WT2 = W2 + kWBytes;
+  uint8_t* XT2 = WT2 + kWBytes;
+  uint8_t* R1 = XT2 + kXtBytes;
   float* RED = reinterpret_cast<float*>(R1 + kR1Bytes);  // [2][TM][4]
   float* W1s = RED + 2 * TM * 4;
   float* B0 = W1s + NO * NH;
@@ -343,20 +360,20 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bar + 1);
   const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31, q = wid & 3, hh = wid >> 2;
   const int m = 32 * q + lane;  // this thread's sample in the tile (its TMEM lane)
-  // W0 (hidden rows) for Z, W0^T (feature rows) for dX, b0, W1, b1; X^T rows 52..63 zero
+  // W0 [hi; lo] (hidden rows) for Z, W0^T [hi; lo] (feature rows) for dX, b0, W1, b1; X^T feature
+  // rows 52..63 (hi and lo) zero
   for (int e = tid; e < NH * 64; e += blockDim.x) {
     const int n = e >> 6, k = e & 63;
     float h, l;
     tc::split_tf32(k < KIN ? w.W0[n * KIN + k] : 0.0f, h, l);
-    *reinterpret_cast<float*>(WH + w_off(n, k)) = h;
-    *reinterpret_cast<float*>(WL + w_off(n, k)) = l;
-    *reinterpret_cast<float*>(WTH + wt_off(k, n)) = h;
-    *reinterpret_cast<float*>(WTL + wt_off(k, n)) = l;
+    *reinterpret_cast<float*>(W2 + w_off(n, k)) = h;
+    *reinterpret_cast<float*>(W2 + w_off(NH + n, k)) = l;
+    *reinterpret_cast<float*>(WT2 + wt_off(k, n)) = h;
+    *reinterpret_cast<float*>(WT2 + wt_off(64 + k, n)) = l;
   }
   for (int e = tid; e < 12 * TM; e += blockDim.x) {
-    const uint32_t off = xt_off(52 + e / TM, e % TM);
-    *reinterpret_cast<float*>(XTH + off) = 0.0f;
-    *reinterpret_cast<float*>(XTL + off) = 0.0f;
+    *reinterpret_cast<float*>(XT2 + xt_off(52 + e / TM, e % TM)) = 0.0f;
+    *reinterpret_cast<float*>(XT2 + xt_off(64 + 52 + e / TM, e % TM)) = 0.0f;
   }
   for (int i = tid; i < NH; i += blockDim.x) B0[i] = w.b0[i];
   for (int i = tid; i < NO * NH; i += blockDim.x) W1s[i] = w.W1[i];
@@ -368,9 +385,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   tc::fence_after_sync();
   const uint32_t tbase = *s_taddr;
   const uint32_t lane_base = (uint32_t)(32 * q) << 16;
-  const uint32_t wh = tc::smem_u32(WH), wl = tc::smem_u32(WL), wth = tc::smem_u32(WTH), wtl = tc::smem_u32(WTL);
-  const uint32_t xth = tc::smem_u32(XTH), xtl = tc::smem_u32(XTL), r1 = tc::smem_u32(R1);
-  constexpr uint32_t idN = tc::idesc_tf32(TM, 64, false, false);
+  const uint32_t w2 = tc::smem_u32(W2), wt2 = tc::smem_u32(WT2), xt2 = tc::smem_u32(XT2), r1 = tc::smem_u32(R1);
   // dW1 accumulators of hidden units 32*hh+j, colour c, summed over this thread's samples: TMEM
   // columns 256 + 96*hh + 32*c + j of this thread's lane (registers are spent on the prefetch)
   const uint32_t g1addr = tbase + lane_base + 256 + 96 * hh;
@@ -410,8 +425,8 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
             tc::split_tf32(v[i], hi[i], lo[i]);
-            *reinterpret_cast<float*>(XTH + xt_off(4 * c + i, m)) = hi[i];
-            *reinterpret_cast<float*>(XTL + xt_off(4 * c + i, m)) = lo[i];
+            *reinterpret_cast<float*>(XT2 + xt_off(4 * c + i, m)) = hi[i];
+            *reinterpret_cast<float*>(XT2 + xt_off(64 + 4 * c + i, m)) = lo[i];
           }
           *reinterpret_cast<float4*>(R1 + x_off(c, m)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
           *reinterpret_cast<float4*>(R1 + kXBytes + x_off(c, m)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
@@ -426,7 +441,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     __syncthreads();
     if (tid == 0) {
       tc::fence_after_sync();
-      issue_z(tbase, r1, r1 + kXBytes, wh, wl);
+      issue_z(tbase, r1, r1 + kXBytes, w2);
       tc::commit(bar);
     }
     bool ok = tc::mbar_wait(bar, phase, kWaitLimit);
@@ -437,8 +452,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     }
     tc::fence_after_sync();
     float z[32];
-    tc::tmem_ld32(tbase + lane_base + 32 * hh, z);
-    tc::tmem_wait_ld();
+    tmem_ld_sum32(tbase + lane_base + 32 * hh, z);
     {
       float p0, p1, p2;
       colour_partial(z, hh, B0, W1s, p0, p1, p2);
@@ -509,16 +523,9 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     tc::fence_smem_to_async();
     tc::fence_before_sync();
     __syncthreads();
-    if (tid == 0) {  // dX = DZ W0 (B = W0^T, feature rows)
+    if (tid == 0) {  // dX = DZ W0 (B = W0^T [hi; lo], feature rows) into the columns Z used
       tc::fence_after_sync();
-#pragma unroll 1
-      for (int ks = 0; ks < 8; ++ks) {
-        const uint64_t ah = tc::sdesc(r1 + ks * 4096, 2048, 128), al = tc::sdesc(r1 + kXBytes + ks * 4096, 2048, 128);
-        const uint64_t bh = tc::sdesc(wth + ks * 2048, 1024, 128), bl = tc::sdesc(wtl + ks * 2048, 1024, 128);
-        tc::mma_tf32(tbase + 64, ah, bh, idN, ks > 0);
-        tc::mma_tf32(tbase + 64, ah, bl, idN, true);
-        tc::mma_tf32(tbase + 64, al, bh, idN, true);
-      }
+      issue_split(tbase, r1, r1 + kXBytes, wt2, 8);
       tc::commit(bar);
     }
     ok = tc::mbar_wait(bar, phase, kWaitLimit);
@@ -543,10 +550,8 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
 #pragma unroll 1
       for (int s = 0; s < 16; ++s) {
         const uint64_t ad = tc::sdesc(r1 + s * 2 * kDztSlab, kDztSlab, 128);
-        const uint64_t bh = tc::sdesc(xth + s * 2 * kXtSlab, kXtSlab, 128);
-        const uint64_t bl = tc::sdesc(xtl + s * 2 * kXtSlab, kXtSlab, 128);
-        tc::mma_tf32(tbase + 128, ad, bh, idN, !first_w);
-        tc::mma_tf32(tbase + 192, ad, bl, idN, !first_w);
+        const uint64_t b = tc::sdesc(xt2 + s * 2 * kXtSlab, kXtSlab, 128);
+        tc::mma_tf32(tbase + 128, ad, b, kId128, !first_w);  // [128,192): x X_hi, [192,256): x X_lo
         first_w = false;
       }
       tc::commit(bar);
@@ -561,18 +566,21 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     // dX readout while the dW0 MMAs run
     if (hh == 0) {
       float v[32];
-      tc::tmem_ld32(tbase + lane_base + 64, v);
-      tc::tmem_wait_ld();
+      tmem_ld_sum32(tbase + lane_base, v);
       if (valid) {
         float4* o = reinterpret_cast<float4*>(d_hash + (m0 + m) * 32);
 #pragma unroll
         for (int c = 0; c < 8; ++c) o[c] = make_float4(v[4 * c], v[4 * c + 1], v[4 * c + 2], v[4 * c + 3]);
       }
     } else {
-      float v[4];
-      tc::tmem_ld4(tbase + lane_base + 64 + 48, v);
+      float v[4], u[4];
+      tc::tmem_ld4(tbase + lane_base + 48, v);
+      tc::tmem_ld4(tbase + lane_base + 64 + 48, u);
       tc::tmem_wait_ld();
       if (valid) {
+        v[0] += u[0];
+        v[1] += u[1];
+        v[2] += u[2];
         d_normal[(m0 + m) * 3] = v[0];
         d_normal[(m0 + m) * 3 + 1] = v[1];
         d_normal[(m0 + m) * 3 + 2] = v[2];
@@ -647,7 +655,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   if (wid == 0) tc::tmem_dealloc(tbase, 512);
 }
 
-constexpr size_t kBwdSmem = 4 * kWBytes + 2 * kXtBytes + kR1Bytes + sizeof(float) * (2 * TM * 4 + NO * NH + NH + 4) + 16;
+constexpr size_t kBwdSmem = 2 * kWBytes + kXtBytes + kR1Bytes + sizeof(float) * (2 * TM * 4 + NO * NH + NH + 4) + 16;
 
 
 // Sum the per-block partials in block order into dW0 (64,51), dW1 (3,64), db0 (64), db1 (3).
