@@ -340,12 +340,13 @@ def test_regularizers_list_golden(golden):
 
 
 @pytest.mark.parametrize("band", [None, 3.0])
-def test_fused_stencil_matches_oracle(band):
-    """Gather-form eikonal + curvature over a V_R bitmap == oracle list form after relax/band filters."""
+@pytest.mark.parametrize("res", [[40, 36, 44], [40, 36, 64]])
+def test_fused_stencil_matches_oracle(band, res):
+    """Gather-form eikonal + curvature over a V_R bitmap == oracle list form after relax/band filters
+    (Z = 64: whole-row bitmap words, the vectorised count path; Z = 44: words spanning rows)."""
     from voxneus_b200 import ops
 
     torch.manual_seed(12)
-    res = [40, 36, 44]
     lo, hi = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
     axes = [torch.linspace(-1, 1, r) for r in res]
     gx, gy, gz = torch.meshgrid(*axes, indexing="ij")
@@ -373,6 +374,45 @@ def test_fused_stencil_matches_oracle(band):
     assert abs(losses[1].item() - lc.item()) <= 1e-5 * max(lc.item(), 1e-12)
     vl, ll = ops.vr_compact(bm, gd, res, lo, hi, 1.2, bnd, counts, v.shape[0])
     assert torch.equal(vl.cpu(), v)
+
+
+def _bitmap_voxels(words: torch.Tensor, nvox: int) -> torch.Tensor:
+    w = words.cpu().numpy().view(np.uint32)
+    bits = np.unpackbits(w.view(np.uint8), bitorder="little")[:nvox]
+    return torch.from_numpy(np.nonzero(bits)[0].astype(np.int64))
+
+
+@pytest.mark.parametrize("res", [[24, 20, 96], [24, 20, 90]])
+def test_vr_count_and_filtered_bitmaps(res):
+    """|V_R| under each filter and the two filtered bitmaps, bit for bit against the oracle's
+    relax and band filters, on a dense random bitmap (whole-row words and row-spanning words)."""
+    from voxneus_b200 import ops
+
+    torch.manual_seed(13)
+    lo, hi = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
+    axes = [torch.linspace(-1, 1, r) for r in res]
+    gx, gy, gz = torch.meshgrid(*axes, indexing="ij")
+    grid = (torch.sqrt(gx ** 2 + gy ** 2 + gz ** 2) - 0.7 + 0.02 * torch.randn(*res)).contiguous()
+    nvox = res[0] * res[1] * res[2]
+    lin = torch.unique(torch.randint(0, nvox, (nvox // 3,)))
+    verts = torch.stack([lin // (res[1] * res[2]), (lin // res[2]) % res[1], lin % res[2]], -1)
+    eps = O.voxel_size(torch.tensor(lo), torch.tensor(hi), torch.tensor(res, dtype=torch.float32))
+    bnd = float(torch.tensor(3.0 * float(eps[0]), dtype=torch.float32))
+
+    def lin_of(v):
+        return (v[:, 0] * res[1] + v[:, 1]) * res[2] + v[:, 2]
+
+    relax = lin_of(O.relax_filter(verts, torch.tensor(lo), eps))
+    band = lin_of(O.band_filter(verts, grid, float(eps[0]), 3.0))
+    both = lin_of(O.band_filter(O.relax_filter(verts, torch.tensor(lo), eps), grid, float(eps[0]), 3.0))
+    bm = ops.new_bitmap(res, DEV)
+    ops.vr_mark_corners(to(verts), res, bm)
+    fb = ops.new_filtered(res, DEV)
+    counts = ops.vr_count(bm, to(grid), res, lo, hi, 1.2, bnd, filtered=fb)
+    assert counts.cpu().tolist() == [lin.numel(), relax.numel(), band.numel(), both.numel()]
+    nw = ops.bitmap_words(res)
+    assert torch.equal(_bitmap_voxels(fb[:nw], nvox), band)
+    assert torch.equal(_bitmap_voxels(fb[nw:], nvox), both)
 
 
 def test_upsample_golden(golden):

@@ -113,6 +113,71 @@ __global__ void __launch_bounds__(256) k_vr_count(VrArgs a, unsigned long long* 
   }
 }
 
+// The same counts and filtered bitmaps when every word lies inside one z row (Z % 32 == 0) and
+// the grid is 16-byte aligned: the 32 voxels of word w share (x, y) and have z = z0..z0+31, so
+// their SDF values are one 128-byte line (eight float4 loads, all in flight together) and the
+// relax distance needs x^2 + y^2 once; every bit of a nonzero word is evaluated without branches.
+__global__ void __launch_bounds__(256) k_vr_count_rows(VrArgs a, unsigned long long* __restrict__ counts,
+                                                       uint32_t* __restrict__ filtered) {
+  unsigned long long c[4] = {0, 0, 0, 0};
+  for (int64_t w = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; w < a.nwords; w += (int64_t)gridDim.x * blockDim.x) {
+    const uint32_t bits = a.bm[w];
+    uint32_t rmask = 0xffffffffu, bmask = 0xffffffffu;
+    if (bits) {
+      int x, y, z0;
+      vox_xyz(a.g, (int)(w * 32), x, y, z0);
+      if (a.relax_r > 0.0f) {
+        const float wx = __fadd_rn(a.g.lo[0], __fmul_rn((float)x, a.g.eps[0]));
+        const float wy = __fadd_rn(a.g.lo[1], __fmul_rn((float)y, a.g.eps[1]));
+        const float xy = __fadd_rn(__fmul_rn(wx, wx), __fmul_rn(wy, wy));
+        rmask = 0;
+#pragma unroll
+        for (int b = 0; b < 32; ++b) {
+          const float wz = __fadd_rn(a.g.lo[2], __fmul_rn((float)(z0 + b), a.g.eps[2]));
+          rmask |= (sqrtf(__fadd_rn(xy, __fmul_rn(wz, wz))) < a.relax_r ? 1u : 0u) << b;
+        }
+      }
+      if (a.band > 0.0f) {
+        const float4* f4 = reinterpret_cast<const float4*>(a.f + w * 32);
+        float4 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) v[k] = __ldg(f4 + k);
+        bmask = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+          bmask |= (fabsf(v[k].x) < a.band ? 1u : 0u) << (4 * k);
+          bmask |= (fabsf(v[k].y) < a.band ? 1u : 0u) << (4 * k + 1);
+          bmask |= (fabsf(v[k].z) < a.band ? 1u : 0u) << (4 * k + 2);
+          bmask |= (fabsf(v[k].w) < a.band ? 1u : 0u) << (4 * k + 3);
+        }
+      }
+      c[0] += __popc(bits);
+      c[1] += __popc(bits & rmask);
+      c[2] += __popc(bits & bmask);
+      c[3] += __popc(bits & rmask & bmask);
+    }
+    if (filtered) {
+      filtered[w] = bits & bmask;
+      filtered[a.nwords + w] = bits & bmask & rmask;
+    }
+  }
+  __shared__ unsigned long long sc[4][8];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    unsigned long long v = c[k];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if (lane == 0) sc[k][warp] = v;
+  }
+  __syncthreads();
+  if (threadIdx.x < 4) {
+    unsigned long long v = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) v += sc[threadIdx.x][w];
+    if (v) atomicAdd(counts + threadIdx.x, v);
+  }
+}
+
 __device__ __forceinline__ bool relax_mode(const unsigned long long* counts, float relax_r) {
   return relax_r > 0.0f && counts[1] > 0;
 }
@@ -325,7 +390,10 @@ int vx_vr_count(const uint32_t* bitmap, const float* grid, const int32_t res[3],
   VrArgs a;
   if (int s = make_vr(a, bitmap, grid, res, xyz_min, xyz_max, relax_radius, band)) return s;
   VX_REQUIRE(counts, "counts is null");
-  k_vr_count<<<grid_for(a.nwords, 256, 8), 256, 0, (cudaStream_t)stream>>>(a, counts, filtered);
+  if (a.g.rz % 32 == 0 && (a.band <= 0.0f || ((uintptr_t)grid & 15) == 0))
+    k_vr_count_rows<<<grid_for(a.nwords, 256, 8), 256, 0, (cudaStream_t)stream>>>(a, counts, filtered);
+  else
+    k_vr_count<<<grid_for(a.nwords, 256, 8), 256, 0, (cudaStream_t)stream>>>(a, counts, filtered);
   count_launches(1);
   return check_launch("vr_count");
 }
