@@ -444,12 +444,15 @@ def test_hash_and_sh_golden(golden):
     assert_close(enc.encoder.embeddings.grad, emb.grad, GRAD_TOL, "hash grad")
 
 
+@pytest.mark.parametrize("ld", [52, 56])
 @pytest.mark.parametrize("p", [3000, 50000])
-def test_fused_mlp_matches_oracle(p):
+def test_fused_mlp_matches_oracle(p, ld):
     """51-64-3 MLP forward (1e-5) and adjoint (input and weight gradients, 1e-4) vs torch fp32 autograd.
 
     3000 rows: one partial tile per block; 50000 rows: blocks accumulate several tiles of the
-    weight gradient in tensor memory. Neither is a multiple of the 128-sample tile.
+    weight gradient in tensor memory. Neither is a multiple of the 128-sample tile. Row stride 52
+    (contiguous rows: the adjoint brings each tile's rows in with one bulk copy) and 56 (strided
+    rows: prefetched through registers).
 
     Rows with a hidden pre-activation within 1e-6 of the largest |z| of zero (FP64) sit on a ReLU
     kink, where any two FP32 evaluation orders can disagree on the unit's sign (and move that
@@ -471,7 +474,9 @@ def test_fused_mlp_matches_oracle(p):
     ref = O.radiance_mlp(x[:, :32], x[:, 32:48], x[:, 48:51], *ws)
     cot = torch.randn(p, 3)
     (ref * cot).sum().backward()
-    rd = to(rows)
+    wide = torch.zeros(p, ld)
+    wide[:, :52] = rows
+    rd = to(wide)
     wd = [to(t.detach()).requires_grad_(True) for t in ws]
     xd = rd[:, :51].requires_grad_(True)
     out = ops.RadianceMLPFn.apply(xd, *wd)

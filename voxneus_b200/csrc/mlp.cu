@@ -330,6 +330,8 @@ constexpr uint32_t kXtSlab = 16 * 128 + 16;   // X^T: 4 samples x 128 rows (feat
 constexpr uint32_t kDztSlab = 16 * 128 + 16;  // DZ^T: 4 samples x 128 rows (hidden hi | hidden lo)
 constexpr uint32_t kXtBytes = 32 * kXtSlab;
 constexpr uint32_t kR1Bytes = 66560;          // X (hi, lo) -> DZ (hi, lo) -> DZ^T, one at a time
+constexpr uint32_t kRowBytes = KP * 4;        // one 52-float input row
+constexpr uint32_t kRowsBytes = TM * kRowBytes;  // the next tile's rows, brought in by a bulk copy
 
 __device__ __forceinline__ uint32_t xt_off(int f, int m) {
   return (uint32_t)((m >> 2) * kXtSlab + (f >> 3) * 128 + (f & 7) * 16 + (m & 3) * 4);
@@ -343,6 +345,11 @@ __device__ __forceinline__ uint32_t wt_off(int f, int n) {
   return (uint32_t)((n >> 2) * 2048 + (f >> 3) * 128 + (f & 7) * 16 + (n & 3) * 4);
 }
 
+// kBulk: the rows are contiguous 52-float rows (ldx = 52, 16-byte aligned); each tile's rows reach
+// shared memory through one bulk copy issued as soon as the previous tile has been staged, so no
+// registers or load instructions are spent on the prefetch. Otherwise the rows are prefetched
+// into registers during the previous tile.
+template <bool kBulk>
 __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__ X, int64_t ldx, int xvec, int64_t P,
                                                       MlpW w, const float* __restrict__ d_out,
                                                       float* __restrict__ d_hash, float* __restrict__ d_normal,
@@ -352,12 +359,14 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   uint8_t* WT2 = W2 + kWBytes;
   uint8_t* XT2 = WT2 + kWBytes;
   uint8_t* R1 = XT2 + kXtBytes;
-  float* RED = reinterpret_cast<float*>(R1 + kR1Bytes);  // [2][TM][4]
+  uint8_t* ROWS = R1 + kR1Bytes;  // kBulk only
+  float* RED = reinterpret_cast<float*>(ROWS + (kBulk ? kRowsBytes : 0));  // [2][TM][4]
   float* W1s = RED + 2 * TM * 4;
   float* B0 = W1s + NO * NH;
   float* B1 = B0 + NH;
   uint64_t* bar = reinterpret_cast<uint64_t*>(B1 + 4);
-  uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bar + 1);
+  uint64_t* bar_rows = bar + 1;
+  uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bar + 2);
   const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31, q = wid & 3, hh = wid >> 2;
   const int m = 32 * q + lane;  // this thread's sample in the tile (its TMEM lane)
   // W0 [hi; lo] (hidden rows) for Z, W0^T [hi; lo] (feature rows) for dX, b0, W1, b1; X^T feature
@@ -378,7 +387,10 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   for (int i = tid; i < NH; i += blockDim.x) B0[i] = w.b0[i];
   for (int i = tid; i < NO * NH; i += blockDim.x) W1s[i] = w.W1[i];
   if (tid < NO) B1[tid] = w.b1[tid];
-  if (tid == 0) tc::mbar_init(bar, 1);
+  if (tid == 0) {
+    tc::mbar_init(bar, 1);
+    tc::mbar_init(bar_rows, 1);
+  }
   if (wid == 0) tc::tmem_alloc(s_taddr, 512);
   tc::fence_before_sync();
   __syncthreads();
@@ -386,6 +398,20 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   const uint32_t tbase = *s_taddr;
   const uint32_t lane_base = (uint32_t)(32 * q) << 16;
   const uint32_t w2 = tc::smem_u32(W2), wt2 = tc::smem_u32(WT2), xt2 = tc::smem_u32(XT2), r1 = tc::smem_u32(R1);
+  const int64_t ntiles = (P + TM - 1) / TM;
+  // rows of tile t into ROWS (kBulk): one copy of the tile's valid rows, issued by thread 0
+  auto fetch_rows = [&](int64_t t) {
+    const int64_t m0 = t * TM;
+    const uint32_t bytes = (uint32_t)(P - m0 < TM ? P - m0 : TM) * kRowBytes;
+    tc::mbar_arrive_expect_tx(bar_rows, bytes);
+    tc::bulk_g2s(ROWS, X + m0 * KP, bytes, bar_rows);
+  };
+  uint32_t rphase = 0;
+  bool rows_pending = false;  // thread 0: a rows copy is in flight
+  if (kBulk && tid == 0 && (int64_t)blockIdx.x < ntiles) {
+    fetch_rows(blockIdx.x);
+    rows_pending = true;
+  }
   // dW1 accumulators of hidden units 32*hh+j, colour c, summed over this thread's samples: TMEM
   // columns 256 + 96*hh + 32*c + j of this thread's lane (registers are spent on the prefetch)
   const uint32_t g1addr = tbase + lane_base + 256 + 96 * hh;
@@ -400,26 +426,40 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   float sb[NO] = {0.0f, 0.0f, 0.0f};
   bool first_w = true, failed = false;
   uint32_t phase = 0;
-  const int64_t ntiles = (P + TM - 1) / TM;
-  float4 pre[7];  // this tile's row chunks, loaded during the previous tile
+  float4 pre[7];  // !kBulk: this tile's row chunks, loaded during the previous tile
   float dy[NO];
   if ((int64_t)blockIdx.x < ntiles) {
     const int64_t m0 = (int64_t)blockIdx.x * TM;
-    load_row_chunks(X, ldx, xvec != 0, P, m0, m, hh, pre);
+    if (!kBulk) load_row_chunks(X, ldx, xvec != 0, P, m0, m, hh, pre);
 #pragma unroll
     for (int c = 0; c < NO; ++c) dy[c] = m0 + m < P ? d_out[(m0 + m) * NO + c] : 0.0f;
   }
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t m0 = t * TM;
     const bool valid = m0 + m < P;
+    if (kBulk) {
+      const bool got = tc::mbar_wait(bar_rows, rphase, kWaitLimit);
+      rphase ^= 1u;
+      if (__syncthreads_or(!got)) {
+        failed = true;
+        break;
+      }
+      if (tid == 0) rows_pending = false;
+    }
     // rows -> X (sample rows, R1) and X^T (feature rows); column 51 = 1 on real rows (db0)
     {
       const int c0 = hh ? 7 : 0;
+      const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * kRowBytes);
 #pragma unroll
       for (int jc = 0; jc < 7; ++jc) {
         const int c = c0 + jc;
         if (c < 13) {
-          float v[4] = {pre[jc].x, pre[jc].y, pre[jc].z, pre[jc].w};
+          float4 u;
+          if (kBulk)
+            u = valid ? rrow[c] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          else
+            u = pre[jc];
+          float v[4] = {u.x, u.y, u.z, u.w};
           if (c == 12 && valid) v[3] = 1.0f;
           float hi[4], lo[4];
 #pragma unroll
@@ -443,6 +483,10 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
       tc::fence_after_sync();
       issue_z(tbase, r1, r1 + kXBytes, w2);
       tc::commit(bar);
+      if (kBulk && t + gridDim.x < ntiles) {  // ROWS has been read: bring the next tile's rows
+        fetch_rows(t + gridDim.x);
+        rows_pending = true;
+      }
     }
     bool ok = tc::mbar_wait(bar, phase, kWaitLimit);
     phase ^= 1u;
@@ -545,7 +589,9 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     tc::fence_smem_to_async();
     tc::fence_before_sync();
     __syncthreads();
-    if (tid == 0) {  // dW0 (+db0) += [DZ_hi | DZ_lo]^T X, K = the tile's samples
+    // dW0 (+db0) += [DZ_hi | DZ_lo]^T X, K = the tile's samples; issued by a warp whose dX readout
+    // is short (d_normal), so the d_hash readout warps are not held behind the issue
+    if (tid == 128) {
       tc::fence_after_sync();
 #pragma unroll 1
       for (int s = 0; s < 16; ++s) {
@@ -559,7 +605,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     // next tile's rows fly during the dW0 MMAs and the dX readout
     if (t + gridDim.x < ntiles) {
       const int64_t mn = (t + gridDim.x) * TM;
-      load_row_chunks(X, ldx, xvec != 0, P, mn, m, hh, pre);
+      if (!kBulk) load_row_chunks(X, ldx, xvec != 0, P, mn, m, hh, pre);
 #pragma unroll
       for (int c = 0; c < NO; ++c) dy[c] = mn + m < P ? d_out[(mn + m) * NO + c] : 0.0f;
     }
@@ -595,7 +641,11 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     }
     tc::fence_after_sync();
   }
-  if (failed && tid == 0) atomicAdd(&g_tc_timeouts, 1);
+  if (failed && tid == 0) {
+    atomicAdd(&g_tc_timeouts, 1);
+    // a rows copy may still be landing in shared memory: wait for it (bounded) before leaving
+    if (kBulk && rows_pending) tc::mbar_wait(bar_rows, rphase, kWaitLimit);
+  }
   // weight-gradient partials of this block
   const bool have = blockIdx.x < ntiles && !failed;  // every block with a tile issued the dW0 MMAs
   float* pb = partials + (int64_t)blockIdx.x * WG;
@@ -655,7 +705,8 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   if (wid == 0) tc::tmem_dealloc(tbase, 512);
 }
 
-constexpr size_t kBwdSmem = 2 * kWBytes + kXtBytes + kR1Bytes + sizeof(float) * (2 * TM * 4 + NO * NH + NH + 4) + 16;
+constexpr size_t kBwdSmemRegs = 2 * kWBytes + kXtBytes + kR1Bytes + sizeof(float) * (2 * TM * 4 + NO * NH + NH + 4) + 24;
+constexpr size_t kBwdSmemBulk = kBwdSmemRegs + kRowsBytes;
 
 
 // Sum the per-block partials in block order into dW0 (64,51), dW1 (3,64), db0 (64), db1 (3).
@@ -822,10 +873,13 @@ int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int 
   MlpW w{W0, b0, W1, b1};
   cudaStream_t st = (cudaStream_t)stream;
   if (n_points > 0) {
-    cudaError_t e = cudaFuncSetAttribute(k_mlp_bwd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kBwdSmem);
-    if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "radiance_mlp_backward: %s", cudaGetErrorString(e));
     const int xvec = (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
-    k_mlp_bwd_tc<<<nb, 256, kBwdSmem, st>>>(x, ldx, xvec, n_points, w, d_colors, d_hash, d_normal, partials);
+    const bool bulk = xvec && ldx == KP;
+    const size_t smem = bulk ? kBwdSmemBulk : kBwdSmemRegs;
+    auto kern = bulk ? k_mlp_bwd_tc<true> : k_mlp_bwd_tc<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "radiance_mlp_backward: %s", cudaGetErrorString(e));
+    kern<<<nb, 256, smem, st>>>(x, ldx, xvec, n_points, w, d_colors, d_hash, d_normal, partials);
   } else {
     cudaMemsetAsync(partials, 0, sizeof(float) * WG, st);
   }
