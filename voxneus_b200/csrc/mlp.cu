@@ -318,6 +318,150 @@ __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* 
 
 constexpr size_t kFwdSmem = 2 * kXBytes + kWBytes + sizeof(float) * (NH + NO * NH + 4 + 2 * TM * 4) + 16;
 
+// Forward on contiguous 52-float rows (ldx = 52, 16-byte aligned): one CTA of 512 threads per SM
+// holding two independent tile slots of 256 threads (slot s = threads 256 s ..), which share the
+// stacked weights and alternate on the tensor core. Each slot has its own X operand, its own
+// 128 TMEM columns, and a row buffer that the next tile's rows reach by one bulk copy, issued as
+// soon as the slot has staged its current tile; a slot synchronises on its own named barrier, so
+// one slot's MMA wait overlaps the other's staging and epilogue. Row prefetch through registers
+// (the general kernel above) left every warp stalled on its 16-byte loads of 32 rows at a time.
+constexpr uint32_t kFwdSlotBytes = 2 * kXBytes + TM * KP * 4 + 2 * TM * 4 * 4;  // XH, XL, rows, RED
+// shared head: W0 [hi; lo], b0, W1, b1, barriers, TMEM address, fail flags; slots from a 1 KB boundary
+constexpr size_t kFwd2Head = 1024 * ((kWBytes + sizeof(float) * (NH + NO * NH + 4) + 64 + 1023) / 1024);
+constexpr size_t kFwd2Smem = kFwd2Head + 2 * (size_t)kFwdSlotBytes;
+
+__device__ __forceinline__ void slot_sync(int slot) {
+  asm volatile("bar.sync %0, 256;" ::"r"(1 + slot) : "memory");
+}
+
+__global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restrict__ X, int64_t P, MlpW w,
+                                                         float* __restrict__ colors) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  uint8_t* W2 = smem;
+  float* B0 = reinterpret_cast<float*>(W2 + kWBytes);
+  float* W1s = B0 + NH;
+  float* B1 = W1s + NO * NH;
+  uint64_t* bars = reinterpret_cast<uint64_t*>(B1 + 4);  // [slot][mma, rows]
+  uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bars + 4);
+  int* s_fail = reinterpret_cast<int*>(s_taddr + 1);  // [2]
+  const int tid = threadIdx.x, slot = tid >> 8, stid = tid & 255;
+  const int wid = stid >> 5, lane = tid & 31, q = wid & 3, hh = wid >> 2;
+  const int m = 32 * q + lane;  // this thread's sample in its slot's tile
+  uint8_t* SL = smem + kFwd2Head + (size_t)slot * kFwdSlotBytes;
+  uint8_t* XH = SL;
+  uint8_t* XL = XH + kXBytes;
+  uint8_t* ROWS = XL + kXBytes;
+  float* RED = reinterpret_cast<float*>(ROWS + TM * KP * 4);  // [2][TM][4]
+  uint64_t* bar = bars + 2 * slot;
+  uint64_t* bar_rows = bar + 1;
+  // weights and each slot's X feature chunks 13..15 (zero), by all 512 threads
+  for (int e = tid; e < NH * 64; e += blockDim.x) {
+    const int n = e >> 6, k = e & 63;
+    float h, l;
+    tc::split_tf32(k < KIN ? w.W0[n * KIN + k] : 0.0f, h, l);
+    *reinterpret_cast<float*>(W2 + w_off(n, k)) = h;
+    *reinterpret_cast<float*>(W2 + w_off(NH + n, k)) = l;
+  }
+  for (int e = stid; e < 3 * TM; e += 256) {
+    const uint32_t off = x_off(13 + e / TM, e % TM);
+    *reinterpret_cast<float4*>(XH + off) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    *reinterpret_cast<float4*>(XL + off) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+  }
+  for (int i = tid; i < NH; i += blockDim.x) B0[i] = w.b0[i];
+  for (int i = tid; i < NO * NH; i += blockDim.x) W1s[i] = w.W1[i];
+  if (tid < NO) B1[tid] = w.b1[tid];
+  if (stid == 0) {
+    tc::mbar_init(bar, 1);
+    tc::mbar_init(bar_rows, 1);
+    s_fail[slot] = 0;
+  }
+  if (tid < 32) tc::tmem_alloc(s_taddr, 256);
+  tc::fence_before_sync();
+  __syncthreads();
+  tc::fence_after_sync();
+  const uint32_t tcol = *s_taddr + 128 * slot;
+  const uint32_t xh = tc::smem_u32(XH), xl = tc::smem_u32(XL), w2 = tc::smem_u32(W2);
+  const int64_t ntiles = (P + TM - 1) / TM;
+  const int64_t t0 = 2 * (int64_t)blockIdx.x + slot, tstride = 2 * (int64_t)gridDim.x;
+  auto fetch_rows = [&](int64_t t) {
+    const int64_t m0 = t * TM;
+    const uint32_t bytes = (uint32_t)(P - m0 < TM ? P - m0 : TM) * (uint32_t)(KP * 4);
+    tc::mbar_arrive_expect_tx(bar_rows, bytes);
+    tc::bulk_g2s(ROWS, X + m0 * KP, bytes, bar_rows);
+  };
+  bool rows_pending = false;  // slot thread 0: a rows copy is in flight
+  if (stid == 0 && t0 < ntiles) {
+    fetch_rows(t0);
+    rows_pending = true;
+  }
+  uint32_t phase = 0, rphase = 0;
+  for (int64_t t = t0; t < ntiles; t += tstride) {
+    const int64_t m0 = t * TM;
+    const bool valid = m0 + m < P;
+    const bool got = tc::mbar_wait(bar_rows, rphase, kWaitLimit);
+    rphase ^= 1u;
+    if (!got) s_fail[slot] = 1;
+    slot_sync(slot);
+    if (s_fail[slot]) break;
+    if (stid == 0) rows_pending = false;
+    {  // rows -> X (hi, lo); column 51 zero (the padding column may hold anything)
+      const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * (KP * 4));
+      const int c0 = hh ? 7 : 0;
+#pragma unroll
+      for (int j = 0; j < 7; ++j) {
+        const int c = c0 + j;
+        if (c < 13) {
+          float4 u = valid ? rrow[c] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          if (c == 12) u.w = 0.0f;
+          st_split4(XH, XL, x_off(c, m), u.x, u.y, u.z, u.w);
+        }
+      }
+    }
+    tc::fence_smem_to_async();
+    slot_sync(slot);
+    if (stid == 0) {
+      tc::fence_after_sync();
+      issue_z(tcol, xh, xl, w2);
+      tc::commit(bar);
+      if (t + tstride < ntiles) {  // ROWS has been read: bring this slot's next tile
+        fetch_rows(t + tstride);
+        rows_pending = true;
+      }
+    }
+    const bool ok = tc::mbar_wait(bar, phase, kWaitLimit);
+    phase ^= 1u;
+    if (!ok) s_fail[slot] = 1;
+    slot_sync(slot);
+    if (s_fail[slot]) break;
+    tc::fence_after_sync();
+    float z[32];
+    tmem_ld_sum32(tcol + ((uint32_t)(32 * q) << 16) + 32 * hh, z);
+    float p0, p1, p2;
+    colour_partial(z, hh, B0, W1s, p0, p1, p2);
+    float* r = RED + (hh * TM + m) * 4;
+    r[0] = p0;
+    r[1] = p1;
+    r[2] = p2;
+    tc::fence_before_sync();
+    slot_sync(slot);
+    if (stid < TM && m0 + stid < P) {
+#pragma unroll
+      for (int c = 0; c < NO; ++c) {
+        const float o = (B1[c] + RED[stid * 4 + c]) + RED[(TM + stid) * 4 + c];
+        colors[(m0 + stid) * NO + c] = sigmoidf_ref(o);
+      }
+    }
+  }
+  if (stid == 0 && s_fail[slot]) {
+    atomicAdd(&g_tc_timeouts, 1);
+    // a rows copy may still be landing in this slot's buffer: wait for it (bounded) before leaving
+    if (rows_pending) tc::mbar_wait(bar_rows, rphase, kWaitLimit);
+  }
+  tc::fence_before_sync();
+  __syncthreads();
+  if (tid < 32) tc::tmem_dealloc(*s_taddr, 256);
+}
+
 // Adjoint. d_out (P,3) -> d_hash (P,32), d_normal (P,3), per-block weight-gradient partials
 // [dW0 (64 x 52) | dW1 (3 x 64) | db0 (64) | db1 (3)]. tcgen05 kind::tf32 takes K-major operands
 // only here, so the sample contraction of dW0 reads transposed copies: X^T (written as the rows
@@ -778,10 +922,18 @@ __global__ void __launch_bounds__(256, 6) k_hash_rows(HashArgs a) {
 template <bool kHashIn, bool kRowsOut>
 int launch_fwd(const HashArgs& a, const float* X, int64_t ldx, int64_t P, const MlpW& w, float* colors,
                cudaStream_t st) {
+  const int64_t tiles = (P + TM - 1) / TM;
+  if (!kHashIn && ldx == KP && (reinterpret_cast<uintptr_t>(X) & 15) == 0) {  // contiguous rows: two slots
+    cudaError_t e = cudaFuncSetAttribute(k_mlp_fwd_rows2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwd2Smem);
+    if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "mlp forward: %s", cudaGetErrorString(e));
+    const int64_t pairs = (tiles + 1) / 2;
+    const unsigned blocks = (unsigned)(pairs < (int64_t)kSMs ? pairs : (int64_t)kSMs);
+    k_mlp_fwd_rows2<<<blocks, 512, kFwd2Smem, st>>>(X, P, w, colors);
+    return VX_OK;
+  }
   auto kern = k_mlp_fwd_tc<kHashIn, kRowsOut>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem);
   if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "mlp forward: %s", cudaGetErrorString(e));
-  const int64_t tiles = (P + TM - 1) / TM;
   const unsigned blocks = (unsigned)(tiles < (int64_t)kSMs * 2 ? tiles : (int64_t)kSMs * 2);
   const int xvec = X && (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
   kern<<<blocks, 256, kFwdSmem, st>>>(a, X, ldx, xvec, P, w, colors);
