@@ -508,6 +508,46 @@ def test_huber_loss_and_gradient():
     assert_close(pd.grad, 3.0 * pr.grad, GRAD_TOL, "huber grad")
 
 
+@pytest.mark.parametrize("ld", [52, 56])
+def test_appearance_rows_match_oracle(ld):
+    """The MLP input rows the training forward writes ([hash 32 | SH 16 | normal 3 | 0]) against the
+    oracle's hash encoding, SH and normals: 397 rays x 127 samples (many 64-sample blocks and a
+    partial last one), a progressive level mask of 9.5 levels (one level weighted 0.5, six skipped),
+    contiguous rows (52) and a wider stride (56)."""
+    from voxneus_b200 import _lib, ops
+
+    torch.manual_seed(21)
+    cfg = ops.HashConfig(16, 2, 14)
+    nr, ns = 397, 127
+    emb = torch.rand(16, 2 ** 14, 2) * 0.2 - 0.1
+    o = torch.randn(nr, 3)
+    o = 2.5 * o / o.norm(dim=-1, keepdim=True)
+    d = -o / o.norm(dim=-1, keepdim=True) + 0.1 * torch.randn(nr, 3)
+    d = d / d.norm(dim=-1, keepdim=True)
+    mid = torch.sort(torch.rand(nr, ns) * 3.0 + 0.5, dim=-1).values
+    nrm = torch.randn(nr * ns, 3)
+    ws = [torch.randn(64, 51) * 0.1, torch.zeros(64), torch.randn(3, 64) * 0.1, torch.zeros(3)]
+    lo, hi = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
+    ed, od, dd, md, nd = (to(t.contiguous()) for t in (emb, o, d, mid, nrm))
+    wd = [to(t) for t in ws]
+    rows = torch.full((nr * ns, ld), float("nan"), device=DEV)
+    colors = torch.empty(nr * ns, 3, device=DEV)
+    P = _lib.ptr
+    _lib.call("vx_appearance_mlp_forward", P(ed), 16, 14, 2, cfg._res_c, cfg.level_weights(9.5), P(od), P(dd), P(md),
+              ns, _lib.f3(lo), _lib.f3(hi), nr * ns, P(nd), *[P(t) for t in wd], P(colors), P(rows), ld,
+              _lib.stream_ptr(torch.device(DEV)))
+    torch.cuda.synchronize()
+    pts = o.unsqueeze(1) + d.unsqueeze(1) * mid.unsqueeze(-1)
+    nx = (pts - torch.tensor(lo)) / (torch.tensor(hi) - torch.tensor(lo) + 1e-8)
+    hf = O.hash_encode(nx.reshape(-1, 3), emb, cfg.resolutions, 9.5)
+    sh = O.sh4(d.unsqueeze(1).expand(nr, ns, 3).reshape(-1, 3))
+    got = rows.cpu()
+    assert_close(got[:, :32], hf, VAL_TOL, "hash features")
+    assert_close(got[:, 32:48], sh, VAL_TOL, "sh", scale=1.0)
+    assert torch.equal(got[:, 48:51], nrm) and bool((got[:, 51] == 0).all())
+    assert bool((got[:, 2 * 10:32] == 0).all())  # levels 10..15 are skipped
+
+
 def test_fused_appearance_render_matches_cublas_path(golden):
     """Fused hash+MLP render gives the same values and gradients as the cuBLAS MLP path."""
     from voxneus_b200.rendering import RaySampler, compute_huber_color_loss

@@ -873,49 +873,66 @@ __global__ void k_mlp_wgrad_reduce(const float* __restrict__ partials, int nbloc
   }
 }
 
-// MLP input rows [hash 32 | SH 16 | normal 3 | 0] of (rays, midpoints), four threads per sample:
-// thread (i, g) gathers hash levels 4g..4g+3 (columns 8g..8g+7) and writes SH coefficients
-// 4g..4g+3 (columns 32+4g..); g = 3 also the normal. Few registers and no shared memory, so many
-// warps keep the table gathers in flight; the arithmetic per level is the fused kernel's.
-__global__ void __launch_bounds__(256, 6) k_hash_rows(HashArgs a) {
+// MLP input rows [hash 32 | SH 16 | normal 3 | 0] of the training forward. A block of 256 threads
+// covers 64 consecutive samples: warp w gathers levels 4(w/2)..4(w/2)+3 for the samples
+// 32(w%2)..32(w%2)+31, so each gather instruction reads one level for 32 consecutive samples of
+// a ray, and neighbouring samples that share a coarse-level cell share its request. Warps of
+// level group 0 also evaluate the SH of the view direction, group 1 copies the normal; the rows
+// meet in shared memory and leave as one contiguous block (or row by row for a wider stride).
+constexpr int kRowsPerBlock = 64;
+
+__global__ void __launch_bounds__(256) k_hash_rows(HashArgs a) {
+  __shared__ float4 srow[kRowsPerBlock * 13];
   const uint32_t mask = (1u << a.log2T) - 1u;
   const size_t T = (size_t)1 << a.log2T;
-  for (int64_t e = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; e < a.P * 4;
-       e += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t i = e >> 2;
-    const int g = (int)(e & 3);
-    float x[3];
-    sample_pos(a, i, x);
-    float f[8];
+  const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, g = w >> 1;
+  const int ls = 32 * (w & 1) + lane;  // this thread's sample in the block
+  for (int64_t base = (int64_t)blockIdx.x * kRowsPerBlock; base < a.P; base += (int64_t)gridDim.x * kRowsPerBlock) {
+    const int64_t i = base + ls;
+    if (i < a.P) {
+      float x[3];
+      sample_pos(a, i, x);
+      float f[8];
 #pragma unroll
-    for (int qq = 0; qq < 4; ++qq) {
-      const int l = 4 * g + qq;
-      const float lw = a.lw[l];
-      float f0 = 0.0f, f1 = 0.0f;
-      if (lw != 0.0f) {
-        LevelCell c;
-        level_cell(x, a.res[l], mask, c);
-        const float2* tab = reinterpret_cast<const float2*>(a.table) + (size_t)l * T;
-        gather_level(tab, c, f0, f1);
-        if (lw < 1.0f) {
-          f0 *= lw;
-          f1 *= lw;
+      for (int qq = 0; qq < 4; ++qq) {
+        const int l = 4 * g + qq;
+        const float lw = a.lw[l];
+        float f0 = 0.0f, f1 = 0.0f;
+        if (lw != 0.0f) {
+          LevelCell c;
+          level_cell(x, a.res[l], mask, c);
+          const float2* tab = reinterpret_cast<const float2*>(a.table) + (size_t)l * T;
+          gather_level(tab, c, f0, f1);
+          if (lw < 1.0f) {
+            f0 *= lw;
+            f1 *= lw;
+          }
         }
+        f[2 * qq] = f0;
+        f[2 * qq + 1] = f1;
       }
-      f[2 * qq] = f0;
-      f[2 * qq + 1] = f1;
+      srow[ls * 13 + 2 * g] = make_float4(f[0], f[1], f[2], f[3]);
+      srow[ls * 13 + 2 * g + 1] = make_float4(f[4], f[5], f[6], f[7]);
+      if (g == 0) {
+        const int64_t r = i / a.S;
+        float o[16];
+        sh16(__ldg(a.rays_d + 3 * r), __ldg(a.rays_d + 3 * r + 1), __ldg(a.rays_d + 3 * r + 2), o);
+#pragma unroll
+        for (int c = 0; c < 4; ++c) srow[ls * 13 + 8 + c] = make_float4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
+      } else if (g == 1) {
+        srow[ls * 13 + 12] = make_float4(a.normals[3 * i], a.normals[3 * i + 1], a.normals[3 * i + 2], 0.0f);
+      }
     }
-    float4* row = reinterpret_cast<float4*>(a.out + i * a.ld);
-    row[2 * g] = make_float4(f[0], f[1], f[2], f[3]);
-    row[2 * g + 1] = make_float4(f[4], f[5], f[6], f[7]);
-    const int64_t r = i / a.S;
-    float o[16];
-    sh16(__ldg(a.rays_d + 3 * r), __ldg(a.rays_d + 3 * r + 1), __ldg(a.rays_d + 3 * r + 2), o);
-    row[8 + g] = g == 0 ? make_float4(o[0], o[1], o[2], o[3])
-                 : g == 1 ? make_float4(o[4], o[5], o[6], o[7])
-                 : g == 2 ? make_float4(o[8], o[9], o[10], o[11])
-                          : make_float4(o[12], o[13], o[14], o[15]);
-    if (g == 3) row[12] = make_float4(a.normals[3 * i], a.normals[3 * i + 1], a.normals[3 * i + 2], 0.0f);
+    __syncthreads();
+    const int nrows = (int)(a.P - base < kRowsPerBlock ? a.P - base : kRowsPerBlock);
+    if (a.ld == KP) {
+      float4* out = reinterpret_cast<float4*>(a.out + base * KP);
+      for (int k = tid; k < nrows * 13; k += 256) out[k] = srow[k];
+    } else {
+      for (int k = tid; k < nrows * 13; k += 256)
+        reinterpret_cast<float4*>(a.out + (base + k / 13) * a.ld)[k % 13] = srow[k];
+    }
+    __syncthreads();
   }
 }
 
@@ -969,7 +986,13 @@ int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, i
   MlpW w{W0, b0, W1, b1};
   cudaStream_t st = (cudaStream_t)stream;
   if (rows) {  // training: rows gathered at high occupancy, then the MLP on the rows
-    k_hash_rows<<<grid_for(n_points * 4, 256), 256, 0, st>>>(a);
+    static int rows_per_sm = 0;  // resident blocks per SM (one wave of the grid-stride loop)
+    if (rows_per_sm == 0) {
+      int nb = 0;
+      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_hash_rows, 256, 0) != cudaSuccess || nb < 1) nb = 4;
+      rows_per_sm = nb;
+    }
+    k_hash_rows<<<grid_for((n_points + kRowsPerBlock - 1) / kRowsPerBlock * 256, 256, rows_per_sm), 256, 0, st>>>(a);
     if (int s = launch_fwd<false, false>(a, rows, ld_rows, n_points, w, colors, st)) return s;
     count_launches(2);
   } else {  // inference: features built in shared memory, nothing else written
