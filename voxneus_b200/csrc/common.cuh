@@ -9,6 +9,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <cmath>
+
 #include "../../include/voxneus_b200.h"
 
 namespace vx {
@@ -42,9 +44,23 @@ struct Grid {
   int rx, ry, rz;
   float lo[3];   // xyz_min
   float den[3];  // (xyz_max - xyz_min) + 1e-8f, the reference's normalisation denominator
+  float inv_den[3];  // 1 / den when den is a power of two (exact), else 0
   float eps[3];  // voxel size (xyz_max - xyz_min) / (res - 1)
   float hi_clamp[3];  // float32(res - 1.0001): Eq.7 coordinate clamp (coordinates.py:73-75)
 };
+
+// 1 / d when d is a power of two (then x / d == x * (1 / d) exactly for every float x), else 0.
+__host__ inline float pow2_recip(float d) {
+  int e = 0;
+  const float m = std::frexp(d, &e);
+  const float r = 1.0f / d;
+  return (d > 0.0f && m == 0.5f && std::isnormal(r)) ? r : 0.0f;
+}
+
+// x / den with IEEE rounding; a multiplication when den is a power of two (inv = pow2_recip(den)).
+__device__ __forceinline__ float div_den(float x, float den, float inv) {
+  return inv != 0.0f ? __fmul_rn(x, inv) : __fdiv_rn(x, den);
+}
 
 __host__ inline Grid make_grid(const int32_t res[3], const float lo[3], const float hi[3]) {
   Grid g;
@@ -55,6 +71,7 @@ __host__ inline Grid make_grid(const int32_t res[3], const float lo[3], const fl
     g.lo[a] = lo[a];
     float span = hi[a] - lo[a];
     g.den[a] = span + 1e-8f;
+    g.inv_den[a] = pow2_recip(g.den[a]);
     g.eps[a] = span / ((float)res[a] - 1.0f);
     g.hi_clamp[a] = (float)((double)res[a] - 1.0001);
   }
@@ -87,8 +104,8 @@ struct Tri {
   unsigned inb;         // bit k set when corner k is inside the grid
 };
 
-__device__ __forceinline__ float gs_coord(float p, float lo, float den, int R) {
-  float n = __fdiv_rn(__fsub_rn(p, lo), den);
+__device__ __forceinline__ float gs_coord(float p, float lo, float den, float inv, int R) {
+  float n = div_den(__fsub_rn(p, lo), den, inv);
   float g = __fsub_rn(__fmul_rn(n, 2.0f), 1.0f);
   float c = __fmul_rn(__fdiv_rn(__fadd_rn(g, 1.0f), 2.0f), (float)(R - 1));
   c = fminf((float)(R - 1), fmaxf(c, 0.0f));
@@ -96,9 +113,9 @@ __device__ __forceinline__ float gs_coord(float p, float lo, float den, int R) {
 }
 
 __device__ __forceinline__ void gs_setup(const Grid& g, float px, float py, float pz, Tri& t) {
-  const float cx = gs_coord(px, g.lo[0], g.den[0], g.rx);
-  const float cy = gs_coord(py, g.lo[1], g.den[1], g.ry);
-  const float cz = gs_coord(pz, g.lo[2], g.den[2], g.rz);
+  const float cx = gs_coord(px, g.lo[0], g.den[0], g.inv_den[0], g.rx);
+  const float cy = gs_coord(py, g.lo[1], g.den[1], g.inv_den[1], g.ry);
+  const float cz = gs_coord(pz, g.lo[2], g.den[2], g.inv_den[2], g.rz);
   t.x0 = (int)floorf(cx);
   t.y0 = (int)floorf(cy);
   t.z0 = (int)floorf(cz);
@@ -155,8 +172,8 @@ struct Eq7 {
   float dx, dy, dz;
 };
 
-__device__ __forceinline__ float eq7_coord(float p, float lo, float den, int R) {
-  return __fmul_rn(__fdiv_rn(__fsub_rn(p, lo), den), (float)R - 1.0f);
+__device__ __forceinline__ float eq7_coord(float p, float lo, float den, float inv, int R) {
+  return __fmul_rn(div_den(__fsub_rn(p, lo), den, inv), (float)R - 1.0f);
 }
 
 __device__ __forceinline__ void eq7_setup_grid_coords(const Grid& g, float cx, float cy, float cz, Eq7& e) {
@@ -180,8 +197,9 @@ __device__ __forceinline__ void eq7_setup_grid_coords(const Grid& g, float cx, f
 }
 
 __device__ __forceinline__ void eq7_setup(const Grid& g, float px, float py, float pz, Eq7& e) {
-  eq7_setup_grid_coords(g, eq7_coord(px, g.lo[0], g.den[0], g.rx), eq7_coord(py, g.lo[1], g.den[1], g.ry),
-                        eq7_coord(pz, g.lo[2], g.den[2], g.rz), e);
+  eq7_setup_grid_coords(g, eq7_coord(px, g.lo[0], g.den[0], g.inv_den[0], g.rx),
+                        eq7_coord(py, g.lo[1], g.den[1], g.inv_den[1], g.ry),
+                        eq7_coord(pz, g.lo[2], g.den[2], g.inv_den[2], g.rz), e);
 }
 
 __device__ __forceinline__ void eq7_weights(const Eq7& e, float w[8]) {
@@ -293,7 +311,7 @@ __device__ __forceinline__ void gs_scatter(float* __restrict__ gg, const Grid& g
 struct Occ {
   const uint8_t* mask;  // (R,R,R) bool, or nullptr for no modulation
   int r;
-  float lo[3], den[3];
+  float lo[3], den[3], inv_den[3];
 };
 
 __device__ __forceinline__ bool occupied(const Occ& oc, float px, float py, float pz) {
@@ -303,7 +321,7 @@ __device__ __forceinline__ bool occupied(const Occ& oc, float px, float py, floa
   const float hi = (float)((double)oc.r - 1.0001);
 #pragma unroll
   for (int a = 0; a < 3; ++a) {
-    const float n = __fdiv_rn(__fsub_rn(p[a], oc.lo[a]), oc.den[a]);
+    const float n = div_den(__fsub_rn(p[a], oc.lo[a]), oc.den[a], oc.inv_den[a]);
     inb = inb && (n >= 0.0f) && (n <= 1.0f);
     const float s = fminf(fmaxf(__fmul_rn(n, (float)oc.r), 0.0f), hi);
     c[a] = (int)s;
@@ -318,6 +336,7 @@ inline Occ make_occ(const uint8_t* mask, int r, const float lo[3], const float h
   for (int a = 0; a < 3; ++a) {
     oc.lo[a] = mask ? lo[a] : 0.f;
     oc.den[a] = mask ? (hi[a] - lo[a]) + 1e-8f : 1.f;
+    oc.inv_den[a] = pow2_recip(oc.den[a]);
   }
   return oc;
 }

@@ -20,7 +20,7 @@ struct HashArgs {
   const float* rays_d;
   const float* mid;
   int S;
-  float lo[3], den[3];
+  float lo[3], den[3], inv_den[3];
   int64_t P;
   float* out;  // rows of length >= 2L
   int64_t ld;
@@ -45,7 +45,7 @@ __device__ __forceinline__ void sample_pos(const HashArgs& a, int64_t i, float x
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
       const float p = ray_at(__ldg(a.rays_o + 3 * r + c), __ldg(a.rays_d + 3 * r + c), t);
-      x[c] = __fdiv_rn(__fsub_rn(p, a.lo[c]), a.den[c]);
+      x[c] = div_den(__fsub_rn(p, a.lo[c]), a.den[c], a.inv_den[c]);
     }
   }
   // RadianceHashGrid.forward clamps to [0, 1] (radiance_hash.py:213)
@@ -174,6 +174,7 @@ inline void fill_positions(HashArgs& a, const float* pts_norm, const float* rays
   for (int c = 0; c < 3; ++c) {
     a.lo[c] = xyz_min ? xyz_min[c] : 0.f;
     a.den[c] = xyz_min ? (xyz_max[c] - xyz_min[c]) + 1e-8f : 1.f;
+    a.inv_den[c] = pow2_recip(a.den[c]);
   }
 }
 

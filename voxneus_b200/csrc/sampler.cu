@@ -39,8 +39,8 @@ __device__ __forceinline__ bool inside_unit(float ox, float oy, float oz, float 
 // Lane j (< ns) ends holding its new sample in `out`; `u_ray` points at ns uniforms or is
 // null (deterministic: u_det table). Returns the searchsorted index through idx_out.
 __device__ void warp_sample_pdf(const WarpArrays& A, int n, int ns, const float* __restrict__ u_ray,
-                                const float* __restrict__ u_det, int lane, float* out_vals, int64_t* out_idx,
-                                float& my_new, int& my_idx) {
+                                const float* __restrict__ u_det, float u_lane, int lane, float* out_vals,
+                                int64_t* out_idx, float& my_new, int& my_idx) {
   const int nb = n - 1;  // number of weights
   // sums and scans accumulate in double and round once to float, like the reference's CPU
   // reductions (at::acc_type<float, false> is double)
@@ -61,7 +61,7 @@ __device__ void warp_sample_pdf(const WarpArrays& A, int n, int ns, const float*
   my_new = 0.0f;
   my_idx = 0;
   for (int j = lane; j < ns; j += 32) {
-    const float u = u_ray ? u_ray[j] : u_det[j];
+    const float u = j == lane ? u_lane : (u_ray ? u_ray[j] : u_det[j]);  // u_lane: this lane's, loaded early
     // searchsorted(cdf, u, right=True): number of entries <= u
     int lo = 0, hi = n;
     while (lo < hi) {
@@ -85,18 +85,31 @@ __device__ void warp_sample_pdf(const WarpArrays& A, int n, int ns, const float*
   }
 }
 
-// up_sample (sampler.py:243-292): interval weights into A.w, then the inverse CDF.
+// up_sample (sampler.py:243-292): interval weights into A.w, then the inverse CDF. Whole-warp
+// chunks of 32 intervals: the inside-sphere test of z_{i+1} and the previous interval's cos come
+// from the neighbouring lane (the same expressions on the same operands), and the occupancy
+// factor 0.9 occ + 0.1 of each interval is looked up here, into A.z2, so that the serial scan
+// below holds no global load.
 __device__ void warp_upsample_weights(const WarpArrays& A, int n, float inv_s, float ox, float oy, float oz, float dx,
                                       float dy, float dz, const Occ& oc, int lane) {
   const int nb = n - 1;
   // alpha per interval (into A.w) and 1 - alpha + 1e-7 (into A.cdf)
-  for (int i = lane; i < nb; i += 32) {
-    const float z0 = A.z[i], z1 = A.z[i + 1];
-    const float f0 = A.f[i], f1 = A.f[i + 1];
-    const bool ins = inside_unit(ox, oy, oz, dx, dy, dz, z0) || inside_unit(ox, oy, oz, dx, dy, dz, z1);
+  float cos_carry = 0.0f;  // cos of the interval before this chunk
+  for (int base = 0; base < nb; base += 32) {
+    const int i = base + lane;
+    const bool valid = i < nb;
+    const int ic = valid ? i : nb - 1;
+    const float z0 = A.z[ic], z1 = A.z[ic + 1];
+    const float f0 = A.f[ic], f1 = A.f[ic + 1];
+    const bool in0 = inside_unit(ox, oy, oz, dx, dy, dz, z0);
+    const bool in_next = __shfl_down_sync(0xffffffffu, in0, 1);
+    const bool in1 = (lane == 31 || i >= nb - 1) ? inside_unit(ox, oy, oz, dx, dy, dz, z1) : in_next;
+    const bool ins = in0 || in1;
     const float cosv = (f1 - f0) / (__fsub_rn(z1, z0) + 1e-5f);
-    float prev = 0.0f;
-    if (i > 0) prev = (f0 - A.f[i - 1]) / (__fsub_rn(z0, A.z[i - 1]) + 1e-5f);
+    float prev = __shfl_up_sync(0xffffffffu, cosv, 1);
+    if (lane == 0) prev = cos_carry;
+    if (i == 0) prev = 0.0f;
+    cos_carry = __shfl_sync(0xffffffffu, cosv, 31);
     float c = fminf(prev, cosv);
     c = fminf(fmaxf(c, -1e3f), 0.0f) * (ins ? 1.0f : 0.0f);
     const float fm = (f0 + f1) * 0.5f;
@@ -105,8 +118,15 @@ __device__ void warp_upsample_weights(const WarpArrays& A, int n, float inv_s, f
     const float e0 = __fsub_rn(fm, half), e1 = __fadd_rn(fm, half);
     const float c0 = sigmoidf_ref(e0 * inv_s), c1 = sigmoidf_ref(e1 * inv_s);
     const float alpha = __fadd_rn(__fsub_rn(c0, c1), 1e-5f) / __fadd_rn(c0, 1e-5f);
-    A.w[i] = alpha;
-    A.cdf[i] = __fadd_rn(__fsub_rn(1.0f, alpha), 1e-7f);
+    if (valid) {
+      A.w[i] = alpha;
+      A.cdf[i] = __fadd_rn(__fsub_rn(1.0f, alpha), 1e-7f);
+      if (oc.mask) {
+        const float zm = (z0 + z1) * 0.5f;
+        const float occ = occupied(oc, ray_at(ox, dx, zm), ray_at(oy, dy, zm), ray_at(oz, dz, zm)) ? 1.0f : 0.0f;
+        A.z2[i] = __fadd_rn(__fmul_rn(occ, 0.90f), 0.10f);
+      }
+    }
   }
   __syncwarp();
   // exclusive product scan: T_i = prod_{j<i} (1 - alpha_j + 1e-7); w_i = alpha_i T_i
@@ -120,11 +140,7 @@ __device__ void warp_upsample_weights(const WarpArrays& A, int n, float inv_s, f
     exc *= carry;
     if (i < nb) {
       float w = A.w[i] * (float)exc;
-      if (oc.mask) {
-        const float zm = (A.z[i] + A.z[i + 1]) * 0.5f;
-        const float occ = occupied(oc, ray_at(ox, dx, zm), ray_at(oy, dy, zm), ray_at(oz, dz, zm)) ? 1.0f : 0.0f;
-        w = w * __fadd_rn(__fmul_rn(occ, 0.90f), 0.10f);
-      }
+      if (oc.mask) w = w * A.z2[i];
       A.w[i] = w;
     }
     carry *= __shfl_sync(0xffffffffu, inc, 31);
@@ -135,6 +151,7 @@ __device__ void warp_upsample_weights(const WarpArrays& A, int n, float inv_s, f
 // Rank-sort the ns (<= 32) new samples held by lanes < ns into A.nz/A.nf (ascending).
 __device__ __forceinline__ void warp_rank_sort_new(const WarpArrays& A, int ns, float v, float fv, int lane) {
   int rank = 0;
+#pragma unroll 8
   for (int k = 0; k < ns; ++k) {
     const float o = __shfl_sync(0xffffffffu, v, k);
     if (lane < ns) rank += (o < v) || (o == v && k < lane);
@@ -224,6 +241,7 @@ __global__ void __launch_bounds__(128) k_sample_multistep(SamplerArgs a, const f
     }
     __syncwarp();
     if (a.n_importance > 0 && a.steps > 0) {
+#pragma unroll 2
       for (int i = lane; i < n; i += 32) {
         const float t = A.z[i];
         A.f[i] = query_sdf(fgrid, g, ray_at(ox, dx, t), ray_at(oy, dy, t), ray_at(oz, dz, t));
@@ -231,11 +249,13 @@ __global__ void __launch_bounds__(128) k_sample_multistep(SamplerArgs a, const f
       __syncwarp();
       for (int s = 0; s < a.steps; ++s) {
         const float inv_s = 64.0f * (float)(1 << s);
-        warp_upsample_weights(A, n, inv_s, ox, oy, oz, dx, dy, dz, oc, lane);
         const float* u_ray = a.u ? a.u + ((int64_t)s * a.n_rays + r) * a.per_step : nullptr;
+        // this lane's uniform, loaded before the weights so its latency is hidden
+        const float u_lane = lane < a.per_step ? (u_ray ? u_ray[lane] : a.u_det[lane]) : 0.0f;
+        warp_upsample_weights(A, n, inv_s, ox, oy, oz, dx, dy, dz, oc, lane);
         float v;
         int idx;
-        warp_sample_pdf(A, n, a.per_step, u_ray, a.u_det, lane, nullptr, nullptr, v, idx);
+        warp_sample_pdf(A, n, a.per_step, u_ray, a.u_det, u_lane, lane, nullptr, nullptr, v, idx);
         const bool last = (s + 1 == a.steps);
         float fv = 0.0f;
         if (!last && lane < a.per_step) fv = query_sdf(fgrid, g, ray_at(ox, dx, v), ray_at(oy, dy, v), ray_at(oz, dz, v));
@@ -290,7 +310,8 @@ __global__ void __launch_bounds__(128) k_up_sample(const float* __restrict__ ray
     warp_upsample_weights(A, n, inv_s, ox, oy, oz, dx, dy, dz, oc, lane);
     float v;
     int idx;
-    warp_sample_pdf(A, n, ns, u ? u + r * ns : nullptr, u_det, lane, out + r * ns, nullptr, v, idx);
+    const float u_lane = lane < ns ? (u ? u[r * ns + lane] : u_det[lane]) : 0.0f;
+    warp_sample_pdf(A, n, ns, u ? u + r * ns : nullptr, u_det, u_lane, lane, out + r * ns, nullptr, v, idx);
     __syncwarp();
   }
 }
@@ -334,7 +355,9 @@ __global__ void __launch_bounds__(128) k_sample_pdf(const float* __restrict__ bi
         if (idx_out) idx_out[r * ns + j] = lo;
       }
     } else {
-      warp_sample_pdf(A, n, ns, u ? u + r * ns : nullptr, u_det, lane, out + r * ns, idx_out ? idx_out + r * ns : nullptr,
+      const float u_lane = lane < ns ? (u ? u[r * ns + lane] : u_det[lane]) : 0.0f;
+      warp_sample_pdf(A, n, ns, u ? u + r * ns : nullptr, u_det, u_lane, lane, out + r * ns,
+                      idx_out ? idx_out + r * ns : nullptr,
                       v, idx);
     }
     __syncwarp();
