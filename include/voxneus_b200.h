@@ -231,6 +231,19 @@ int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, i
                               const float* b0, const float* W1, const float* b1, float* colors, float* rows,
                               int64_t ld_rows, void* stream);
 
+/* Inference form of vx_appearance_mlp_forward (no rows kept for an adjoint): the same colours,
+ * computed chunk by chunk of whole rays through the caller's scratch rows (scratch_count x 52
+ * floats, 16-byte aligned; at least n_samples rows): each chunk's rows are gathered into the
+ * scratch and the MLP reads them back (the gather and the MLP each at their own best occupancy).
+ * Fewer, larger chunks cost less: each chunk adds two launches and their tails. n_points must be a
+ * multiple of n_samples (whole rays). */
+int vx_appearance_mlp_forward_chunked(const float* table, int n_levels, int log2_size, int n_features,
+                                      const int32_t* level_res, const float* level_weights, const float* rays_o,
+                                      const float* rays_d, const float* mid, int n_samples, const float xyz_min[3],
+                                      const float xyz_max[3], int64_t n_points, const float* normals,
+                                      const float* W0, const float* b0, const float* W1, const float* b1,
+                                      float* colors, float* scratch_rows, int64_t scratch_count, void* stream);
+
 /* Blocks of vx_radiance_mlp_backward and the floats of one block's weight-gradient partial. */
 int vx_mlp_blocks(int64_t n_points);
 int vx_mlp_partial_floats(void);

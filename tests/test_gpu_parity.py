@@ -548,6 +548,48 @@ def test_appearance_rows_match_oracle(ld):
     assert bool((got[:, 2 * 10:32] == 0).all())  # levels 10..15 are skipped
 
 
+def test_chunked_inference_appearance_matches_rows_path():
+    """The inference form (rows through a small scratch, whole rays per chunk) gives the same colour
+    bits as the training form that keeps all rows: a 5-ray scratch (many chunks, a partial last one)
+    and a single-chunk scratch; the in-shared-memory fused kernel agrees within 1e-5; a scratch
+    smaller than one ray is refused."""
+    from voxneus_b200 import _lib, ops
+
+    torch.manual_seed(22)
+    cfg = ops.HashConfig(16, 2, 14)
+    nr, ns = 397, 127
+    emb = torch.rand(16, 2 ** 14, 2) * 0.2 - 0.1
+    o = torch.randn(nr, 3)
+    o = 2.5 * o / o.norm(dim=-1, keepdim=True)
+    d = -o / o.norm(dim=-1, keepdim=True) + 0.1 * torch.randn(nr, 3)
+    d = d / d.norm(dim=-1, keepdim=True)
+    mid = torch.sort(torch.rand(nr, ns) * 3.0 + 0.5, dim=-1).values
+    ed, od, dd, md, nd = (to(t.contiguous()) for t in (emb, o, d, mid, torch.randn(nr * ns, 3)))
+    wd = [to(t) for t in (torch.randn(64, 51) * 0.3, torch.randn(64) * 0.1, torch.randn(3, 64) * 0.3,
+                          torch.randn(3) * 0.1)]
+    P = _lib.ptr
+    lo, hi = _lib.f3((-1.0, -1.0, -1.0)), _lib.f3((1.0, 1.0, 1.0))
+    head = (P(ed), 16, 14, 2, cfg._res_c, cfg.level_weights(None), P(od), P(dd), P(md), ns, lo, hi, nr * ns, P(nd),
+            *[P(t) for t in wd])
+    st = _lib.stream_ptr(torch.device(DEV))
+    rows = torch.empty(nr * ns, 52, device=DEV)
+    ref = torch.empty(nr * ns, 3, device=DEV)
+    _lib.call("vx_appearance_mlp_forward", *head, P(ref), P(rows), 52, st)
+    for n_rows in (5 * ns, 262144):
+        scratch = torch.empty(n_rows, 52, device=DEV)
+        got = torch.full((nr * ns, 3), float("nan"), device=DEV)
+        _lib.call("vx_appearance_mlp_forward_chunked", *head, P(got), P(scratch), n_rows, st)
+        torch.cuda.synchronize()
+        assert torch.equal(got, ref), n_rows
+    fused = torch.empty(nr * ns, 3, device=DEV)
+    _lib.call("vx_appearance_mlp_forward", *head, P(fused), None, 0, st)
+    torch.cuda.synchronize()
+    assert_close(fused, ref, VAL_TOL, "rgb", scale=1.0)
+    small = torch.empty(ns - 1, 52, device=DEV)
+    with pytest.raises(RuntimeError, match="fewer than one ray"):
+        _lib.call("vx_appearance_mlp_forward_chunked", *head, P(fused), P(small), ns - 1, st)
+
+
 def test_fused_appearance_render_matches_cublas_path(golden):
     """Fused hash+MLP render gives the same values and gradients as the cuBLAS MLP path."""
     from voxneus_b200.rendering import RaySampler, compute_huber_color_loss

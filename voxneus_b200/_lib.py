@@ -54,6 +54,8 @@ _PROTOS = {
     "vx_radiance_mlp_forward": [P, I64, I64, I32, I32, I32, P, P, P, P, P, P],
     "vx_appearance_mlp_forward": [P, I32, I32, I32, HI3, HF3, P, P, P, I32, HF3, HF3, I64, P, P, P, P, P, P, P, I64,
                                   P],
+    "vx_appearance_mlp_forward_chunked": [P, I32, I32, I32, HI3, HF3, P, P, P, I32, HF3, HF3, I64, P, P, P, P, P,
+                                          P, P, I64, P],
     "vx_mlp_blocks": [I64],
     "vx_mlp_partial_floats": [],
     "vx_tensor_core_timeouts": [],

@@ -936,6 +936,17 @@ __global__ void __launch_bounds__(256) k_hash_rows(HashArgs a) {
   }
 }
 
+// k_hash_rows over a.P samples, one wave of resident blocks.
+void launch_hash_rows(const HashArgs& a, cudaStream_t st) {
+  static int rows_per_sm = 0;
+  if (rows_per_sm == 0) {
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_hash_rows, 256, 0) != cudaSuccess || nb < 1) nb = 4;
+    rows_per_sm = nb;
+  }
+  k_hash_rows<<<grid_for((a.P + kRowsPerBlock - 1) / kRowsPerBlock * 256, 256, rows_per_sm), 256, 0, st>>>(a);
+}
+
 template <bool kHashIn, bool kRowsOut>
 int launch_fwd(const HashArgs& a, const float* X, int64_t ldx, int64_t P, const MlpW& w, float* colors,
                cudaStream_t st) {
@@ -986,13 +997,7 @@ int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, i
   MlpW w{W0, b0, W1, b1};
   cudaStream_t st = (cudaStream_t)stream;
   if (rows) {  // training: rows gathered at high occupancy, then the MLP on the rows
-    static int rows_per_sm = 0;  // resident blocks per SM (one wave of the grid-stride loop)
-    if (rows_per_sm == 0) {
-      int nb = 0;
-      if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_hash_rows, 256, 0) != cudaSuccess || nb < 1) nb = 4;
-      rows_per_sm = nb;
-    }
-    k_hash_rows<<<grid_for((n_points + kRowsPerBlock - 1) / kRowsPerBlock * 256, 256, rows_per_sm), 256, 0, st>>>(a);
+    launch_hash_rows(a, st);
     if (int s = launch_fwd<false, false>(a, rows, ld_rows, n_points, w, colors, st)) return s;
     count_launches(2);
   } else {  // inference: features built in shared memory, nothing else written
@@ -1000,6 +1005,48 @@ int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, i
     count_launches(1);
   }
   return check_launch("appearance_mlp_forward");
+}
+
+int vx_appearance_mlp_forward_chunked(const float* table, int n_levels, int log2_size, int n_features,
+                                      const int32_t* level_res, const float* level_weights, const float* rays_o,
+                                      const float* rays_d, const float* mid, int n_samples, const float xyz_min[3],
+                                      const float xyz_max[3], int64_t n_points, const float* normals,
+                                      const float* W0, const float* b0, const float* W1, const float* b1,
+                                      float* colors, float* scratch_rows, int64_t scratch_count, void* stream) {
+  HashArgs a{};
+  if (int s = fill_hash(a, table, n_levels, log2_size, n_features, level_res, level_weights)) return s;
+  VX_REQUIRE(n_levels == 16, "the fused appearance MLP takes 16 hash levels x 2 features (got %d)", n_levels);
+  VX_REQUIRE(n_points >= 0 && n_samples >= 1, "bad sizes");
+  VX_REQUIRE(n_points % n_samples == 0, "n_points must be whole rays (a multiple of n_samples)");
+  if (n_points == 0) return VX_OK;
+  VX_REQUIRE(table && rays_o && rays_d && mid && xyz_min && xyz_max && normals && W0 && b0 && W1 && b1 && colors &&
+                 scratch_rows,
+             "null pointer");
+  VX_REQUIRE(((uintptr_t)scratch_rows & 15) == 0, "scratch rows must be 16-byte aligned");
+  VX_REQUIRE(scratch_count >= n_samples, "scratch holds %lld rows, fewer than one ray's %d samples",
+             (long long)scratch_count, n_samples);
+  fill_positions(a, nullptr, rays_o, rays_d, mid, n_samples, xyz_min, xyz_max);
+  a.ld = KP;
+  a.out = scratch_rows;
+  MlpW w{W0, b0, W1, b1};
+  cudaStream_t st = (cudaStream_t)stream;
+  const int64_t chunk = (scratch_count / n_samples) * n_samples;  // whole rays per pass
+  int launches = 0;
+  for (int64_t c0 = 0; c0 < n_points; c0 += chunk) {
+    const int64_t len = n_points - c0 < chunk ? n_points - c0 : chunk;
+    HashArgs ac = a;
+    const int64_t r0 = c0 / n_samples;
+    ac.rays_o = rays_o + 3 * r0;
+    ac.rays_d = rays_d + 3 * r0;
+    ac.mid = mid + c0;
+    ac.normals = normals + 3 * c0;
+    ac.P = len;
+    launch_hash_rows(ac, st);
+    if (int s = launch_fwd<false, false>(ac, scratch_rows, KP, len, w, colors + 3 * c0, st)) return s;
+    launches += 2;
+  }
+  count_launches(launches);
+  return check_launch("appearance_mlp_forward_chunked");
 }
 
 int vx_mlp_blocks(int64_t n_points) {
