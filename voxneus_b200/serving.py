@@ -12,10 +12,12 @@ Design:
   graph captured once (all graphs share one memory pool: they replay on one stream, one at a
   time), so a chunk costs one graph launch whatever kernels it contains.
 * The engine thread admits pending requests while the reserved device memory stays under the
-  budget (a fraction of the free HBM measured at start), then each iteration takes one chunk
-  from every active request in turn (round robin), so requests that arrive while others are
-  running start at the next iteration and their chunks interleave with the older ones on the
-  device; input copies run on a separate copy stream ahead of the compute stream. Results for
+  budget (a fraction of the free HBM measured at start). It keeps about AHEAD_MS of estimated
+  device work queued on the compute stream (each bucket's graph is timed once at start) and
+  fills it with chunks of the active request with the least remaining work, so a small request
+  that arrives behind large ones runs after at most that much queued work instead of behind
+  every chunk already admitted, while the queue still covers pauses of the engine thread; input
+  copies run on a separate copy stream ahead of the compute stream. Results for
   host requests come back through a fixed ring of pinned staging blocks on the copy stream and
   are copied into ordinary host tensors by the engine thread as each block lands (allocating
   pinned memory per request would cost milliseconds and synchronise the device).
@@ -144,6 +146,7 @@ class ServingEngine:
     QUERY_BUCKETS = (65536, 262144, 1048576)
     STAGE_BYTES = 16 << 20  # pinned staging block
     STAGE_BLOCKS = 8
+    AHEAD_MS = 20.0  # estimated device time kept queued on the compute stream
 
     def __init__(self, store: SceneStore, memory_fraction: float = 0.5, n_samples: int = 64,
                  n_importance: int = 64, budget_bytes: Optional[int] = None, fault_injector=None,
@@ -167,6 +170,20 @@ class ServingEngine:
                 self.graphs[(name, "query", size)] = _GraphBucket(m, "query", size, self.sampler, self.pool,
                                                                   self.compute)
         torch.cuda.synchronize(self.device)
+        # device time of one replay of each bucket (the first scene's graphs stand for all scenes)
+        self._cost_ms: Dict[Tuple[str, int], float] = {}
+        first = next(iter(store.scenes))
+        with torch.cuda.stream(self.compute):
+            for (name, kind, size), gb in self.graphs.items():
+                if name != first:
+                    continue
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                gb.graph.replay()
+                e0.record(self.compute)
+                gb.graph.replay()
+                e1.record(self.compute)
+                e1.synchronize()
+                self._cost_ms[(kind, size)] = max(e0.elapsed_time(e1), 1e-3)
         if budget_bytes is None:
             free, _ = torch.cuda.mem_get_info(self.device)
             budget_bytes = int(free * memory_fraction)
@@ -184,6 +201,8 @@ class ServingEngine:
         self._free_stage: List[int] = list(range(self.STAGE_BLOCKS))
         self._pieces: "collections.deque" = collections.deque()  # (req, src flat view, dst flat view)
         self._pieces_inflight: List[Tuple[torch.cuda.Event, int, Request, torch.Tensor, int]] = []
+        self._ahead: "collections.deque" = collections.deque()  # (completion event, cost ms) of queued chunks
+        self._ahead_ms = 0.0
         self._rid = 0
         self._stop = threading.Event()
         self._failed: Optional[str] = None
@@ -277,7 +296,22 @@ class ServingEngine:
             gb.graph.replay()
             for k, v in gb.out.items():
                 req._dev_out[k][start:start + cnt].copy_(v[:cnt])
+            evt = torch.cuda.Event()
+            evt.record(s)
+        cost = self._cost_ms[(req.kind, size)]
+        self._ahead.append((evt, cost))
+        self._ahead_ms += cost
         req._next = start + cnt
+
+    def _room(self) -> bool:
+        """Less than AHEAD_MS of estimated work still queued on the compute stream."""
+        while self._ahead and self._ahead[0][0].query():
+            self._ahead_ms -= self._ahead.popleft()[1]
+        return self._ahead_ms < self.AHEAD_MS
+
+    def _remaining(self, req: Request) -> float:
+        size = self._bucket(req.kind, req.n - req._next)
+        return (req.n - req._next) / size * self._cost_ms[(req.kind, size)]
 
     def _finish(self, req: Request):
         """All chunks of req are queued on the compute stream: queue its results for the host."""
@@ -348,11 +382,12 @@ class ServingEngine:
             while not self._stop.is_set():
                 self._admit()
                 self._poll()
-                if not self.active:
-                    if not self._busy():
+                if not self.active or not self._room():
+                    if not self._busy() or self.active:
                         time.sleep(0.0002)
                     continue
-                for req in list(self.active):
+                while self.active and self._room():
+                    req = min(self.active, key=self._remaining)  # least remaining work first
                     if self._fault is not None:
                         self._fault(req)
                     self._run_chunk(req)
