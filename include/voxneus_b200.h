@@ -231,7 +231,8 @@ int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, i
                               const float* b0, const float* W1, const float* b1, float* colors, float* rows,
                               int64_t ld_rows, void* stream);
 
-/* Inference form of vx_appearance_mlp_forward (no rows kept for an adjoint): the same colours,
+/* Inference form of vx_appearance_mlp_forward (models/voxneus.py:147-157 under no_grad, the path
+ * of scripts/render.py:35-54; no rows kept for an adjoint): the same colours,
  * computed chunk by chunk of whole rays through the caller's scratch rows (scratch_count x 52
  * floats, 16-byte aligned; at least n_samples rows): each chunk's rows are gathered into the
  * scratch and the MLP reads them back (the gather and the MLP each at their own best occupancy).
