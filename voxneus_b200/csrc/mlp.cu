@@ -21,7 +21,7 @@
 // The forward writes the colours (and, for the adjoint, the 52-float input rows); the adjoint
 // recomputes Z with the identical MMA sequence, writes dL/d(hash) and dL/d(normal), accumulates
 // dW0 (and db0 through a ones column) in TMEM across its tiles and dW1/db1 in registers, and
-// writes per-block partials that k_mlp_wgrad_reduce sums in block order (deterministic).
+// writes per-block partials that k_mlp_wgrad_reduce sums in a fixed order (deterministic).
 #include "hashgrid.cuh"
 #include "tc.cuh"
 
@@ -853,23 +853,36 @@ constexpr size_t kBwdSmemRegs = 2 * kWBytes + kXtBytes + kR1Bytes + sizeof(float
 constexpr size_t kBwdSmemBulk = kBwdSmemRegs + kRowsBytes;
 
 
-// Sum the per-block partials in block order into dW0 (64,51), dW1 (3,64), db0 (64), db1 (3).
-__global__ void k_mlp_wgrad_reduce(const float* __restrict__ partials, int nblocks, float* __restrict__ dW0,
-                                   float* __restrict__ db0, float* __restrict__ dW1, float* __restrict__ db1) {
-  for (int e = blockIdx.x * blockDim.x + threadIdx.x; e < WG; e += gridDim.x * blockDim.x) {
-    double acc = 0.0;
-    for (int b = 0; b < nblocks; ++b) acc += (double)partials[(int64_t)b * WG + e];
-    const float v = (float)acc;
-    if (e < NH * KP) {
-      const int n = e / KP, k = e % KP;
-      if (k < KIN) dW0[n * KIN + k] = v;
-    } else if (e < NH * KP + NO * NH) {
-      dW1[e - NH * KP] = v;
-    } else if (e < NH * KP + NO * NH + NH) {
-      db0[e - NH * KP - NO * NH] = v;
-    } else {
-      db1[e - NH * KP - NO * NH - NH] = v;
-    }
+// Sum the per-block partials into dW0 (64,51), dW1 (3,64), db0 (64), db1 (3), in a fixed order
+// (deterministic): a block of 32 x 8 threads takes 32 consecutive elements; thread (x, y) sums
+// the partials of blocks y, y + 8, y + 16, ... in increasing order, and the 8 slice sums are then
+// added in slice order. Loads are coalesced along the elements.
+constexpr int kReduceSlices = 8;
+
+__global__ void __launch_bounds__(256) k_mlp_wgrad_reduce(const float* __restrict__ partials, int nblocks,
+                                                          float* __restrict__ dW0, float* __restrict__ db0,
+                                                          float* __restrict__ dW1, float* __restrict__ db1) {
+  __shared__ double part[kReduceSlices][32];
+  const int e = blockIdx.x * 32 + threadIdx.x;
+  double acc = 0.0;
+  if (e < WG)
+    for (int b = threadIdx.y; b < nblocks; b += kReduceSlices) acc += (double)__ldg(partials + (int64_t)b * WG + e);
+  part[threadIdx.y][threadIdx.x] = acc;
+  __syncthreads();
+  if (threadIdx.y != 0 || e >= WG) return;
+  double sum = 0.0;
+#pragma unroll
+  for (int y = 0; y < kReduceSlices; ++y) sum += part[y][threadIdx.x];
+  const float v = (float)sum;
+  if (e < NH * KP) {
+    const int n = e / KP, k = e % KP;
+    if (k < KIN) dW0[n * KIN + k] = v;
+  } else if (e < NH * KP + NO * NH) {
+    dW1[e - NH * KP] = v;
+  } else if (e < NH * KP + NO * NH + NH) {
+    db0[e - NH * KP - NO * NH] = v;
+  } else {
+    db1[e - NH * KP - NO * NH - NH] = v;
   }
 }
 
@@ -1105,7 +1118,8 @@ int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int 
   } else {
     cudaMemsetAsync(partials, 0, sizeof(float) * WG, st);
   }
-  k_mlp_wgrad_reduce<<<(WG + 255) / 256, 256, 0, st>>>(partials, n_points > 0 ? nb : 1, dW0, db0, dW1, db1);
+  k_mlp_wgrad_reduce<<<(WG + 31) / 32, dim3(32, kReduceSlices), 0, st>>>(partials, n_points > 0 ? nb : 1, dW0, db0,
+                                                                        dW1, db1);
   count_launches(2);
   return check_launch("radiance_mlp_backward");
 }
