@@ -101,6 +101,18 @@ int vx_field_query(const float* grid, const int32_t res[3], const float xyz_min[
                    const float* xyz, int64_t n, float* sdf, float* grad, float* normal, int64_t* corners,
                    float* weights, void* stream);
 
+/* vx_field_query's sdf, grad and normal outputs (models/sdf_grid.py:90-160) for a large batch of
+ * scattered points, computed in spatial order: the points are sorted by the Morton code of their
+ * grid cell, queried in that order and each result is written at the point's own index, so the
+ * outputs are bit-identical to vx_field_query's. For grids larger than the L2 cache, where
+ * scattered points read every stencil from a different DRAM row. n < 2^31; workspace: at least
+ * vx_field_query_sorted_workspace(n, res) bytes, 256-byte aligned (0 when the size query fails,
+ * which needs a CUDA device). */
+int64_t vx_field_query_sorted_workspace(int64_t n, const int32_t res[3]);
+int vx_field_query_sorted(const float* grid, const int32_t res[3], const float xyz_min[3], const float xyz_max[3],
+                          const float* xyz, int64_t n, float* sdf, float* grad, float* normal, void* workspace,
+                          int64_t workspace_bytes, void* stream);
+
 /* Adjoint of vx_field_query: accumulates dL/dgrid from d_sdf (n), d_grad (n,3), d_normal (n,3)
  * (each nullable) into grad_grid. */
 int vx_field_query_backward(const float* grid, const int32_t res[3], const float xyz_min[3], const float xyz_max[3],

@@ -35,6 +35,8 @@ _PROTOS = {
     "vx_masked_adam_upd": [P, P, P, P, I64, I32, F32, F32, F32, F32, P],
     "vx_field_query": [P, HI3, HF3, HF3, P, I64, P, P, P, P, P, P],
     "vx_field_query_backward": [P, HI3, HF3, HF3, P, I64, P, P, P, P, P],
+    "vx_field_query_sorted_workspace": [I64, HI3],
+    "vx_field_query_sorted": [P, HI3, HF3, HF3, P, I64, P, P, P, P, I64, P],
     "vx_corners_weights": [P, I64, HI3, P, P, P],
     "vx_field_query_lattice": [P, HI3, HF3, HF3, HI3, HF3, HF3, P, P, P],
     "vx_near_far_from_sphere": [P, P, I64, F32, P, P, P],
@@ -95,6 +97,7 @@ _RESTYPES = {
     "vx_reg_stencil_blocks": I64,
     "vx_reg_stencil_workspace": I64,
     "vx_occupancy_workspace": I64,
+    "vx_field_query_sorted_workspace": I64,
     "vx_geometry_backward_det_workspace": ctypes.c_size_t,
     "vx_hash_backward_det_workspace": ctypes.c_size_t,
 }

@@ -75,10 +75,37 @@ def _grid3(grid: torch.Tensor):
 # ------------------------------------------------------------------ field queries ---------
 
 
+# Batches of scattered points against grids larger than the L2 cache are queried in Morton order
+# (vx_field_query_sorted; bit-identical outputs): at least this many points, this many grid bytes.
+SORTED_QUERY_MIN_POINTS = 1 << 20
+SORTED_QUERY_MIN_GRID_BYTES = 128 << 20
+
+
+def field_query_sorted(grid, xyz_min, xyz_max, xyz, sdf=True, grad=False, normal=False):
+    """field_query's sdf/grad/normal through the spatially sorted path."""
+    res = _grid3(grid)
+    xyz = check_tensor(xyz, "xyz")
+    n = xyz.numel() // 3
+    dev = xyz.device
+    need = int(L.query("vx_field_query_sorted_workspace", n, i3(res)))
+    if need <= 0:
+        raise RuntimeError("vx_field_query_sorted_workspace failed (needs a CUDA device, n < 2^31)")
+    ws = torch.empty(need, dtype=torch.uint8, device=dev)
+    o_sdf = torch.empty(n, device=dev) if sdf else None
+    o_grad = torch.empty(n, 3, device=dev) if grad else None
+    o_nrm = torch.empty(n, 3, device=dev) if normal else None
+    call("vx_field_query_sorted", ptr(grid), i3(res), f3(xyz_min), f3(xyz_max), ptr(xyz), n, ptr(o_sdf), ptr(o_grad),
+         ptr(o_nrm), ptr(ws), need, stream_ptr(dev))
+    return o_sdf, o_grad, o_nrm, None, None
+
+
 def field_query(grid, xyz_min, xyz_max, xyz, sdf=True, grad=False, normal=False, corners=False, weights=False):
     res = _grid3(grid)
     xyz = check_tensor(xyz, "xyz")
     n = xyz.numel() // 3
+    if (not corners and not weights and n >= SORTED_QUERY_MIN_POINTS and n < (1 << 31)
+            and grid.numel() * 4 >= SORTED_QUERY_MIN_GRID_BYTES):
+        return field_query_sorted(grid, xyz_min, xyz_max, xyz, sdf=sdf, grad=grad, normal=normal)
     dev = xyz.device
     o_sdf = torch.empty(n, device=dev) if sdf else None
     o_grad = torch.empty(n, 3, device=dev) if grad else None
