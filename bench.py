@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--rays", type=int, default=8192)
     ap.add_argument("--res", type=int, default=256)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--eager", action="store_true", help="train: launch every kernel from the host (no CUDA graph)")
     ap.add_argument("--workload", default="train", choices=["train", "field", "serving"],
                     help="train (the metric line), field (512^3 queries), serving (the request mix)")
     ap.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
@@ -296,7 +297,7 @@ def run_fused(args):
     from voxneus_b200 import _lib, ops
     from voxneus_b200 import synthetic
     from voxneus_b200.rendering import RaySampler
-    from voxneus_b200.training import FusedTrainer
+    from voxneus_b200.training import GRAPH_WARMUP_STEPS, FusedTrainer
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -316,7 +317,9 @@ def run_fused(args):
     _lib.load()
     torch.backends.cuda.matmul.allow_tf32 = False
     m, up_ms = make_scene(args.res, dev)
-    tr = FusedTrainer(m, RaySampler(N_SAMPLES, N_IMPORTANCE, perturb=True), band_voxels=3.0, exchange=exchange)
+    tr = FusedTrainer(m, RaySampler(N_SAMPLES, N_IMPORTANCE, perturb=True), band_voxels=3.0, exchange=exchange,
+                      cuda_graph=not args.eager)
+    graph_mode = tr.cuda_graph and exchange is None
     pool = synthetic.RayPool(seed=100 + rank)
     nb = 8
     batches = []
@@ -330,40 +333,58 @@ def run_fused(args):
 
             dist.barrier()
 
-    # warm-up, with a per-kernel attribution pass on the last warm-up step
-    for i in range(max(args.warmup, 3)):
-        timer = _lib.KernelTimer() if i == max(args.warmup, 3) - 1 else None
-        _lib.set_timer(timer)
+    # warm-up, with a per-kernel attribution pass on one eager step (the last warm-up step, or in
+    # graph mode the last eager step before the capture); the capture then records CUDA events
+    # around the dominant calls only
+    n_warm = max(args.warmup, 3)
+    attr_at = GRAPH_WARMUP_STEPS - 1 if graph_mode else n_warm - 1
+    dom_timer = None
+    for i in range(n_warm):
+        if i == attr_at:
+            timer = _lib.KernelTimer()
+            _lib.set_timer(timer)
+        elif graph_mode and dom_timer is not None and tr.graph() is None:
+            _lib.set_timer(dom_timer)  # this step captures the graph
         o, d, t = batches[i % nb]
         tr.step(o, d, t, step=i)
         _lib.set_timer(None)
+        if i == attr_at:
+            torch.cuda.synchronize()
+            per_kernel = {k: sum(v) for k, v in timer.durations_ms().items()}
+            nnz = int((m.sdf_grid.grid.grad != 0).sum().item()) if m.sdf_grid.grid.grad is not None else None
+            sizes = dict(n_rays=args.rays, n_samples=N_SAMPLES + N_IMPORTANCE, res=args.res, nnz=nnz)
+            hbm_cands = {k: v for k, v in per_kernel.items() if algorithmic_bytes(k, **sizes) is not None}
+            hbm_dom = max(hbm_cands, key=hbm_cands.get)  # the longest HBM/L2-bound call
+            cands = dict(hbm_cands)
+            cands.update({k: v for k, v in per_kernel.items() if k in MLP_FLOPS})
+            dominant = max(cands, key=cands.get)  # the longest call overall (tensor-core MLP or HBM-bound)
+            dom_timer = _lib.KernelTimer(sorted({dominant, hbm_dom}))
     torch.cuda.synchronize()
-    per_kernel = {k: sum(v) for k, v in timer.durations_ms().items()}
-    nnz = int((m.sdf_grid.grid.grad != 0).sum().item()) if m.sdf_grid.grid.grad is not None else None
-    sizes = dict(n_rays=args.rays, n_samples=N_SAMPLES + N_IMPORTANCE, res=args.res, nnz=nnz)
-    hbm_cands = {k: v for k, v in per_kernel.items() if algorithmic_bytes(k, **sizes) is not None}
-    hbm_dom = max(hbm_cands, key=hbm_cands.get)  # the longest HBM/L2-bound call
-    cands = dict(hbm_cands)
-    cands.update({k: v for k, v in per_kernel.items() if k in MLP_FLOPS})
-    dominant = max(cands, key=cands.get)  # the longest call overall (tensor-core MLP or HBM-bound)
+    graph_timer = GraphEventTimer(tr.graph(), dom_timer, args.steps) if graph_mode else None
 
-    # timed region: K steps, events around the dominant calls, clocks sampled alongside
-    dom_timer = _lib.KernelTimer(sorted({dominant, hbm_dom}))
+    # timed region: K steps, events around the dominant calls (eager: recorded by the library's
+    # timer; graph: the captured event nodes re-pointed to a fresh pair before each replay),
+    # clocks sampled alongside
     l0 = _lib.launch_count()
+    r0 = tr.replayed_launches
     barrier()
     torch.cuda.synchronize()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(local) as clk:
         ev0.record()
-        _lib.set_timer(dom_timer)
+        if not graph_mode:
+            dom_timer = _lib.KernelTimer(sorted({dominant, hbm_dom}))
+            _lib.set_timer(dom_timer)
         for i in range(args.steps):
             o, d, t = batches[i % nb]
-            tr.step(o, d, t, step=args.warmup + i)
+            if graph_timer is not None:
+                graph_timer.arm(i)
+            tr.step(o, d, t, step=n_warm + i)
         _lib.set_timer(None)
         ev1.record()
         torch.cuda.synchronize()
     barrier()
-    launches = _lib.launch_count() - l0
+    launches = _lib.launch_count() - l0 + tr.replayed_launches - r0
     ms = ev0.elapsed_time(ev1) / args.steps
     if world > 1:
         import torch.distributed as dist
@@ -372,7 +393,7 @@ def run_fused(args):
         dist.all_reduce(t_ms, op=dist.ReduceOp.MAX)
         ms = float(t_ms.item())
     value = args.rays * world / (ms / 1e3)
-    timed = dom_timer.durations_ms()
+    timed = graph_timer.durations_ms() if graph_timer is not None else dom_timer.durations_ms()
     peak, peak_kind = peak_hbm()
 
     def hbm_roofline(name):
@@ -414,7 +435,7 @@ def run_fused(args):
         o = ho.to(dev, non_blocking=True)
         d = hd.to(dev, non_blocking=True)
         t = ht.to(dev, non_blocking=True)
-        out = tr.step(o, d, t, step=args.warmup + args.steps + i)
+        out = tr.step(o, d, t, step=n_warm + args.steps + i)
         slots[i % 2:i % 2 + 1].copy_(out["loss_rgb"].reshape(1), non_blocking=True)
         evts[i % 2].record()
         if i >= 1:
@@ -448,6 +469,8 @@ def run_fused(args):
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, rays and targets)",
             "config": config(args, world), "e2e": e2e, "gpu_launches": int(launches),
+            "launch": "one CUDA graph replay per step (render .. optimizer; occupancy refresh and input copies "
+                      "eager)" if graph_mode else "eager (every kernel launched from the host)",
             "roofline": roofline, "roofline_hbm": roofline_hbm,
             "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(per_kernel.items(), key=lambda x: -x[1])},
             "mlp_tensor": mlp_tensor(per_kernel, args.rays * (N_SAMPLES + N_IMPORTANCE)),
@@ -457,6 +480,62 @@ def run_fused(args):
         import torch.distributed as dist
 
         dist.destroy_process_group()
+
+
+class GraphEventTimer:
+    """Per-replay CUDA events around kernels inside a captured step graph.
+
+    The capture recorded one external event pair around each timed call (the library's
+    KernelTimer under capture); before replay i, `arm(i)` points those event-record nodes of the
+    executable graph at the i-th fresh pair (cudaGraphExecEventRecordNodeSetEvent affects only
+    later launches), so each replay's kernel time is kept, on the stream the kernel runs on."""
+
+    def __init__(self, step_graph, captured, steps):
+        from cuda.bindings import runtime as rt
+
+        self.rt = rt
+        g = rt.cudaGraph_t(init_value=step_graph.graph.raw_cuda_graph())
+        self.exec = rt.cudaGraphExec_t(init_value=step_graph.graph.raw_cuda_graph_exec())
+        err, _, n = rt.cudaGraphGetNodes(g, 0)
+        self._check(err, "cudaGraphGetNodes")
+        err, nodes, _ = rt.cudaGraphGetNodes(g, n)
+        self._check(err, "cudaGraphGetNodes")
+        by_event = {}
+        for nd in nodes:
+            err, typ = rt.cudaGraphNodeGetType(nd)
+            self._check(err, "cudaGraphNodeGetType")
+            if typ == rt.cudaGraphNodeType.cudaGraphNodeTypeEventRecord:
+                err, ev = rt.cudaGraphEventRecordNodeGetEvent(nd)
+                self._check(err, "cudaGraphEventRecordNodeGetEvent")
+                by_event[int(ev)] = nd
+        self.nodes = {}
+        for name, pairs in captured.events.items():
+            if len(pairs) != 1:
+                raise RuntimeError(f"{name}: {len(pairs)} captured calls per step; the timer takes one")
+            s, e = pairs[0]
+            self.nodes[name] = (by_event[s.cuda_event], by_event[e.cuda_event])
+        self.pairs = {name: [] for name in self.nodes}
+        for name in self.nodes:
+            for _ in range(steps):
+                a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                a.record()  # creates the event handles
+                b.record()
+                self.pairs[name].append((a, b))
+
+    def _check(self, err, what):
+        if err != self.rt.cudaError_t.cudaSuccess:
+            raise RuntimeError(f"{what}: {err}")
+
+    def arm(self, i: int) -> None:
+        for name, (ns, ne) in self.nodes.items():
+            a, b = self.pairs[name][i]
+            for nd, ev in ((ns, a), (ne, b)):
+                (err,) = self.rt.cudaGraphExecEventRecordNodeSetEvent(self.exec, nd,
+                                                                      self.rt.cudaEvent_t(init_value=ev.cuda_event))
+                self._check(err, "cudaGraphExecEventRecordNodeSetEvent")
+
+    def durations_ms(self):
+        return {name: [a.elapsed_time(b) for a, b in pairs] for name, pairs in self.pairs.items()}
 
 
 def _events():

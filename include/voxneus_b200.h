@@ -89,8 +89,24 @@ typedef struct vx_adam_segment {
   int64_t n;
   int64_t step;
   float lr;
+  /* Optional, for launches replayed from a CUDA graph: device floats {lr / (1 - b1^t),
+   * 1 / sqrt(1 - b2^t), the step size to use when *lr_flag is nonzero}, written before each replay
+   * (vx_adam_torch_step_scalars); step and lr are then ignored. lr_flag may be NULL. */
+  const float* step_scalars;
+  const int* lr_flag;
 } vx_adam_segment;
 int vx_adam_torch(const vx_adam_segment* segs, int n_segs, float beta1, float beta2, float eps, void* stream);
+
+/* Host helpers giving exactly the scalars the updates above compute from (step, lr): the
+ * reference formula's step size lr * sqrt(1 - b2^t) / (1 - b1^t) in float, and torch's
+ * {lr / (1 - b1^t), 1 / sqrt(1 - b2^t)} in double rounded to float. */
+float vx_adam_reference_step_size(int step, float beta1, float beta2, float lr);
+void vx_adam_torch_step_scalars(int64_t step, float beta1, float beta2, float lr, float out[2]);
+
+/* vx_masked_adam_upd with its step size read from device memory (*step_size, from
+ * vx_adam_reference_step_size), for launches replayed from a CUDA graph. */
+int vx_masked_adam_upd_dev(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n,
+                           const float* step_size, float beta1, float beta2, float eps, void* stream);
 
 /* ------------------------------------------------------------ field queries --------------- */
 

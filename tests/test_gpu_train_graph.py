@@ -1,0 +1,95 @@
+"""The CUDA-graph training step against the eager step (training/trainer.py:166-393 as one unit).
+
+Same seeded model, rays and default-generator draws; deterministic adjoints (sorted segmented
+sums, no float atomics), so the two must agree bit for bit: parameters, Adam state, occupancy
+grid and the step's outputs, across an occupancy refresh between replays, the cosine LR schedule
+and the switch to the amplified-s variant (a second capture).
+"""
+
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+DEV = torch.device("cuda", 0)
+
+
+def _model():
+    from voxneus_b200.models import VoxNeuS
+
+    torch.manual_seed(3)
+    m = VoxNeuS(grid_res=32, hash_log2_size=12, occupancy_res=16).to(DEV)
+    with torch.no_grad():
+        m.sdf_grid.grid.add_(0.01 * torch.randn_like(m.sdf_grid.grid))
+        m.radiance_hash.encoder.embeddings.uniform_(-0.1, 0.1)
+    return m
+
+
+def _rays(n, seed):
+    g = torch.Generator().manual_seed(seed)
+    o = torch.randn(n, 3, generator=g)
+    o = 3.0 * o / o.norm(dim=-1, keepdim=True)
+    d = -o / 3.0 + 0.05 * torch.randn(n, 3, generator=g)
+    d = d / d.norm(dim=-1, keepdim=True)
+    return o.to(DEV), d.to(DEV), torch.rand(n, 3, generator=g).to(DEV)
+
+
+def _run(cuda_graph, steps, warmup_s):
+    from voxneus_b200.rendering import RaySampler
+    from voxneus_b200.training import FusedTrainer
+
+    m = _model()
+    tr = FusedTrainer(m, RaySampler(16, 16, perturb=True), band_voxels=3.0, s_warmup_steps=warmup_s,
+                      total_steps=10, occupancy_update_interval=3, cuda_graph=cuda_graph)
+    torch.manual_seed(11)  # the sampler's and occupancy refresh's draws (default CUDA generator)
+    hist = []
+    for i in range(steps):
+        o, d, t = _rays(256, 100 + i)
+        out = tr.step(o, d, t, step=i)
+        hist.append({k: v.clone() for k, v in out.items()})
+    torch.cuda.synchronize()
+    return m, tr, hist
+
+
+def test_graph_step_is_bitwise_the_eager_step():
+    from voxneus_b200 import ops
+
+    ops.set_deterministic(True)
+    try:
+        me, te, he = _run(False, 8, 5)
+        mg, tg, hg = _run(True, 8, 5)
+    finally:
+        ops.set_deterministic(False)
+    assert tg.graph() is not None and tg.graph().amplify  # captured, and recaptured with amplification
+    assert tg.replayed_launches > 0
+    for i, (a, b) in enumerate(zip(he, hg)):
+        for k in a:
+            assert torch.equal(a[k], b[k]), (i, k)
+    for (n, pa), pb in zip(me.named_parameters(), mg.parameters()):
+        assert torch.equal(pa, pb), n
+    for name in ("sdf_optimizer", "net_optimizer"):
+        oe, og = te.optimizers[name], tg.optimizers[name]
+        for pa, pb in zip(me.parameters(), mg.parameters()):
+            if pa in oe.state:
+                sa, sb = oe.state[pa], og.state[pb]
+                assert sa["step"] == sb["step"]
+                assert torch.equal(sa["exp_avg"], sb["exp_avg"]) and torch.equal(sa["exp_avg_sq"], sb["exp_avg_sq"])
+    assert torch.equal(me.occupancy_grid.density_grid, mg.occupancy_grid.density_grid)
+    assert torch.equal(me.occupancy_grid.occupancy_mask, mg.occupancy_grid.occupancy_mask)
+
+
+def test_graph_mode_falls_back_to_eager_with_explicit_randoms():
+    """Caller-supplied uniforms are not graph inputs: such a step runs eagerly (and drops the graph)."""
+    from voxneus_b200.rendering import RaySampler
+    from voxneus_b200.training import FusedTrainer
+
+    m = _model()
+    tr = FusedTrainer(m, RaySampler(16, 16, perturb=True), band_voxels=3.0, cuda_graph=True)
+    for i in range(3):
+        o, d, t = _rays(128, i)
+        tr.step(o, d, t, step=i)
+    assert tr.graph() is not None
+    o, d, t = _rays(128, 9)
+    randoms = m.draw_sampler_randoms(128, 16, 16, 4, DEV)
+    out = tr.step(o, d, t, step=3, randoms=randoms)
+    assert tr.graph() is None and torch.isfinite(out["loss_rgb"]).all()

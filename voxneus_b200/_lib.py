@@ -83,6 +83,9 @@ _PROTOS = {
     "vx_grid_upsample": [P, HI3, P, HI3, P],
     "vx_occupancy_workspace": [I64],
     "vx_adam_torch": [P, I32, F32, F32, F32, P],
+    "vx_adam_reference_step_size": [I32, F32, F32, F32],
+    "vx_adam_torch_step_scalars": [I64, F32, F32, F32, HF3],
+    "vx_masked_adam_upd_dev": [P, P, P, P, I64, P, F32, F32, F32, P],
     "vx_occupancy_points": [I32, HF3, HF3, P, P, P, I64, P, P],
     "vx_occupancy_query": [P, I32, HF3, HF3, P, I64, P, P],
     "vx_occupancy_update": [P, HI3, HF3, HF3, P, I32, HF3, HF3, P, P, P, I64, P, I32, F32, I32, F32, F32, P, P, P, I64,
@@ -97,6 +100,8 @@ _RESTYPES = {
     "vx_reg_stencil_blocks": I64,
     "vx_reg_stencil_workspace": I64,
     "vx_occupancy_workspace": I64,
+    "vx_adam_reference_step_size": ctypes.c_float,
+    "vx_adam_torch_step_scalars": None,
     "vx_field_query_sorted_workspace": I64,
     "vx_geometry_backward_det_workspace": ctypes.c_size_t,
     "vx_hash_backward_det_workspace": ctypes.c_size_t,
@@ -140,7 +145,10 @@ def exported_symbols() -> Sequence[str]:
 
 
 class KernelTimer:
-    """CUDA events around selected entry points, recorded on the launching (current) stream."""
+    """CUDA events around selected entry points, recorded on the launching (current) stream.
+
+    Under stream capture the events are recorded as external event nodes of the graph, so every
+    replay re-records them (the pair then times the latest replay)."""
 
     def __init__(self, names=None):
         self.names = None if names is None else set(names)
@@ -167,7 +175,9 @@ def call(name: str, *args):
     fn = getattr(lib, name)
     t = _timer
     if t is not None and t.wants(name):
-        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        ext = torch.cuda.is_current_stream_capturing()
+        s = torch.cuda.Event(enable_timing=True, external=ext)
+        e = torch.cuda.Event(enable_timing=True, external=ext)
         s.record()
         st = fn(*args)
         e.record()
@@ -218,7 +228,7 @@ class AdamSegment(ctypes.Structure):
 
     _fields_ = [("param", ctypes.c_void_p), ("grad", ctypes.c_void_p), ("exp_avg", ctypes.c_void_p),
                 ("exp_avg_sq", ctypes.c_void_p), ("n", ctypes.c_int64), ("step", ctypes.c_int64),
-                ("lr", ctypes.c_float)]
+                ("lr", ctypes.c_float), ("step_scalars", ctypes.c_void_p), ("lr_flag", ctypes.c_void_p)]
 
 
 def ptr(t: Optional[torch.Tensor]):

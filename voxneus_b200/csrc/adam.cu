@@ -30,6 +30,8 @@ struct AdamSeg {
   float step_size;
   float inv_bc2_sqrt;  // 1 / sqrt(1 - b2^t), torch formula only
   int vec;         // all four pointers 16-byte aligned
+  const float* dev;  // nullable: {step size, 1/sqrt(1 - b2^t), step size when *flag} read on the device
+  const int* flag;   // nullable: selects dev[2] instead of dev[0] when nonzero
 };
 
 struct AdamArgs {
@@ -38,8 +40,12 @@ struct AdamArgs {
   float b1, b2, eps;
 };
 
+struct AdamScal {
+  float step_size, inv_bc2_sqrt;
+};
+
 template <bool kMasked, bool kTorch>
-__device__ __forceinline__ void adam1(float& p, float g, float& m, float& v, const AdamSeg& s, const AdamArgs& a) {
+__device__ __forceinline__ void adam1(float& p, float g, float& m, float& v, const AdamScal& s, const AdamArgs& a) {
   if (kMasked && g == 0.0f) return;
   m = a.b1 * m + (1.0f - a.b1) * g;
   v = a.b2 * v + (1.0f - a.b2) * g * g;
@@ -50,7 +56,7 @@ __device__ __forceinline__ void adam1(float& p, float g, float& m, float& v, con
 }
 
 template <bool kMasked, bool kTorch>
-__device__ __forceinline__ void adam4(float4& p, const float4& g, float4& m, float4& v, const AdamSeg& s,
+__device__ __forceinline__ void adam4(float4& p, const float4& g, float4& m, float4& v, const AdamScal& s,
                                       const AdamArgs& a) {
   adam1<kMasked, kTorch>(p.x, g.x, m.x, v.x, s, a);
   adam1<kMasked, kTorch>(p.y, g.y, m.y, v.y, s, a);
@@ -64,6 +70,11 @@ __device__ __forceinline__ bool any_nonzero(const float4& g) {
 
 template <bool kMasked, bool kTorch>
 __device__ __forceinline__ void adam_segment(const AdamSeg& s, const AdamArgs& a, int64_t tid, int64_t nt) {
+  AdamScal sc{s.step_size, s.inv_bc2_sqrt};
+  if (s.dev) {  // scalars of this step from device memory (a launch replayed from a CUDA graph)
+    sc.step_size = (s.flag && *s.flag) ? s.dev[2] : s.dev[0];
+    sc.inv_bc2_sqrt = s.dev[1];
+  }
   int64_t done = 0;
   if (s.vec) {
     const int64_t n4 = s.n >> 2;
@@ -90,13 +101,13 @@ __device__ __forceinline__ void adam_segment(const AdamSeg& s, const AdamArgs& a
         vb = v4[j];
       }
       if (aa) {
-        adam4<kMasked, kTorch>(pa, ga, ma, va, s, a);
+        adam4<kMasked, kTorch>(pa, ga, ma, va, sc, a);
         p4[i] = pa;
         m4[i] = ma;
         v4[i] = va;
       }
       if (ab) {
-        adam4<kMasked, kTorch>(pb, gb, mb, vb, s, a);
+        adam4<kMasked, kTorch>(pb, gb, mb, vb, sc, a);
         p4[j] = pb;
         m4[j] = mb;
         v4[j] = vb;
@@ -108,7 +119,7 @@ __device__ __forceinline__ void adam_segment(const AdamSeg& s, const AdamArgs& a
     float p = s.p[i], m = s.m[i], v = s.v[i];
     const float g = __ldg(s.g + i);
     if (kMasked && g == 0.0f) continue;
-    adam1<kMasked, kTorch>(p, g, m, v, s, a);
+    adam1<kMasked, kTorch>(p, g, m, v, sc, a);
     s.p[i] = p;
     s.m[i] = m;
     s.v[i] = v;
@@ -150,10 +161,24 @@ int launch_adam(const AdamArgs& a, bool masked, bool torch_formula, int64_t tota
   return check_launch(torch_formula ? "adam_torch" : (masked ? "masked_adam_upd" : "adam_upd"));
 }
 
+// The reference's step size, evaluated on the host in float (adam_upd_kernel.cu:50).
+float reference_step_size(int step, float beta1, float beta2, float lr) {
+  return lr * sqrtf(1.0f - powf(beta2, (float)step)) / (1.0f - powf(beta1, (float)step));
+}
+
+// torch.optim.Adam's per-step scalars, evaluated on the host in double.
+void torch_step_scalars(int64_t step, float beta1, float beta2, float lr, float& step_size, float& inv_bc2_sqrt) {
+  const double bc1 = 1.0 - pow((double)beta1, (double)step);
+  const double bc2 = 1.0 - pow((double)beta2, (double)step);
+  step_size = (float)((double)lr / bc1);
+  inv_bc2_sqrt = (float)(1.0 / sqrt(bc2));
+}
+
 int adam_reference(bool masked, float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n,
-                   int step, float beta1, float beta2, float lr, float eps, void* stream) {
+                   int step, float beta1, float beta2, float lr, float eps, void* stream,
+                   const float* dev_step_size = nullptr) {
   VX_REQUIRE(n >= 0, "n < 0");
-  VX_REQUIRE(step >= 1, "step must be >= 1");
+  VX_REQUIRE(dev_step_size || step >= 1, "step must be >= 1");
   if (n == 0) return VX_OK;
   VX_REQUIRE(param && grad && exp_avg && exp_avg_sq, "null pointer");
   AdamArgs a{};
@@ -167,8 +192,8 @@ int adam_reference(bool masked, float* param, const float* grad, float* exp_avg,
   s.m = exp_avg;
   s.v = exp_avg_sq;
   s.n = n;
-  // the reference evaluates the step size on the host in float
-  s.step_size = lr * sqrtf(1.0f - powf(beta2, (float)step)) / (1.0f - powf(beta1, (float)step));
+  s.step_size = dev_step_size ? 0.0f : reference_step_size(step, beta1, beta2, lr);
+  s.dev = dev_step_size;  // dev_step_size[1] is not read by the reference formula
   s.vec = aligned16(param) && aligned16(grad) && aligned16(exp_avg) && aligned16(exp_avg_sq);
   return launch_adam(a, masked, false, n, (cudaStream_t)stream);
 }
@@ -190,6 +215,20 @@ int vx_masked_adam_upd(float* param, const float* grad, float* exp_avg, float* e
   return adam_reference(true, param, grad, exp_avg, exp_avg_sq, n, step, beta1, beta2, lr, eps, stream);
 }
 
+float vx_adam_reference_step_size(int step, float beta1, float beta2, float lr) {
+  return reference_step_size(step, beta1, beta2, lr);
+}
+
+void vx_adam_torch_step_scalars(int64_t step, float beta1, float beta2, float lr, float out[2]) {
+  torch_step_scalars(step, beta1, beta2, lr, out[0], out[1]);
+}
+
+int vx_masked_adam_upd_dev(float* param, const float* grad, float* exp_avg, float* exp_avg_sq, int64_t n,
+                           const float* step_size, float beta1, float beta2, float eps, void* stream) {
+  VX_REQUIRE(step_size, "null step size");
+  return adam_reference(true, param, grad, exp_avg, exp_avg_sq, n, 0, beta1, beta2, 0.0f, eps, stream, step_size);
+}
+
 int vx_adam_torch(const vx_adam_segment* segs, int n_segs, float beta1, float beta2, float eps, void* stream) {
   VX_REQUIRE(n_segs >= 0, "n_segs < 0");
   if (n_segs == 0) return VX_OK;
@@ -197,7 +236,7 @@ int vx_adam_torch(const vx_adam_segment* segs, int n_segs, float beta1, float be
   for (int k = 0; k < n_segs; ++k) {  // validate everything before the first launch
     const vx_adam_segment& in = segs[k];
     VX_REQUIRE(in.n >= 0, "segment %d: n < 0", k);
-    VX_REQUIRE(in.step >= 1, "segment %d: step must be >= 1", k);
+    VX_REQUIRE(in.step_scalars || in.step >= 1, "segment %d: step must be >= 1", k);
     VX_REQUIRE(in.n == 0 || (in.param && in.grad && in.exp_avg && in.exp_avg_sq), "segment %d: null pointer", k);
   }
   for (int base = 0; base < n_segs; base += kMaxSegs) {
@@ -215,10 +254,12 @@ int vx_adam_torch(const vx_adam_segment* segs, int n_segs, float beta1, float be
       s.m = in.exp_avg;
       s.v = in.exp_avg_sq;
       s.n = in.n;
-      const double bc1 = 1.0 - pow((double)beta1, (double)in.step);
-      const double bc2 = 1.0 - pow((double)beta2, (double)in.step);
-      s.step_size = (float)((double)in.lr / bc1);
-      s.inv_bc2_sqrt = (float)(1.0 / sqrt(bc2));
+      if (in.step_scalars) {
+        s.dev = in.step_scalars;
+        s.flag = in.lr_flag;
+      } else {
+        torch_step_scalars(in.step, beta1, beta2, in.lr, s.step_size, s.inv_bc2_sqrt);
+      }
       s.vec = aligned16(in.param) && aligned16(in.grad) && aligned16(in.exp_avg) && aligned16(in.exp_avg_sq);
       total += in.n;
     }

@@ -425,8 +425,7 @@ def hash_backward(d_emb, cfg, active_levels, pts, rays_o, rays_d, mid, n_samples
         if need == 0:
             raise RuntimeError("batch too large for one deterministic hash pass")
         ws = _workspace(dev, need)
-        res_d = torch.tensor(cfg.resolutions, dtype=torch.int32, device=dev)
-        lw_d = torch.tensor(list(lw)[:cfg.n_levels], dtype=torch.float32, device=dev)
+        res_d, lw_d = cfg.device_tables(dev, lw)
         call("vx_hash_encode_backward_det", ptr(d_emb), cfg.n_levels, cfg.log2_size, cfg.n_features, ptr(res_d),
              ptr(lw_d), ptr(pts), ptr(rays_o), ptr(rays_d), ptr(mid), n_samples,
              f3(xyz_min) if xyz_min is not None else None, f3(xyz_max) if xyz_max is not None else None, n_points,
@@ -448,6 +447,21 @@ class HashConfig:
         b = math.exp((math.log(finest) - math.log(base)) / max(n_levels - 1, 1))
         self.resolutions = [math.floor(base * (b ** lvl)) for lvl in range(n_levels)]
         self._res_c = L.iarr(self.resolutions)
+        self._dev_tables: Dict[tuple, tuple] = {}
+
+    def device_tables(self, dev, level_weights):
+        """(resolutions int32, level weights float32) on `dev`, cached per weights. Uploaded from
+        pinned host copies (kept alive here), so a first use inside CUDA graph capture is legal."""
+        idx = torch.device(dev).index
+        lw = tuple(float(w) for w in list(level_weights)[:self.n_levels])
+        key = (idx, lw)
+        t = self._dev_tables.get(key)
+        if t is None:
+            hr = torch.tensor(self.resolutions, dtype=torch.int32).pin_memory()
+            hw = torch.tensor(lw, dtype=torch.float32).pin_memory()
+            t = (hr.to(dev, non_blocking=True), hw.to(dev, non_blocking=True), hr, hw)
+            self._dev_tables[key] = t
+        return t[0], t[1]
 
     def level_weights(self, active_levels: Optional[float]):
         w = []
@@ -968,19 +982,34 @@ def grid_upsample(grid: torch.Tensor, new_res) -> torch.Tensor:
 
 
 def adam_torch(segments, beta1: float, beta2: float, eps: float):
-    """torch.optim.Adam's update over [(param, grad, exp_avg, exp_avg_sq, step, lr), ...] in place."""
+    """torch.optim.Adam's update over [(param, grad, exp_avg, exp_avg_sq, step, lr), ...] in place.
+
+    A segment may carry two more items, (..., scalars, flag): a float32 device tensor of 3 values
+    {lr / (1 - b1^t), 1 / sqrt(1 - b2^t), the step size used when flag is nonzero} read by the
+    kernel in place of (step, lr) — for launches replayed from a CUDA graph — and an int32 device
+    flag or None.
+    """
     import ctypes
 
     if not segments:
         return
     arr = (L.AdamSegment * len(segments))()
     dev = segments[0][0].device
-    for k, (p, g, m, v, step, lr) in enumerate(segments):
+    for k, seg in enumerate(segments):
+        p, g, m, v, step, lr = seg[:6]
+        scal, flag = (seg[6], seg[7]) if len(seg) > 6 else (None, None)
         for t, nm in ((p, "param"), (g, "grad"), (m, "exp_avg"), (v, "exp_avg_sq")):
             check_tensor(t, nm, device=dev)
             if t.numel() != p.numel():
                 raise RuntimeError(f"{nm} has {t.numel()} elements, param has {p.numel()}")
-        arr[k] = L.AdamSegment(p.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), p.numel(), int(step), float(lr))
+        if scal is not None:
+            check_tensor(scal, "scalars", device=dev)
+            if scal.numel() < 3:
+                raise RuntimeError("scalars holds fewer than 3 values")
+        if flag is not None:
+            check_tensor(flag, "flag", dtype=torch.int32, device=dev)
+        arr[k] = L.AdamSegment(p.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), p.numel(), int(step), float(lr),
+                               None if scal is None else scal.data_ptr(), None if flag is None else flag.data_ptr())
     call("vx_adam_torch", ctypes.cast(arr, ctypes.c_void_p), len(segments), float(beta1), float(beta2), float(eps),
          stream_ptr(dev))
 
@@ -990,3 +1019,27 @@ def adam_update(param, grad, exp_avg, exp_avg_sq, step, beta1, beta2, lr, eps, m
         check_tensor(t, nm)
     call("vx_masked_adam_upd" if masked else "vx_adam_upd", ptr(param), ptr(grad), ptr(exp_avg), ptr(exp_avg_sq),
          param.numel(), int(step), float(beta1), float(beta2), float(lr), float(eps), stream_ptr(param.device))
+
+
+def masked_adam_update_dev(param, grad, exp_avg, exp_avg_sq, step_size, beta1, beta2, eps):
+    """The masked (reference-formula) update with its step size read from device memory
+    (`step_size`: a float32 device tensor, from `adam_reference_step_size`)."""
+    for t, nm in ((param, "param"), (grad, "grad"), (exp_avg, "exp_avg"), (exp_avg_sq, "exp_avg_sq"),
+                  (step_size, "step_size")):
+        check_tensor(t, nm, device=param.device)
+    call("vx_masked_adam_upd_dev", ptr(param), ptr(grad), ptr(exp_avg), ptr(exp_avg_sq), param.numel(),
+         ptr(step_size), float(beta1), float(beta2), float(eps), stream_ptr(param.device))
+
+
+def adam_reference_step_size(step: int, beta1: float, beta2: float, lr: float) -> float:
+    """The reference formula's step size, exactly as the masked update computes it from (step, lr)."""
+    return float(L.query("vx_adam_reference_step_size", int(step), float(beta1), float(beta2), float(lr)))
+
+
+def adam_torch_step_scalars(step: int, beta1: float, beta2: float, lr: float):
+    """(lr / (1 - b1^t), 1 / sqrt(1 - b2^t)) exactly as `adam_torch` computes them from (step, lr)."""
+    import ctypes
+
+    out = (ctypes.c_float * 2)()
+    L.query("vx_adam_torch_step_scalars", int(step), float(beta1), float(beta2), float(lr), out)
+    return float(out[0]), float(out[1])

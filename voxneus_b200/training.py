@@ -7,6 +7,12 @@ render's corner bitmap, the fused eikonal + curvature stencil into grid.grad, an
 steps (masked grid Adam kernel; one multi-tensor Adam launch for the hash table, MLP and
 variance). No host synchronisation unless the s amplification is active (its LR rule needs the
 flag).
+
+With `cuda_graph=True` (single process), the step from render to optimizer is captured once per
+s-amplification setting into a CUDA graph and replayed: the step-dependent optimizer scalars
+(cosine LR, bias corrections, the amplified variance LR picked on the device from the flag) are
+computed on the host exactly as the eager optimizers compute them and copied to the device before
+each replay; the occupancy refresh runs eagerly between replays.
 """
 
 from __future__ import annotations
@@ -120,7 +126,7 @@ class FusedTrainer:
                  amplify_k: float = 5.0, s_warmup_steps: int = 5000, total_steps: int = 40000, lr_sdf: float = 0.1,
                  lr_hash: float = 0.01, lr_mlp: float = 0.001, lr_variance: float = 0.0005, up_sample_steps: int = 4,
                  huber_delta: float = 0.1, optimize: bool = True, exchange=None,
-                 occupancy_update_interval: int = 16, occupancy_seed: int = 0):
+                 occupancy_update_interval: int = 16, occupancy_seed: int = 0, cuda_graph: bool = False):
         self.model = model
         self.exchange = exchange  # dataparallel.GradExchange for world_size > 1
         self.sampler = sampler or RaySampler(64, 64, perturb=True)
@@ -152,21 +158,38 @@ class FusedTrainer:
         if exchange is not None:
             self.occ_generator = torch.Generator(device=dev)
             self.occ_generator.manual_seed(int(occupancy_seed))
+        self.cuda_graph = bool(cuda_graph)
+        self._graphs: Dict[bool, _StepGraph] = {}
+        self._eager_steps = 0
+        self.replayed_launches = 0  # library kernel launches run by graph replays (not in the launch counter)
+
+    def lr_factor(self, step: int) -> float:
+        """Cosine decay to 0.05 of the base LR (training/trainer.py:378-385)."""
+        return (math.cos(math.pi * step / max(self.total_steps, 1)) + 1.0) * 0.5 * (1.0 - 0.05) + 0.05
 
     def step(self, rays_o, rays_d, target, step: int = 0, randoms=None) -> Dict[str, torch.Tensor]:
+        """One training step. In graph mode the returned tensors are the graph's outputs, overwritten
+        by the next step (copy them to keep them)."""
         m = self.model
         if [int(r) for r in m.sdf_grid.res] != self.res:
             raise RuntimeError("grid resolution changed; build a new FusedTrainer after scale_volume_grid")
-        for opt in self.optimizers.values():
-            opt.zero_grad(set_to_none=True)
-        if not self.optimize:
-            for p in m.parameters():
-                p.grad = None
+        graphable = (self.cuda_graph and self.exchange is None and self.optimize and randoms is None
+                     and rays_o.is_cuda and torch.is_grad_enabled())
+        if graphable and self._eager_steps >= GRAPH_WARMUP_STEPS:
+            return self._graph_step(rays_o, rays_d, target, step)
+        self._graphs.clear()  # an eager step owns fresh gradients; replays would no longer see them
+        self._eager_steps += 1
+        return self._eager_step(rays_o, rays_d, target, step, randoms)
+
+    def _refresh_occupancy(self, step: int) -> None:
         if self.occupancy_update_interval > 0 and step % self.occupancy_update_interval == 0:
-            m.update_occupancy_grid(subsample_ratio=0.25, generator=self.occ_generator)
+            self.model.update_occupancy_grid(subsample_ratio=0.25, generator=self.occ_generator)
+
+    def _render_backward_regularize(self, rays_o, rays_d, target, amp_k: float, randoms=None):
+        """Render, loss, backward, gradient exchange, V_R and the regularizer stencil."""
+        m = self.model
         self.bitmap.zero_()
         self.counts.zero_()
-        amp_k = self.amplify_k if step >= self.s_warmup_steps else 0.0
         ex = self.exchange
         out = m.render(rays_o, rays_d, self.sampler, None, None, up_sample_steps=self.up_sample_steps,
                        sphere_radius=1.0, randoms=randoms, vr_bitmap=self.bitmap, extras=False,
@@ -186,8 +209,21 @@ class FusedTrainer:
                      self.filtered)
         ops.reg_stencil(grid.detach(), self.filtered, self.res, lo, hi, self.relax_radius, self.band, self.counts,
                         self.w_eik, self.w_curv, grid.grad, self.reg_losses)
+        return {"loss_rgb": loss.detach(), "loss_eik": self.reg_losses[0], "loss_curv": self.reg_losses[1],
+                "n_active": ops.final_count(self.counts, self.relax_radius, self.band), "rgb": out["rgb"].detach()}
+
+    def _eager_step(self, rays_o, rays_d, target, step: int, randoms) -> Dict[str, torch.Tensor]:
+        m = self.model
+        for opt in self.optimizers.values():
+            opt.zero_grad(set_to_none=True)
+        if not self.optimize:
+            for p in m.parameters():
+                p.grad = None
+        self._refresh_occupancy(step)
+        amp_k = self.amplify_k if step >= self.s_warmup_steps else 0.0
+        res = self._render_backward_regularize(rays_o, rays_d, target, amp_k, randoms)
         if self.optimize:
-            lr_factor = (math.cos(math.pi * step / max(self.total_steps, 1)) + 1.0) * 0.5 * (1.0 - 0.05) + 0.05
+            lr_factor = self.lr_factor(step)
             net = self.optimizers["net_optimizer"]
             net.param_groups[0]["lr"] = self.lr_hash * lr_factor
             net.param_groups[1]["lr"] = self.lr_mlp * lr_factor
@@ -195,5 +231,134 @@ class FusedTrainer:
             net.param_groups[2]["lr"] = self.lr_variance * (self.amplify_k if amplified else 1.0)
             for opt in self.optimizers.values():
                 opt.step()
-        return {"loss_rgb": loss.detach(), "loss_eik": self.reg_losses[0], "loss_curv": self.reg_losses[1],
-                "n_active": ops.final_count(self.counts, self.relax_radius, self.band), "rgb": out["rgb"].detach()}
+        return res
+
+    # ---------------------------------------------------------------- CUDA graph mode ------
+
+    def _graph_step(self, rays_o, rays_d, target, step: int) -> Dict[str, torch.Tensor]:
+        amplify = step >= self.s_warmup_steps
+        g = self._graphs.get(amplify)
+        if g is None:
+            self._graphs.clear()  # one captured variant at a time (amplification switches on once)
+            g = _StepGraph(self, rays_o, rays_d, target, amplify)
+            self._graphs[amplify] = g
+        self._refresh_occupancy(step)
+        g.run(rays_o, rays_d, target, step)
+        self.replayed_launches += g.launches
+        return g.outputs
+
+    def graph(self) -> Optional["_StepGraph"]:
+        """The captured step graph in use (None before the first graph step)."""
+        return next(iter(self._graphs.values()), None)
+
+
+GRAPH_WARMUP_STEPS = 2  # eager steps before the first capture (optimizer state, autograd, allocator)
+_SCALAR_SLOTS = 4  # pinned host copies of the per-step optimizer scalars in flight
+
+
+class _StepGraph:
+    """One captured training step (render .. optimizer) of a FusedTrainer.
+
+    Static inputs: rays_o, rays_d, target buffers (the caller's tensors are copied in) and a device
+    table of optimizer scalars: [grid step size, then per network parameter {lr/(1-b1^t),
+    1/sqrt(1-b2^t), step size when amplified}]. The sampler's uniforms come from torch's default
+    CUDA generator inside the graph (torch advances its offset per replay, so the draws are the
+    eager step's). Gradients live in the graph's memory pool and are rewritten by every replay.
+    """
+
+    def __init__(self, tr: FusedTrainer, rays_o, rays_d, target, amplify: bool):
+        m = tr.model
+        dev = rays_o.device
+        self.tr = tr
+        self.amplify = amplify
+        self.o = torch.empty_like(rays_o, memory_format=torch.contiguous_format)
+        self.d = torch.empty_like(rays_d, memory_format=torch.contiguous_format)
+        self.t = torch.empty_like(target, memory_format=torch.contiguous_format)
+        self.grid_opt = tr.optimizers["sdf_optimizer"]
+        self.net_opt = tr.optimizers["net_optimizer"]
+        if not isinstance(self.grid_opt, SparseGridAdam) or not isinstance(self.net_opt, FusedAdam):
+            raise RuntimeError("graph mode needs the masked grid Adam and the fused network Adam")
+        self.net_params = [(gi, p) for gi, grp in enumerate(self.net_opt.param_groups) for p in grp["params"]]
+        for opt in (self.grid_opt, self.net_opt):
+            for grp in opt.param_groups:
+                for p in grp["params"]:
+                    if not opt.state.get(p):
+                        raise RuntimeError("graph mode starts after an eager step has created the optimizer state")
+        n = 1 + 3 * len(self.net_params)
+        self.scalars = torch.zeros(n, device=dev)
+        self.host = torch.zeros(_SCALAR_SLOTS, n).pin_memory()
+        self.slot_events = [None] * _SCALAR_SLOTS
+        self.slot = 0
+        for opt in (self.grid_opt, self.net_opt):
+            opt.zero_grad(set_to_none=True)  # backward inside the capture allocates the gradients
+        amp_k = tr.amplify_k if amplify else 0.0
+        from . import _lib
+
+        self.graph = torch.cuda.CUDAGraph(keep_graph=True)
+        l0 = _lib.launch_count()
+        with torch.cuda.graph(self.graph):
+            self.outputs = tr._render_backward_regularize(self.o, self.d, self.t, amp_k)
+            self._optimizer_launches(m)
+        self.launches = _lib.launch_count() - l0
+        self.graph.instantiate()
+
+    def _optimizer_launches(self, m) -> None:
+        grid = m.sdf_grid.grid
+        b1, b2 = self.grid_opt.param_groups[0]["betas"]
+        st = self.grid_opt.state[grid]
+        ops.masked_adam_update_dev(grid, grid.grad, st["exp_avg"], st["exp_avg_sq"], self.scalars[0:1], b1, b2,
+                                   self.grid_opt.param_groups[0]["eps"])
+        flag = self.tr.amp_flag if self.amplify else None
+        batches: Dict[tuple, list] = {}
+        for k, (gi, p) in enumerate(self.net_params):
+            grp = self.net_opt.param_groups[gi]
+            if p.grad is None:
+                raise RuntimeError("graph mode needs a gradient for every network parameter")
+            st = self.net_opt.state[p]
+            b1, b2 = grp["betas"]
+            batches.setdefault((float(b1), float(b2), float(grp["eps"])), []).append(
+                (p, p.grad, st["exp_avg"], st["exp_avg_sq"], 0, 0.0, self.scalars[1 + 3 * k:4 + 3 * k],
+                 flag if gi == 2 else None))
+        for (b1, b2, eps), segs in batches.items():
+            ops.adam_torch(segs, b1, b2, eps)
+
+    def _advance_scalars(self, step: int) -> torch.Tensor:
+        """Advance the optimizer state's step counts as the eager optimizers do; return this
+        step's scalar row (the values the eager kernels would compute on the host)."""
+        tr = self.tr
+        row = [0.0] * self.scalars.numel()
+        grp = self.grid_opt.param_groups[0]
+        st = self.grid_opt.state[tr.model.sdf_grid.grid]
+        st["step"] += 1
+        b1, b2 = grp["betas"]
+        row[0] = ops.adam_reference_step_size(st["step"], b1, b2, grp["lr"])
+        f = tr.lr_factor(step)
+        lrs = [tr.lr_hash * f, tr.lr_mlp * f, tr.lr_variance]
+        for gi, lr in enumerate(lrs):
+            self.net_opt.param_groups[gi]["lr"] = lr
+        for k, (gi, p) in enumerate(self.net_params):
+            grp = self.net_opt.param_groups[gi]
+            st = self.net_opt.state[p]
+            st["step"] += 1
+            b1, b2 = grp["betas"]
+            ss, inv = ops.adam_torch_step_scalars(st["step"], b1, b2, lrs[gi])
+            amp = ss
+            if gi == 2 and self.amplify:
+                amp = ops.adam_torch_step_scalars(st["step"], b1, b2, tr.lr_variance * tr.amplify_k)[0]
+            row[1 + 3 * k:4 + 3 * k] = [ss, inv, amp]
+        return torch.tensor(row, dtype=torch.float32)
+
+    def run(self, rays_o, rays_d, target, step: int) -> None:
+        self.o.copy_(rays_o, non_blocking=True)
+        self.d.copy_(rays_d, non_blocking=True)
+        self.t.copy_(target, non_blocking=True)
+        s = self.slot
+        self.slot = (s + 1) % _SCALAR_SLOTS
+        if self.slot_events[s] is not None:
+            self.slot_events[s].synchronize()  # the copy that last read this pinned slot has run
+        self.host[s].copy_(self._advance_scalars(step))
+        self.scalars.copy_(self.host[s], non_blocking=True)
+        ev = self.slot_events[s] or torch.cuda.Event()
+        ev.record()
+        self.slot_events[s] = ev
+        self.graph.replay()
