@@ -739,6 +739,9 @@ class CompositeFn(torch.autograd.Function):
              ptr(ptsc), ptr(rays_o), ptr(s_c), int(s_is_variance), float(s_max), float(radius), ptr(bg), bg_per_ray,
              int(iter_cos), float(cos_anneal), nr, ns, *[ptr(t) for t in outs], stream_ptr(dev))
         ctx.save_for_backward(colors_c, sdf_c, nrm_c, s_c, d, z, dists, ptsc, rays_o, bg)
+        # outputs the loss does not use (depth, weights, alpha, ...) reach the adjoint as None, which
+        # the kernel reads as zero: no zero-filled (N, S) gradient tensors
+        ctx.set_materialize_grads(False)
         ctx.meta = (drs, dss, int(s_is_variance), float(s_max), float(radius), bg_per_ray, int(iter_cos),
                     float(cos_anneal), float(amplify_k), amp_flag, sdf.shape, normals.shape, colors.shape,
                     s_param.shape)
