@@ -140,6 +140,18 @@ __device__ __forceinline__ void issue_split(uint32_t t, uint32_t ah0, uint32_t a
   }
 }
 
+// issue_split with the A hi part in tensor memory: A_hi's K elements in columns ah_tmem + 8*ks of the
+// sample lanes (the same products in the same order as issue_split).
+__device__ __forceinline__ void issue_split_ts(uint32_t t, uint32_t ah_tmem, uint32_t al0, uint32_t b0, int ksteps) {
+#pragma unroll 1
+  for (int ks = 0; ks < ksteps; ++ks) {
+    const uint64_t al = tc::sdesc(al0 + ks * 4096, 2048, 128);
+    const uint64_t b = tc::sdesc(b0 + ks * 4096, 2048, 128);
+    tc::mma_tf32_ts(t, ah_tmem + 8 * ks, b, kId128, ks > 0);
+    tc::mma_tf32(t, al, b, kId64, true);
+  }
+}
+
 // Z = X W0^T into TMEM columns [tz, tz + 128) as two halves to add (same sequence in both passes).
 __device__ __forceinline__ void issue_z(uint32_t tz, uint32_t xh, uint32_t xl, uint32_t w2) {
   issue_split(tz, xh, xl, w2, 7);
@@ -320,15 +332,19 @@ constexpr size_t kFwdSmem = 2 * kXBytes + kWBytes + sizeof(float) * (NH + NO * N
 
 // Forward on contiguous 52-float rows (ldx = 52, 16-byte aligned): one CTA of 512 threads per SM
 // holding two independent tile slots of 256 threads (slot s = threads 256 s ..), which share the
-// stacked weights and alternate on the tensor core. Each slot has its own X operand, its own
-// 128 TMEM columns, and a row buffer that the next tile's rows reach by one bulk copy, issued as
-// soon as the slot has staged its current tile; a slot synchronises on its own named barrier, so
-// one slot's MMA wait overlaps the other's staging and epilogue. Row prefetch through registers
-// (the general kernel above) left every warp stalled on its 16-byte loads of 32 rows at a time.
-constexpr uint32_t kFwdSlotBytes = 2 * kXBytes + TM * KP * 4 + 2 * TM * 4 * 4;  // XH, XL, rows, RED
+// stacked weights and alternate on the tensor core. Each slot has its own X operand (the lo part in
+// shared memory, the hi part in TMEM columns 256 + 64 s, sample lanes, written with tcgen05.st),
+// its own 128 accumulator columns, and a row buffer that the next tile's rows reach by one bulk
+// copy, issued as soon as the slot has staged its current tile; a slot synchronises on its own
+// named barrier, so one slot's MMA wait overlaps the other's staging and epilogue. Row prefetch
+// through registers (the general kernel above) left every warp stalled on its 16-byte loads of 32
+// rows at a time.
+constexpr uint32_t kFwdSlotBytes = kXBytes + TM * KP * 4 + 2 * TM * 4 * 4;  // XL, rows, RED
 // shared head: W0 [hi; lo], b0, W1, b1, barriers, TMEM address, fail flags; slots from a 1 KB boundary
 constexpr size_t kFwd2Head = 1024 * ((kWBytes + sizeof(float) * (NH + NO * NH + 4) + 64 + 1023) / 1024);
 constexpr size_t kFwd2Smem = kFwd2Head + 2 * (size_t)kFwdSlotBytes;
+// one CTA per SM (it allocates all 512 TMEM columns): two would need <= 116 KB each
+static_assert(kFwd2Smem > 116 * 1024, "two forward CTAs would fit on an SM and contend for TMEM");
 
 __device__ __forceinline__ void slot_sync(int slot) {
   asm volatile("bar.sync %0, 256;" ::"r"(1 + slot) : "memory");
@@ -348,13 +364,12 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
   const int wid = stid >> 5, lane = tid & 31, q = wid & 3, hh = wid >> 2;
   const int m = 32 * q + lane;  // this thread's sample in its slot's tile
   uint8_t* SL = smem + kFwd2Head + (size_t)slot * kFwdSlotBytes;
-  uint8_t* XH = SL;
-  uint8_t* XL = XH + kXBytes;
+  uint8_t* XL = SL;
   uint8_t* ROWS = XL + kXBytes;
   float* RED = reinterpret_cast<float*>(ROWS + TM * KP * 4);  // [2][TM][4]
   uint64_t* bar = bars + 2 * slot;
   uint64_t* bar_rows = bar + 1;
-  // weights and each slot's X feature chunks 13..15 (zero), by all 512 threads
+  // weights and each slot's X_lo feature chunks 13..15 (zero), by all 512 threads
   for (int e = tid; e < NH * 64; e += blockDim.x) {
     const int n = e >> 6, k = e & 63;
     float h, l;
@@ -362,11 +377,8 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
     *reinterpret_cast<float*>(W2 + w_off(n, k)) = h;
     *reinterpret_cast<float*>(W2 + w_off(NH + n, k)) = l;
   }
-  for (int e = stid; e < 3 * TM; e += 256) {
-    const uint32_t off = x_off(13 + e / TM, e % TM);
-    *reinterpret_cast<float4*>(XH + off) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-    *reinterpret_cast<float4*>(XL + off) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-  }
+  for (int e = stid; e < 3 * TM; e += 256)
+    *reinterpret_cast<float4*>(XL + x_off(13 + e / TM, e % TM)) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
   for (int i = tid; i < NH; i += blockDim.x) B0[i] = w.b0[i];
   for (int i = tid; i < NO * NH; i += blockDim.x) W1s[i] = w.W1[i];
   if (tid < NO) B1[tid] = w.b1[tid];
@@ -375,12 +387,14 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
     tc::mbar_init(bar_rows, 1);
     s_fail[slot] = 0;
   }
-  if (tid < 32) tc::tmem_alloc(s_taddr, 256);
+  if (tid < 32) tc::tmem_alloc(s_taddr, 512);
   tc::fence_before_sync();
   __syncthreads();
   tc::fence_after_sync();
-  const uint32_t tcol = *s_taddr + 128 * slot;
-  const uint32_t xh = tc::smem_u32(XH), xl = tc::smem_u32(XL), w2 = tc::smem_u32(W2);
+  const uint32_t tcol = *s_taddr + 128 * slot;       // Z accumulator (two halves)
+  const uint32_t acol = *s_taddr + 256 + 64 * slot;  // X_hi: feature f in column acol + f
+  const uint32_t lane_base = (uint32_t)(32 * q) << 16;
+  const uint32_t xl = tc::smem_u32(XL), w2 = tc::smem_u32(W2);
   const int64_t ntiles = (P + TM - 1) / TM;
   const int64_t t0 = 2 * (int64_t)blockIdx.x + slot, tstride = 2 * (int64_t)gridDim.x;
   auto fetch_rows = [&](int64_t t) {
@@ -404,24 +418,45 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
     slot_sync(slot);
     if (s_fail[slot]) break;
     if (stid == 0) rows_pending = false;
-    {  // rows -> X (hi, lo); column 51 zero (the padding column may hold anything)
+    {  // rows -> X_hi (TMEM) and X_lo (sample rows); column 51 zero (the padding column may hold anything)
       const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * (KP * 4));
       const int c0 = hh ? 7 : 0;
+      float xh[28];  // features 4*c0 .. 4*c0 + 27 (hh = 1: 28..55, with 52..55 the zero chunk 13)
 #pragma unroll
       for (int j = 0; j < 7; ++j) {
         const int c = c0 + j;
         if (c < 13) {
           float4 u = valid ? rrow[c] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
           if (c == 12) u.w = 0.0f;
-          st_split4(XH, XL, x_off(c, m), u.x, u.y, u.z, u.w);
+          const float v[4] = {u.x, u.y, u.z, u.w};
+          float lo[4];
+#pragma unroll
+          for (int i = 0; i < 4; ++i) tc::split_tf32(v[i], xh[4 * j + i], lo[i]);
+          *reinterpret_cast<float4*>(XL + x_off(c, m)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+        } else {
+#pragma unroll
+          for (int i = 0; i < 4; ++i) xh[4 * j + i] = 0.0f;
         }
       }
+      // stores aligned to their widths (the column base is a multiple of 64)
+      const uint32_t ta = acol + lane_base + 4 * c0;
+      if (hh == 0) {
+        tc::tmem_st16(ta, xh);
+        tc::tmem_st8(ta + 16, xh + 16);
+        tc::tmem_st4(ta + 24, xh + 24);
+      } else {
+        tc::tmem_st4(ta, xh);
+        tc::tmem_st16(ta + 4, xh + 4);
+        tc::tmem_st8(ta + 20, xh + 20);
+      }
+      tc::tmem_wait_st();
     }
     tc::fence_smem_to_async();
+    tc::fence_before_sync();
     slot_sync(slot);
     if (stid == 0) {
       tc::fence_after_sync();
-      issue_z(tcol, xh, xl, w2);
+      issue_split_ts(tcol, acol, xl, w2, 7);
       tc::commit(bar);
       if (t + tstride < ntiles) {  // ROWS has been read: bring this slot's next tile
         fetch_rows(t + tstride);
@@ -435,7 +470,7 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
     if (s_fail[slot]) break;
     tc::fence_after_sync();
     float z[32];
-    tmem_ld_sum32(tcol + ((uint32_t)(32 * q) << 16) + 32 * hh, z);
+    tmem_ld_sum32(tcol + lane_base + 32 * hh, z);
     float p0, p1, p2;
     colour_partial(z, hh, B0, W1s, p0, p1, p2);
     float* r = RED + (hh * TM + m) * 4;
@@ -459,7 +494,7 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
   }
   tc::fence_before_sync();
   __syncthreads();
-  if (tid < 32) tc::tmem_dealloc(*s_taddr, 256);
+  if (tid < 32) tc::tmem_dealloc(*s_taddr, 512);
 }
 
 // Adjoint. d_out (P,3) -> d_hash (P,32), d_normal (P,3), per-block weight-gradient partials
@@ -469,13 +504,17 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
 // of 4 samples sit 1040 / 2064 bytes apart (one 16-byte pad per chunk slab).
 // Per tile: stage rows -> Z MMA -> epilogue (colours, dO, dW1 in registers, DZ) -> dX MMA ->
 // DZ^T -> dW0 MMA (overlapping the dX readout). TMEM columns: Z, then dX, in [0,128) (two halves
-// each); dW0 = [DZ_hi | DZ_lo]^T X_hi in [128,192) and x X_lo in [192,256).
+// each); dW0 = [DZ_hi | DZ_lo]^T X_hi in [128,192) and x X_lo in [192,256); dW1 sums in
+// [256,448); the hi part of the Z and dX MMAs' A operand (X_hi, then DZ_hi; sample lanes, K along
+// the columns) in [448,512), written by the threads with tcgen05.st, so it takes no shared-memory
+// stores or operand reads (the lo parts stay in R1).
 constexpr uint32_t kXtSlab = 16 * 128 + 16;   // X^T: 4 samples x 128 rows (features hi | features lo)
 constexpr uint32_t kDztSlab = 16 * 128 + 16;  // DZ^T: 4 samples x 128 rows (hidden hi | hidden lo)
 constexpr uint32_t kXtBytes = 32 * kXtSlab;
 constexpr uint32_t kR1Bytes = 66560;          // X (hi, lo) -> DZ (hi, lo) -> DZ^T, one at a time
 constexpr uint32_t kRowBytes = KP * 4;        // one 52-float input row
 constexpr uint32_t kRowsBytes = TM * kRowBytes;  // the next tile's rows, brought in by a bulk copy
+constexpr uint32_t kAhiCol = 448;                // TMEM column of A_hi (X_hi, then DZ_hi)
 
 __device__ __forceinline__ uint32_t xt_off(int f, int m) {
   return (uint32_t)((m >> 2) * kXtSlab + (f >> 3) * 128 + (f & 7) * 16 + (m & 3) * 4);
@@ -590,10 +629,12 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
       }
       if (tid == 0) rows_pending = false;
     }
-    // rows -> X (sample rows, R1) and X^T (feature rows); column 51 = 1 on real rows (db0)
+    // rows -> X_hi (TMEM, sample lanes), X_lo (sample rows, R1) and X^T (feature rows); column 51
+    // = 1 on real rows (db0)
     {
       const int c0 = hh ? 7 : 0;
       const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * kRowBytes);
+      float xh[28];  // features 4*c0 .. 4*c0 + 27 (hh = 1: 28..55, with 52..55 the zero chunk 13)
 #pragma unroll
       for (int jc = 0; jc < 7; ++jc) {
         const int c = c0 + jc;
@@ -605,27 +646,39 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
             u = pre[jc];
           float v[4] = {u.x, u.y, u.z, u.w};
           if (c == 12 && valid) v[3] = 1.0f;
-          float hi[4], lo[4];
+          float lo[4];
 #pragma unroll
           for (int i = 0; i < 4; ++i) {
-            tc::split_tf32(v[i], hi[i], lo[i]);
-            *reinterpret_cast<float*>(XT2 + xt_off(4 * c + i, m)) = hi[i];
+            tc::split_tf32(v[i], xh[4 * jc + i], lo[i]);
+            *reinterpret_cast<float*>(XT2 + xt_off(4 * c + i, m)) = xh[4 * jc + i];
             *reinterpret_cast<float*>(XT2 + xt_off(64 + 4 * c + i, m)) = lo[i];
           }
-          *reinterpret_cast<float4*>(R1 + x_off(c, m)) = make_float4(hi[0], hi[1], hi[2], hi[3]);
           *reinterpret_cast<float4*>(R1 + kXBytes + x_off(c, m)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+        } else {  // feature chunk 13 (columns 52..55) is inside the Z contraction: zero
+#pragma unroll
+          for (int i = 0; i < 4; ++i) xh[4 * jc + i] = 0.0f;
+          *reinterpret_cast<float4*>(R1 + kXBytes + x_off(13, m)) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
       }
-      if (hh) {  // feature chunk 13 (columns 52..55) is inside the Z contraction: zero it
-        *reinterpret_cast<float4*>(R1 + x_off(13, m)) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-        *reinterpret_cast<float4*>(R1 + kXBytes + x_off(13, m)) = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+      // X_hi at TMEM column kAhiCol + feature, in stores aligned to their widths
+      const uint32_t ta = tbase + lane_base + kAhiCol + 4 * c0;
+      if (hh == 0) {
+        tc::tmem_st16(ta, xh);
+        tc::tmem_st8(ta + 16, xh + 16);
+        tc::tmem_st4(ta + 24, xh + 24);
+      } else {
+        tc::tmem_st4(ta, xh);
+        tc::tmem_st16(ta + 4, xh + 4);
+        tc::tmem_st8(ta + 20, xh + 20);
       }
+      tc::tmem_wait_st();
     }
     tc::fence_smem_to_async();
+    tc::fence_before_sync();
     __syncthreads();
     if (tid == 0) {
       tc::fence_after_sync();
-      issue_z(tbase, r1, r1 + kXBytes, w2);
+      issue_split_ts(tbase, tbase + kAhiCol, r1 + kXBytes, w2, 7);
       tc::commit(bar);
       if (kBulk && t + gridDim.x < ntiles) {  // ROWS has been read: bring the next tile's rows
         fetch_rows(t + gridDim.x);
@@ -661,7 +714,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
 #pragma unroll
       for (int c = 0; c < NO; ++c) sb[c] += d[c];
     }
-    // dW1 (TMEM accumulators), dL/dz (kept in z), DZ (sample rows) into R1: the Z MMA has read X
+    // dW1 (TMEM accumulators), dL/dz (kept in z), then DZ: the Z MMA has read X
 #pragma unroll
     for (int j4 = 0; j4 < 8; ++j4) {
       const float4 b = *reinterpret_cast<const float4*>(B0 + 32 * hh + 4 * j4);
@@ -701,19 +754,19 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
       const float v = z[j];
       tc::split_tf32(v, z[j], zl[j]);
     }
+    // DZ_hi into TMEM (over X_hi: the Z MMA has completed), DZ_lo (sample rows) into R1
+    tc::tmem_st32(tbase + lane_base + kAhiCol + 32 * hh, z);
 #pragma unroll
-    for (int j4 = 0; j4 < 8; ++j4) {
-      const uint32_t off = x_off(8 * hh + j4, m);
-      *reinterpret_cast<float4*>(R1 + off) = make_float4(z[4 * j4], z[4 * j4 + 1], z[4 * j4 + 2], z[4 * j4 + 3]);
-      *reinterpret_cast<float4*>(R1 + kXBytes + off) =
+    for (int j4 = 0; j4 < 8; ++j4)
+      *reinterpret_cast<float4*>(R1 + kXBytes + x_off(8 * hh + j4, m)) =
           make_float4(zl[4 * j4], zl[4 * j4 + 1], zl[4 * j4 + 2], zl[4 * j4 + 3]);
-    }
+    tc::tmem_wait_st();
     tc::fence_smem_to_async();
     tc::fence_before_sync();
     __syncthreads();
     if (tid == 0) {  // dX = DZ W0 (B = W0^T [hi; lo], feature rows) into the columns Z used
       tc::fence_after_sync();
-      issue_split(tbase, r1, r1 + kXBytes, wt2, 8);
+      issue_split_ts(tbase, tbase + kAhiCol, r1 + kXBytes, wt2, 8);
       tc::commit(bar);
     }
     ok = tc::mbar_wait(bar, phase, kWaitLimit);
