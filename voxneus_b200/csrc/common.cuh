@@ -218,8 +218,21 @@ __device__ __forceinline__ void eq7_weights(const Eq7& e, float w[8]) {
 __device__ __forceinline__ float fd_den(int p, int m, float eps) { return fmaxf((float)(p - m) * eps, eps); }
 
 // Interpolated gradient g = sum_k w_k n[c_k].
-__device__ __forceinline__ void eq7_gradient(const float* __restrict__ f, const Grid& g, const Eq7& e,
-                                             const float w[8], float out[3]) {
+// The 2x2x2 block of corner values (corner k: x bit 4, y bit 2, z bit 1).
+__device__ __forceinline__ void eq7_load_block(const float* __restrict__ f, const Grid& g, const Eq7& e, float c[8]) {
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    c[k] = __ldg(f + lin3(g, (k & 4) ? e.x1 : e.x0, (k & 2) ? e.y1 : e.y0, (k & 1) ? e.z1 : e.z0));
+}
+
+// Eq.7 gradient from the corner block c: per corner the central differences of Eq.6 (indices
+// clamped, one-sided at the border) blended with the corner weights. A corner's neighbour towards
+// the other side of the cell is a block value (the lower corner's +1 neighbour is the upper corner by
+// definition; the upper corner's -1 neighbour is the lower one unless the cell is degenerate at the
+// border, then it is loaded), so a point loads 8 + 24 values instead of 48; the arithmetic and its
+// order are those of the per-corner formula (geometry/gradients.py:59-139).
+__device__ __forceinline__ void eq7_gradient_block(const float* __restrict__ f, const Grid& g, const Eq7& e,
+                                                   const float w[8], const float c[8], float out[3]) {
   float gx = 0.0f, gy = 0.0f, gz = 0.0f;
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
@@ -229,9 +242,31 @@ __device__ __forceinline__ void eq7_gradient(const float* __restrict__ f, const 
     const int xp = min(x + 1, g.rx - 1), xm = max(x - 1, 0);
     const int yp = min(y + 1, g.ry - 1), ym = max(y - 1, 0);
     const int zp = min(z + 1, g.rz - 1), zm = max(z - 1, 0);
-    const float nx = (__ldg(f + lin3(g, xp, y, z)) - __ldg(f + lin3(g, xm, y, z))) / fd_den(xp, xm, g.eps[0]);
-    const float ny = (__ldg(f + lin3(g, x, yp, z)) - __ldg(f + lin3(g, x, ym, z))) / fd_den(yp, ym, g.eps[1]);
-    const float nz = (__ldg(f + lin3(g, x, y, zp)) - __ldg(f + lin3(g, x, y, zm))) / fd_den(zp, zm, g.eps[2]);
+    float fxp, fxm, fyp, fym, fzp, fzm;
+    if (k & 4) {
+      fxp = __ldg(f + lin3(g, xp, y, z));
+      fxm = xm == e.x0 ? c[k ^ 4] : __ldg(f + lin3(g, xm, y, z));
+    } else {
+      fxp = c[k ^ 4];  // xp == e.x1
+      fxm = __ldg(f + lin3(g, xm, y, z));
+    }
+    if (k & 2) {
+      fyp = __ldg(f + lin3(g, x, yp, z));
+      fym = ym == e.y0 ? c[k ^ 2] : __ldg(f + lin3(g, x, ym, z));
+    } else {
+      fyp = c[k ^ 2];  // yp == e.y1
+      fym = __ldg(f + lin3(g, x, ym, z));
+    }
+    if (k & 1) {
+      fzp = __ldg(f + lin3(g, x, y, zp));
+      fzm = zm == e.z0 ? c[k ^ 1] : __ldg(f + lin3(g, x, y, zm));
+    } else {
+      fzp = c[k ^ 1];  // zp == e.z1
+      fzm = __ldg(f + lin3(g, x, y, zm));
+    }
+    const float nx = (fxp - fxm) / fd_den(xp, xm, g.eps[0]);
+    const float ny = (fyp - fym) / fd_den(yp, ym, g.eps[1]);
+    const float nz = (fzp - fzm) / fd_den(zp, zm, g.eps[2]);
     gx = fmaf(w[k], nx, gx);
     gy = fmaf(w[k], ny, gy);
     gz = fmaf(w[k], nz, gz);
@@ -239,6 +274,27 @@ __device__ __forceinline__ void eq7_gradient(const float* __restrict__ f, const 
   out[0] = gx;
   out[1] = gy;
   out[2] = gz;
+}
+
+__device__ __forceinline__ void eq7_gradient(const float* __restrict__ f, const Grid& g, const Eq7& e,
+                                             const float w[8], float out[3]) {
+  float c[8];
+  eq7_load_block(f, g, e, c);
+  eq7_gradient_block(f, g, e, w, c, out);
+}
+
+// query_sdf reusing an Eq.7 corner block: when grid_sample's cell is the same cell with all eight
+// corners inside the grid (interior points), its corner values are c (same accumulation order);
+// otherwise the corners are loaded.
+__device__ __forceinline__ float query_sdf_block(const float* __restrict__ f, const Grid& g, float px, float py,
+                                                 float pz, const Eq7& e, const float c[8]) {
+  Tri t;
+  gs_setup(g, px, py, pz, t);
+  if (t.inb != 0xffu || t.x0 != e.x0 || t.y0 != e.y0 || t.z0 != e.z0) return gs_sample(f, g, t);
+  float acc = 0.0f;
+#pragma unroll
+  for (int k = 0; k < 8; ++k) acc = fmaf(c[k], t.w[k], acc);
+  return acc;
 }
 
 __device__ __forceinline__ float norm3(float x, float y, float z) { return sqrtf(x * x + y * y + z * z); }
@@ -268,8 +324,12 @@ __device__ __forceinline__ void normalize_eps_bwd(const float gr[3], float len, 
 }
 
 // Scatter of dL/dg into the 32-value Eq.7 stencil: grid[c_k +- e_a] += +-w_k dL/dg_a / den.
-__device__ __forceinline__ void eq7_scatter(float* __restrict__ gg, const Grid& g, const Eq7& e, const float w[8],
-                                            const float dg[3]) {
+// Adjoint of eq7_gradient: dL/dg scattered into the Eq.6 differences. Contributions that land on
+// the cell's own corners are summed in acc (which may already hold other terms for those corners,
+// e.g. the SDF's) and added with one atomic per corner; the 24 outer face neighbours take one each:
+// 32 atomics per point instead of 48 (the atomic order is unspecified either way).
+__device__ __forceinline__ void eq7_scatter_acc(float* __restrict__ gg, const Grid& g, const Eq7& e,
+                                                const float w[8], const float dg[3], float acc[8]) {
 #pragma unroll
   for (int k = 0; k < 8; ++k) {
     const int x = (k & 4) ? e.x1 : e.x0;
@@ -281,13 +341,38 @@ __device__ __forceinline__ void eq7_scatter(float* __restrict__ gg, const Grid& 
     const float vx = (w[k] * dg[0]) / fd_den(xp, xm, g.eps[0]);
     const float vy = (w[k] * dg[1]) / fd_den(yp, ym, g.eps[1]);
     const float vz = (w[k] * dg[2]) / fd_den(zp, zm, g.eps[2]);
-    atomicAdd(gg + lin3(g, xp, y, z), vx);
-    atomicAdd(gg + lin3(g, xm, y, z), -vx);
-    atomicAdd(gg + lin3(g, x, yp, z), vy);
-    atomicAdd(gg + lin3(g, x, ym, z), -vy);
-    atomicAdd(gg + lin3(g, x, y, zp), vz);
-    atomicAdd(gg + lin3(g, x, y, zm), -vz);
+    if (k & 4) {
+      atomicAdd(gg + lin3(g, xp, y, z), vx);
+      if (xm == e.x0) acc[k ^ 4] -= vx; else atomicAdd(gg + lin3(g, xm, y, z), -vx);
+    } else {
+      acc[k ^ 4] += vx;  // xp == e.x1
+      atomicAdd(gg + lin3(g, xm, y, z), -vx);
+    }
+    if (k & 2) {
+      atomicAdd(gg + lin3(g, x, yp, z), vy);
+      if (ym == e.y0) acc[k ^ 2] -= vy; else atomicAdd(gg + lin3(g, x, ym, z), -vy);
+    } else {
+      acc[k ^ 2] += vy;  // yp == e.y1
+      atomicAdd(gg + lin3(g, x, ym, z), -vy);
+    }
+    if (k & 1) {
+      atomicAdd(gg + lin3(g, x, y, zp), vz);
+      if (zm == e.z0) acc[k ^ 1] -= vz; else atomicAdd(gg + lin3(g, x, y, zm), -vz);
+    } else {
+      acc[k ^ 1] += vz;  // zp == e.z1
+      atomicAdd(gg + lin3(g, x, y, zm), -vz);
+    }
   }
+#pragma unroll
+  for (int k = 0; k < 8; ++k)
+    if (acc[k] != 0.0f)
+      atomicAdd(gg + lin3(g, (k & 4) ? e.x1 : e.x0, (k & 2) ? e.y1 : e.y0, (k & 1) ? e.z1 : e.z0), acc[k]);
+}
+
+__device__ __forceinline__ void eq7_scatter(float* __restrict__ gg, const Grid& g, const Eq7& e, const float w[8],
+                                            const float dg[3]) {
+  float acc[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+  eq7_scatter_acc(gg, g, e, w, dg, acc);
 }
 
 // Scatter of dL/dsdf into the grid_sample corners.

@@ -45,15 +45,17 @@ __global__ void __launch_bounds__(256) k_field_query(const float* __restrict__ f
                                                      float* __restrict__ weights) {
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
     const float px = xyz[3 * i], py = xyz[3 * i + 1], pz = xyz[3 * i + 2];
-    if (sdf) sdf[i] = query_sdf(f, g, px, py, pz);
+    if (sdf && !(grad || normal)) sdf[i] = query_sdf(f, g, px, py, pz);
     if (grad || normal || corners || weights) {
       Eq7 e;
       eq7_setup(g, px, py, pz, e);
       float w[8];
       eq7_weights(e, w);
       if (grad || normal) {
-        float gr[3], nn[3], len;
-        eq7_gradient(f, g, e, w, gr);
+        float c[8], gr[3], nn[3], len;  // the cell's corner values, shared by the SDF and the gradient
+        eq7_load_block(f, g, e, c);
+        if (sdf) sdf[i] = query_sdf_block(f, g, px, py, pz, e, c);
+        eq7_gradient_block(f, g, e, w, c, gr);
         if (grad) {
           grad[3 * i] = gr[0];
           grad[3 * i + 1] = gr[1];
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(256) k_field_query(const float* __restrict__ f
 
 // Adjoint of k_field_query with respect to the grid: d_sdf (n), d_grad (n,3), d_normal (n,3),
 // each optional.
-__global__ void __launch_bounds__(256) k_field_query_bwd(const float* __restrict__ f, Grid g,
+__global__ void __launch_bounds__(256, 4) k_field_query_bwd(const float* __restrict__ f, Grid g,
                                                          const float* __restrict__ xyz, int64_t n,
                                                          const float* __restrict__ d_sdf,
                                                          const float* __restrict__ d_grad,
@@ -130,7 +132,7 @@ __device__ __forceinline__ float lattice_coord(float lo, float hi, int n, int i)
   return __fsub_rn(hi, __fmul_rn(step, (float)(n - 1 - i)));
 }
 
-__global__ void __launch_bounds__(256) k_field_lattice(const float* __restrict__ f, Grid g, int nx, int ny, int nz,
+__global__ void __launch_bounds__(256, 4) k_field_lattice(const float* __restrict__ f, Grid g, int nx, int ny, int nz,
                                                        float lx, float ly, float lz, float hx, float hy, float hz,
                                                        float* __restrict__ sdf, float* __restrict__ normal) {
   const int64_t total = (int64_t)nx * ny * nz;
@@ -140,13 +142,15 @@ __global__ void __launch_bounds__(256) k_field_lattice(const float* __restrict__
     const int j = (int)(r % ny);
     const int ii = (int)(r / ny);
     const float px = lattice_coord(lx, hx, nx, ii), py = lattice_coord(ly, hy, ny, j), pz = lattice_coord(lz, hz, nz, k);
-    if (sdf) sdf[i] = query_sdf(f, g, px, py, pz);
+    if (sdf && !normal) sdf[i] = query_sdf(f, g, px, py, pz);
     if (normal) {
       Eq7 e;
       eq7_setup(g, px, py, pz, e);
-      float w[8], gr[3], nn[3], len;
+      float c[8], w[8], gr[3], nn[3], len;
+      eq7_load_block(f, g, e, c);
+      if (sdf) sdf[i] = query_sdf_block(f, g, px, py, pz, e, c);
       eq7_weights(e, w);
-      eq7_gradient(f, g, e, w, gr);
+      eq7_gradient_block(f, g, e, w, c, gr);
       normalize_eps(gr, nn, len);
       normal[3 * i] = nn[0];
       normal[3 * i + 1] = nn[1];

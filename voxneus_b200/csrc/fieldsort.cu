@@ -43,14 +43,16 @@ __global__ void __launch_bounds__(256) k_field_query_order(const float* __restri
   for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < n; j += (int64_t)gridDim.x * blockDim.x) {
     const int64_t i = __ldg(order + j);
     const float px = __ldg(xyz + 3 * i), py = __ldg(xyz + 3 * i + 1), pz = __ldg(xyz + 3 * i + 2);
-    if (sdf) sdf[i] = query_sdf(f, g, px, py, pz);
+    if (sdf && !(grad || normal)) sdf[i] = query_sdf(f, g, px, py, pz);
     if (grad || normal) {
       Eq7 e;
       eq7_setup(g, px, py, pz, e);
-      float w[8];
+      float c[8], w[8];
+      eq7_load_block(f, g, e, c);
+      if (sdf) sdf[i] = query_sdf_block(f, g, px, py, pz, e, c);
       eq7_weights(e, w);
       float gr[3], nn[3], len;
-      eq7_gradient(f, g, e, w, gr);
+      eq7_gradient_block(f, g, e, w, c, gr);
       if (grad) {
         grad[3 * i] = gr[0];
         grad[3 * i + 1] = gr[1];

@@ -16,7 +16,7 @@ namespace vx {
 
 // ------------------------------- geometry -------------------------------------------------
 
-__global__ void __launch_bounds__(256) k_geometry_fwd(const float* __restrict__ f, Grid g,
+__global__ void __launch_bounds__(256, 4) k_geometry_fwd(const float* __restrict__ f, Grid g,
                                                       const float* __restrict__ rays_o,
                                                       const float* __restrict__ rays_d,
                                                       const float* __restrict__ mid, int64_t n, int S,
@@ -28,12 +28,14 @@ __global__ void __launch_bounds__(256) k_geometry_fwd(const float* __restrict__ 
     const float px = ray_at(__ldg(rays_o + 3 * r), __ldg(rays_d + 3 * r), t);
     const float py = ray_at(__ldg(rays_o + 3 * r + 1), __ldg(rays_d + 3 * r + 1), t);
     const float pz = ray_at(__ldg(rays_o + 3 * r + 2), __ldg(rays_d + 3 * r + 2), t);
-    if (sdf) sdf[i] = query_sdf(f, g, px, py, pz);
     Eq7 e;
     eq7_setup(g, px, py, pz, e);
+    float c[8];  // the cell's corner values, shared by the SDF and the gradient
+    eq7_load_block(f, g, e, c);
+    if (sdf) sdf[i] = query_sdf_block(f, g, px, py, pz, e, c);
     float w[8], gr[3], nn[3], len;
     eq7_weights(e, w);
-    eq7_gradient(f, g, e, w, gr);
+    eq7_gradient_block(f, g, e, w, c, gr);
     normalize_eps(gr, nn, len);
     normal[3 * i] = nn[0];
     normal[3 * i + 1] = nn[1];
@@ -48,7 +50,7 @@ __global__ void __launch_bounds__(256) k_geometry_fwd(const float* __restrict__ 
 }
 
 // d_normal2 (row stride ld2) is a second dL/dnormal source (the appearance branch input).
-__global__ void __launch_bounds__(256) k_geometry_bwd(const float* __restrict__ f, Grid g,
+__global__ void __launch_bounds__(256, 3) k_geometry_bwd(const float* __restrict__ f, Grid g,
                                                       const float* __restrict__ rays_o,
                                                       const float* __restrict__ rays_d,
                                                       const float* __restrict__ mid, int64_t n, int S,
@@ -62,14 +64,7 @@ __global__ void __launch_bounds__(256) k_geometry_bwd(const float* __restrict__ 
     const float px = ray_at(__ldg(rays_o + 3 * r), __ldg(rays_d + 3 * r), t);
     const float py = ray_at(__ldg(rays_o + 3 * r + 1), __ldg(rays_d + 3 * r + 1), t);
     const float pz = ray_at(__ldg(rays_o + 3 * r + 2), __ldg(rays_d + 3 * r + 2), t);
-    if (d_sdf) {
-      const float ds = d_sdf[i];
-      if (ds != 0.0f) {
-        Tri tr;
-        gs_setup(g, px, py, pz, tr);
-        gs_scatter(gg, g, tr, ds);
-      }
-    }
+    const float ds = d_sdf ? d_sdf[i] : 0.0f;
     float dn[3] = {0.0f, 0.0f, 0.0f};
     if (d_normal) {
       dn[0] = d_normal[3 * i];
@@ -89,11 +84,31 @@ __global__ void __launch_bounds__(256) k_geometry_bwd(const float* __restrict__ 
     }
     const bool any_n = dn[0] != 0.0f || dn[1] != 0.0f || dn[2] != 0.0f;
     const bool any_g = dg[0] != 0.0f || dg[1] != 0.0f || dg[2] != 0.0f;
-    if (!any_n && !any_g) continue;
+    if (!any_n && !any_g) {
+      if (ds != 0.0f) {
+        Tri tr;
+        gs_setup(g, px, py, pz, tr);
+        gs_scatter(gg, g, tr, ds);
+      }
+      continue;
+    }
     Eq7 e;
     eq7_setup(g, px, py, pz, e);
     float w[8];
     eq7_weights(e, w);
+    // dL/dsdf on the grid_sample corners: summed with the Eq.7 terms of the same corners when the
+    // cell is the same one (interior points), else scattered on its own
+    float acc[8] = {0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    if (ds != 0.0f) {
+      Tri tr;
+      gs_setup(g, px, py, pz, tr);
+      if (tr.inb == 0xffu && tr.x0 == e.x0 && tr.y0 == e.y0 && tr.z0 == e.z0) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) acc[k] = tr.w[k] * ds;
+      } else {
+        gs_scatter(gg, g, tr, ds);
+      }
+    }
     if (any_n) {
       float gr[3], nn[3], len, dgn[3];
       eq7_gradient(f, g, e, w, gr);
@@ -103,7 +118,7 @@ __global__ void __launch_bounds__(256) k_geometry_bwd(const float* __restrict__ 
       dg[1] += dgn[1];
       dg[2] += dgn[2];
     }
-    eq7_scatter(gg, g, e, w, dg);
+    eq7_scatter_acc(gg, g, e, w, dg, acc);
   }
 }
 
