@@ -107,7 +107,9 @@ struct Tri {
 __device__ __forceinline__ float gs_coord(float p, float lo, float den, float inv, int R) {
   float n = div_den(__fsub_rn(p, lo), den, inv);
   float g = __fsub_rn(__fmul_rn(n, 2.0f), 1.0f);
-  float c = __fmul_rn(__fdiv_rn(__fadd_rn(g, 1.0f), 2.0f), (float)(R - 1));
+  // (g + 1) / 2 as a multiply by 0.5: dividing by a power of two is exact scaling, so the two give
+  // the same bits (a rounded division costs a multi-instruction sequence per axis)
+  float c = __fmul_rn(__fmul_rn(__fadd_rn(g, 1.0f), 0.5f), (float)(R - 1));
   c = fminf((float)(R - 1), fmaxf(c, 0.0f));
   return c;
 }
