@@ -420,9 +420,10 @@ def run_fused(args):
     roofline = tensor_roofline(dominant) if dominant in MLP_FLOPS else hbm_roofline(dominant)
     roofline_hbm = hbm_roofline(hbm_dom)
 
-    # end to end through the public API: pinned host rays/targets in, every step's loss copied back
-    # to pinned host memory and read by the host one step later (as a training loop logs it), so
-    # the readback does not drain the launch queue
+    # end to end through the public API: pinned host rays/targets handed to FusedTrainer.step
+    # (which copies them to the device, in graph mode straight into the graph's input buffers),
+    # every step's loss copied back to pinned host memory and read by the host one step later (as
+    # a training loop logs it), so the readback does not drain the launch queue
     host = [(o.cpu().pin_memory(), d.cpu().pin_memory(), t.cpu().pin_memory()) for o, d, t in batches]
     slots = torch.empty(2, dtype=torch.float32).pin_memory()
     evts = [torch.cuda.Event(), torch.cuda.Event()]
@@ -432,10 +433,7 @@ def run_fused(args):
     t0 = time.perf_counter()
     for i in range(args.steps):
         ho, hd, ht = host[i % nb]
-        o = ho.to(dev, non_blocking=True)
-        d = hd.to(dev, non_blocking=True)
-        t = ht.to(dev, non_blocking=True)
-        out = tr.step(o, d, t, step=n_warm + args.steps + i)
+        out = tr.step(ho, hd, ht, step=n_warm + args.steps + i)
         slots[i % 2:i % 2 + 1].copy_(out["loss_rgb"].reshape(1), non_blocking=True)
         evts[i % 2].record()
         if i >= 1:

@@ -25,16 +25,19 @@ def _model():
     return m
 
 
-def _rays(n, seed):
+def _rays(n, seed, host=False):
     g = torch.Generator().manual_seed(seed)
     o = torch.randn(n, 3, generator=g)
     o = 3.0 * o / o.norm(dim=-1, keepdim=True)
     d = -o / 3.0 + 0.05 * torch.randn(n, 3, generator=g)
     d = d / d.norm(dim=-1, keepdim=True)
-    return o.to(DEV), d.to(DEV), torch.rand(n, 3, generator=g).to(DEV)
+    t = torch.rand(n, 3, generator=g)
+    if host:
+        return o.pin_memory(), d.pin_memory(), t.pin_memory()
+    return o.to(DEV), d.to(DEV), t.to(DEV)
 
 
-def _run(cuda_graph, steps, warmup_s):
+def _run(cuda_graph, steps, warmup_s, host=False):
     from voxneus_b200.rendering import RaySampler
     from voxneus_b200.training import FusedTrainer
 
@@ -44,7 +47,7 @@ def _run(cuda_graph, steps, warmup_s):
     torch.manual_seed(11)  # the sampler's and occupancy refresh's draws (default CUDA generator)
     hist = []
     for i in range(steps):
-        o, d, t = _rays(256, 100 + i)
+        o, d, t = _rays(256, 100 + i, host)
         out = tr.step(o, d, t, step=i)
         hist.append({k: v.clone() for k, v in out.items()})
     torch.cuda.synchronize()
@@ -76,6 +79,25 @@ def test_graph_step_is_bitwise_the_eager_step():
                 assert torch.equal(sa["exp_avg"], sb["exp_avg"]) and torch.equal(sa["exp_avg_sq"], sb["exp_avg_sq"])
     assert torch.equal(me.occupancy_grid.density_grid, mg.occupancy_grid.density_grid)
     assert torch.equal(me.occupancy_grid.occupancy_mask, mg.occupancy_grid.occupancy_mask)
+
+
+def test_graph_step_takes_pinned_host_inputs():
+    """Pinned host rays and targets (copied by the step, in graph mode straight into the graph's
+    input buffers) give the bits of device inputs."""
+    from voxneus_b200 import ops
+
+    ops.set_deterministic(True)
+    try:
+        me, _, he = _run(False, 5, 100)
+        mh, th, hh = _run(True, 5, 100, host=True)
+    finally:
+        ops.set_deterministic(False)
+    assert th.graph() is not None
+    for a, b in zip(he, hh):
+        for k in a:
+            assert torch.equal(a[k], b[k]), k
+    for pa, pb in zip(me.parameters(), mh.parameters()):
+        assert torch.equal(pa, pb)
 
 
 def test_graph_mode_falls_back_to_eager_with_explicit_randoms():

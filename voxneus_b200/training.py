@@ -168,17 +168,22 @@ class FusedTrainer:
         return (math.cos(math.pi * step / max(self.total_steps, 1)) + 1.0) * 0.5 * (1.0 - 0.05) + 0.05
 
     def step(self, rays_o, rays_d, target, step: int = 0, randoms=None) -> Dict[str, torch.Tensor]:
-        """One training step. In graph mode the returned tensors are the graph's outputs, overwritten
-        by the next step (copy them to keep them)."""
+        """One training step. rays_o, rays_d, target may be device tensors or (pinned) host tensors,
+        which are copied to the device on the current stream: in graph mode straight into the
+        graph's input buffers. In graph mode the returned tensors are the graph's outputs,
+        overwritten by the next step (copy them to keep them)."""
         m = self.model
         if [int(r) for r in m.sdf_grid.res] != self.res:
             raise RuntimeError("grid resolution changed; build a new FusedTrainer after scale_volume_grid")
         graphable = (self.cuda_graph and self.exchange is None and self.optimize and randoms is None
-                     and rays_o.is_cuda and torch.is_grad_enabled())
+                     and torch.is_grad_enabled())
         if graphable and self._eager_steps >= GRAPH_WARMUP_STEPS:
             return self._graph_step(rays_o, rays_d, target, step)
         self._graphs.clear()  # an eager step owns fresh gradients; replays would no longer see them
         self._eager_steps += 1
+        dev = self.bitmap.device
+        rays_o, rays_d, target = (t if t.device == dev else t.to(dev, non_blocking=True)
+                                  for t in (rays_o, rays_d, target))
         return self._eager_step(rays_o, rays_d, target, step, randoms)
 
     def _refresh_occupancy(self, step: int) -> None:
@@ -238,9 +243,11 @@ class FusedTrainer:
     def _graph_step(self, rays_o, rays_d, target, step: int) -> Dict[str, torch.Tensor]:
         amplify = step >= self.s_warmup_steps
         g = self._graphs.get(amplify)
+        if g is not None and (g.o.shape != rays_o.shape or g.d.shape != rays_d.shape or g.t.shape != target.shape):
+            g = None  # a new batch shape: capture again
         if g is None:
             self._graphs.clear()  # one captured variant at a time (amplification switches on once)
-            g = _StepGraph(self, rays_o, rays_d, target, amplify)
+            g = _StepGraph(self, rays_o, rays_d, target, amplify, self.bitmap.device)
             self._graphs[amplify] = g
         self._refresh_occupancy(step)
         g.run(rays_o, rays_d, target, step)
@@ -266,14 +273,13 @@ class _StepGraph:
     eager step's). Gradients live in the graph's memory pool and are rewritten by every replay.
     """
 
-    def __init__(self, tr: FusedTrainer, rays_o, rays_d, target, amplify: bool):
+    def __init__(self, tr: FusedTrainer, rays_o, rays_d, target, amplify: bool, dev: torch.device):
         m = tr.model
-        dev = rays_o.device
         self.tr = tr
         self.amplify = amplify
-        self.o = torch.empty_like(rays_o, memory_format=torch.contiguous_format)
-        self.d = torch.empty_like(rays_d, memory_format=torch.contiguous_format)
-        self.t = torch.empty_like(target, memory_format=torch.contiguous_format)
+        self.o = torch.empty(rays_o.shape, dtype=rays_o.dtype, device=dev)
+        self.d = torch.empty(rays_d.shape, dtype=rays_d.dtype, device=dev)
+        self.t = torch.empty(target.shape, dtype=target.dtype, device=dev)
         self.grid_opt = tr.optimizers["sdf_optimizer"]
         self.net_opt = tr.optimizers["net_optimizer"]
         if not isinstance(self.grid_opt, SparseGridAdam) or not isinstance(self.net_opt, FusedAdam):
