@@ -354,12 +354,14 @@ class VoxNeuS(nn.Module):
             _, dists, mid = ops.sample_multistep(self.sdf_grid.grid.detach(), lo, hi, o, d, near, far, ns, ni,
                                                  up_sample_steps, perturb, t_rand, u, occ.occupancy_mask,
                                                  *occ.bounds(), want_z=False)
-        sdf, normal, gsamp = ops.RenderGeometryFn.apply(self.sdf_grid.grid, o, d, mid, lo, hi, vr_bitmap, extras)
+        handoff = ops.NormalGradHandoff() if fused_mlp else None
+        sdf, normal, gsamp = ops.RenderGeometryFn.apply(self.sdf_grid.grid, o, d, mid, lo, hi, vr_bitmap, extras,
+                                                        handoff)
         if fused_mlp:
             l0, l1 = self.radiance_mlp.net[0], self.radiance_mlp.net[2]
             colors = ops.AppearanceMLPFn.apply(self.radiance_hash.encoder.embeddings, normal, l0.weight, l0.bias,
                                                l1.weight, l1.bias, o, d, mid, lo, hi, self.radiance_hash.encoder.cfg,
-                                               active_levels, torch.is_grad_enabled())
+                                               active_levels, torch.is_grad_enabled(), handoff)
         else:
             x = ops.AppearanceInputFn.apply(self.radiance_hash.encoder.embeddings, normal, o, d, mid, lo, hi,
                                             self.radiance_hash.encoder.cfg, active_levels)

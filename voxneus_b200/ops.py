@@ -341,11 +341,21 @@ def sample_pdf(bins, weights, n_samples, det=False, u=None, cdf=None, return_ind
 # ------------------------------------------------------------------ render geometry -------
 
 
+class NormalGradHandoff:
+    """dL/dnormal of the appearance branch, handed from AppearanceMLPFn's adjoint to
+    RenderGeometryFn's, which adds it to the compositing branch's inside the geometry adjoint kernel
+    (the same single addition autograd would make, without its (P, 3) sum kernel). The geometry
+    adjoint runs after both consumers of the normals, so the hand-off is complete by then."""
+
+    def __init__(self):
+        self.d_normal = None
+
+
 class RenderGeometryFn(torch.autograd.Function):
     """Pass-2 geometry (positions, SDF, Eq.7 normal) of (rays, midpoints); marks V_R corners."""
 
     @staticmethod
-    def forward(ctx, grid, rays_o, rays_d, mid, xyz_min, xyz_max, bitmap, want_grad):
+    def forward(ctx, grid, rays_o, rays_d, mid, xyz_min, xyz_max, bitmap, want_grad, handoff=None):
         g = grid.detach()
         res = _grid3(g)
         nr, ns = mid.shape
@@ -357,6 +367,7 @@ class RenderGeometryFn(torch.autograd.Function):
              ptr(mid), nr, ns, ptr(sdf), ptr(nrm), ptr(gr), ptr(bitmap), stream_ptr(dev))
         ctx.save_for_backward(grid, rays_o, rays_d, mid)
         ctx.bounds = (xyz_min, xyz_max)
+        ctx.handoff = handoff
         if gr is not None:
             ctx.mark_non_differentiable(gr)
         return sdf, nrm, gr
@@ -364,16 +375,19 @@ class RenderGeometryFn(torch.autograd.Function):
     @staticmethod
     def backward(ctx, d_sdf, d_nrm, _d_gr):
         grid, rays_o, rays_d, mid = ctx.saved_tensors
+        d_nrm2 = None
+        if ctx.handoff is not None:
+            d_nrm2, ctx.handoff.d_normal = ctx.handoff.d_normal, None
         if not ctx.needs_input_grad[0]:
-            return (None,) * 8
+            return (None,) * 9
         g = grid.detach()
         res = _grid3(g)
         nr, ns = mid.shape
         gg = torch.zeros(res, device=mid.device)
         d_sdf = None if d_sdf is None else d_sdf.contiguous()
         d_nrm = None if d_nrm is None else d_nrm.contiguous()
-        geometry_backward(g, res, ctx.bounds, rays_o, rays_d, mid, d_sdf, d_nrm, gg)
-        return gg.reshape(grid.shape), None, None, None, None, None, None, None
+        geometry_backward(g, res, ctx.bounds, rays_o, rays_d, mid, d_sdf, d_nrm, gg, d_nrm2)
+        return gg.reshape(grid.shape), None, None, None, None, None, None, None, None
 
 
 # ------------------------------------------------------------------ deterministic mode ------
@@ -400,20 +414,25 @@ def _workspace(dev, nbytes: int) -> torch.Tensor:
     return ws
 
 
-def geometry_backward(g, res, bounds, rays_o, rays_d, mid, d_sdf, d_normal, out):
+def geometry_backward(g, res, bounds, rays_o, rays_d, mid, d_sdf, d_normal, out, d_normal2=None):
+    """d_normal2: a second dL/dnormal source, (P, 3) contiguous, added to d_normal in the kernel."""
     nr, ns = mid.shape
     dev = mid.device
+    if d_normal2 is not None:
+        check_tensor(d_normal2, "d_normal2", device=dev)
+        if d_normal2.numel() != nr * ns * 3:
+            raise RuntimeError(f"d_normal2 has {d_normal2.numel()} elements, need {nr * ns * 3}")
     if _deterministic:
         need = int(L.query("vx_geometry_backward_det_workspace", nr, ns, i3(res)))
         if need == 0:
             raise RuntimeError("batch too large for one deterministic geometry pass")
         ws = _workspace(dev, need)
         call("vx_render_geometry_backward_det", ptr(g), i3(res), f3(bounds[0]), f3(bounds[1]), ptr(rays_o),
-             ptr(rays_d), ptr(mid), nr, ns, ptr(d_sdf), ptr(d_normal), None, 3, ptr(out), ptr(ws), ws.numel(),
-             stream_ptr(dev))
+             ptr(rays_d), ptr(mid), nr, ns, ptr(d_sdf), ptr(d_normal), ptr(d_normal2), 3, ptr(out), ptr(ws),
+             ws.numel(), stream_ptr(dev))
     else:
         call("vx_render_geometry_backward", ptr(g), i3(res), f3(bounds[0]), f3(bounds[1]), ptr(rays_o), ptr(rays_d),
-             ptr(mid), nr, ns, ptr(d_sdf), ptr(d_normal), None, 3, None, ptr(out), stream_ptr(dev))
+             ptr(mid), nr, ns, ptr(d_sdf), ptr(d_normal), ptr(d_normal2), 3, None, ptr(out), stream_ptr(dev))
 
 
 def hash_backward(d_emb, cfg, active_levels, pts, rays_o, rays_d, mid, n_samples, xyz_min, xyz_max, n_points,
@@ -582,7 +601,7 @@ class AppearanceMLPFn(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, embeddings, normals, W0, b0, W1, b1, rays_o, rays_d, mid, xyz_min, xyz_max, cfg, active_levels,
-                keep_rows=True):
+                keep_rows=True, handoff=None):
         nr, ns = mid.shape
         p = nr * ns
         width = 2 * cfg.n_levels + 16 + 3
@@ -608,6 +627,7 @@ class AppearanceMLPFn(torch.autograd.Function):
             rows = rows[:, :width]
         ctx.save_for_backward(rays_o, rays_d, mid, W0, b0, W1, b1)
         ctx.rows = rows
+        ctx.handoff = handoff
         ctx.meta = (xyz_min, xyz_max, cfg, active_levels, embeddings.shape, normals.shape)
         return colors.reshape(nr, ns, 3)
 
@@ -626,7 +646,10 @@ class AppearanceMLPFn(torch.autograd.Function):
             d_emb = torch.zeros(eshape, device=g.device)
             hash_backward(d_emb, cfg, active_levels, None, rays_o, rays_d, mid, ns, xyz_min, xyz_max, nr * ns, d_hash,
                           32)
-        return (d_emb, d_normal.reshape(nshape), dW0, db0, dW1, db1, None, None, None, None, None, None, None, None)
+        d_nrm = d_normal.reshape(nshape)
+        if ctx.handoff is not None and ctx.needs_input_grad[1]:
+            ctx.handoff.d_normal, d_nrm = d_normal, None  # summed inside the geometry adjoint
+        return (d_emb, d_nrm, dW0, db0, dW1, db1, None, None, None, None, None, None, None, None, None)
 
 
 class HashEncodeFn(torch.autograd.Function):
