@@ -294,14 +294,23 @@ struct CompGrads {
 // composited normal sum; pass 2 forms dL/dw and dT_j T_j; a reverse warp scan turns those
 // into the suffix sums G_i = sum_{j>i} dT_j T_j (cumprod's adjoint, divided by q_i below);
 // pass 3 back-propagates through the clamps, Eq.2 and the normal inner product.
-__global__ void __launch_bounds__(128) k_composite_bwd(CompArgs a, CompGrads gr) {
+// kKeep: pass 1 keeps each sample's alpha terms and pass 2 its dL/dw in shared memory (13 floats
+// per sample and warp), so pass 3 reads them instead of recomputing the alpha (two sigmoids, the
+// divisions, the sphere mask) and reloading colours, depths and normals; the same values, so the
+// same results. Without it (very long rays) pass 3 recomputes them.
+constexpr int kCompKeepFields = 13;  // T, alpha, G | dw, mask, ratio, den, diff, p0, p1, f0, f1, cos_t
+
+template <bool kKeep>
+__global__ void __launch_bounds__(128, 8) k_composite_bwd(CompArgs a, CompGrads gr) {
   extern __shared__ float sm[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
   const int64_t wpb = blockDim.x >> 5;
-  float* T_s = sm + warp * 3 * a.S;  // transmittance
+  float* T_s = sm + warp * (kKeep ? kCompKeepFields : 3) * a.S;  // transmittance
   float* A_s = T_s + a.S;            // masked alpha
   float* G_s = A_s + a.S;            // dT_j T_j, then the suffix sums
+  float* D_s = G_s + a.S;            // kKeep: dL/dw, then the alpha terms below
+  float* K_s = D_s + a.S;            // kKeep: [mask, ratio, den, diff, p0, p1, f0, f1, cos_t][S]
   __shared__ double ds_warp[32];
   __shared__ bool is_last;
   const float s = get_s(a);
@@ -322,6 +331,17 @@ __global__ void __launch_bounds__(128) k_composite_bwd(CompArgs a, CompGrads gr)
         alpha_fwd(a, s, r, i, a.sdf[k], nrm, o);
         am = o.am;
         q = fminf(fmaxf(__fadd_rn(__fsub_rn(1.0f, am), 1e-7f), 0.0f), 1.0f);
+        if (kKeep) {
+          K_s[i] = o.mask;
+          K_s[a.S + i] = o.ratio;
+          K_s[2 * a.S + i] = o.den;
+          K_s[3 * a.S + i] = o.diff;
+          K_s[4 * a.S + i] = o.p0;
+          K_s[5 * a.S + i] = o.p1;
+          K_s[6 * a.S + i] = o.f0;
+          K_s[7 * a.S + i] = o.f1;
+          K_s[8 * a.S + i] = o.cos_t;
+        }
       }
       const double inc = warp_incl_prod_d((double)q, lane);
       double Td = __shfl_up_sync(0xffffffffu, inc, 1);
@@ -371,6 +391,7 @@ __global__ void __launch_bounds__(128) k_composite_bwd(CompArgs a, CompGrads gr)
         dw += gN[0] * a.normals[3 * k] + gN[1] * a.normals[3 * k + 1] + gN[2] * a.normals[3 * k + 2];
         if (gr.g_weights) dw += gr.g_weights[k];
         if (T < 1e-4f) dw = 0.0f;
+        if (kKeep) D_s[i] = dw;
         float dT = dw * A_s[i];
         if (gr.g_trans) dT += gr.g_trans[k];
         G_s[i] = dT * T;
@@ -397,16 +418,31 @@ __global__ void __launch_bounds__(128) k_composite_bwd(CompArgs a, CompGrads gr)
       const int i = base + lane;
       if (i >= a.S) continue;
       const int64_t k = r * a.S + i;
-      const float nrm[3] = {a.normals[3 * k], a.normals[3 * k + 1], a.normals[3 * k + 2]};
       SampleFwd o;
-      alpha_fwd(a, s, r, i, a.sdf[k], nrm, o);
+      float dw;
+      if (kKeep) {
+        o.am = A_s[i];
+        o.mask = K_s[i];
+        o.ratio = K_s[a.S + i];
+        o.den = K_s[2 * a.S + i];
+        o.diff = K_s[3 * a.S + i];
+        o.p0 = K_s[4 * a.S + i];
+        o.p1 = K_s[5 * a.S + i];
+        o.f0 = K_s[6 * a.S + i];
+        o.f1 = K_s[7 * a.S + i];
+        o.cos_t = K_s[8 * a.S + i];
+        dw = D_s[i];
+      } else {
+        const float nrm[3] = {a.normals[3 * k], a.normals[3 * k + 1], a.normals[3 * k + 2]};
+        alpha_fwd(a, s, r, i, a.sdf[k], nrm, o);
+        dw = g_op + g_dep * a.zv[k];
+        dw += g_rgb[0] * a.colors[3 * k] + g_rgb[1] * a.colors[3 * k + 1] + g_rgb[2] * a.colors[3 * k + 2];
+        dw += gN[0] * nrm[0] + gN[1] * nrm[1] + gN[2] * nrm[2];
+        if (gr.g_weights) dw += gr.g_weights[k];
+        if (T_s[i] < 1e-4f) dw = 0.0f;
+      }
       const float T = T_s[i];
       const float w = (T < 1e-4f) ? 0.0f : o.am * T;
-      float dw = g_op + g_dep * a.zv[k];
-      dw += g_rgb[0] * a.colors[3 * k] + g_rgb[1] * a.colors[3 * k + 1] + g_rgb[2] * a.colors[3 * k + 2];
-      dw += gN[0] * nrm[0] + gN[1] * nrm[1] + gN[2] * nrm[2];
-      if (gr.g_weights) dw += gr.g_weights[k];
-      if (T < 1e-4f) dw = 0.0f;
       float dam = dw * T;
       if (gr.g_alpha) dam += gr.g_alpha[k];
       const float qraw = __fadd_rn(__fsub_rn(1.0f, o.am), 1e-7f);
@@ -688,12 +724,18 @@ int vx_composite_backward(const float* colors, const float* sdf, const float* no
   VX_REQUIRE(colors && z_vals && partials && counter && d_s, "null pointer");
   const int blocks = (int)grid_for(n_rays * 32, 128, 8);
   VX_REQUIRE(n_partials >= blocks, "partials buffer holds %d entries, need %d", n_partials, blocks);
+  const size_t smem_keep = (size_t)4 * kCompKeepFields * n_samples * sizeof(float);
   const size_t smem = (size_t)4 * 3 * n_samples * sizeof(float);
   VX_REQUIRE(smem <= 200 * 1024, "too many samples per ray");
-  if (smem > 48 * 1024) cudaFuncSetAttribute(k_composite_bwd, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   CompGrads gr{g_rgb, g_depth, g_normal, g_opacity, g_weights, g_alpha, g_transmittance, d_colors, d_sdf, d_normals,
                partials, counter, d_s, amplify_k, amplified};
-  k_composite_bwd<<<blocks, 128, smem, (cudaStream_t)stream>>>(a, gr);
+  if (smem_keep <= 32 * 1024) {  // up to 157 samples per ray: 8 blocks per SM still fit
+    k_composite_bwd<true><<<blocks, 128, smem_keep, (cudaStream_t)stream>>>(a, gr);
+  } else {
+    if (smem > 48 * 1024)
+      cudaFuncSetAttribute(k_composite_bwd<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_composite_bwd<false><<<blocks, 128, smem, (cudaStream_t)stream>>>(a, gr);
+  }
   count_launches(1);
   return check_launch("composite_backward");
 }
