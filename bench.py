@@ -424,7 +424,12 @@ def run_fused(args):
     # (which copies them to the device, in graph mode straight into the graph's input buffers),
     # every step's loss copied back to pinned host memory and read by the host one step later (as
     # a training loop logs it), so the readback does not drain the launch queue
-    host = [(o.cpu().pin_memory(), d.cpu().pin_memory(), t.cpu().pin_memory()) for o, d, t in batches]
+    # each batch as one pinned (3, N, 3) tensor whose slices are the rays and targets: the step
+    # copies it to the device in one transfer
+    host = []
+    for o, d, t in batches:
+        hb = torch.stack([o, d, t]).cpu().pin_memory()
+        host.append((hb[0], hb[1], hb[2]))
     slots = torch.empty(2, dtype=torch.float32).pin_memory()
     evts = [torch.cuda.Event(), torch.cuda.Event()]
     host_losses = []

@@ -32,6 +32,9 @@ def _rays(n, seed, host=False):
     d = -o / 3.0 + 0.05 * torch.randn(n, 3, generator=g)
     d = d / d.norm(dim=-1, keepdim=True)
     t = torch.rand(n, 3, generator=g)
+    if host == "packed":  # the three slices of one pinned (3, N, 3) tensor: one copy
+        hb = torch.stack([o, d, t]).pin_memory()
+        return hb[0], hb[1], hb[2]
     if host:
         return o.pin_memory(), d.pin_memory(), t.pin_memory()
     return o.to(DEV), d.to(DEV), t.to(DEV)
@@ -47,7 +50,7 @@ def _run(cuda_graph, steps, warmup_s, host=False):
     torch.manual_seed(11)  # the sampler's and occupancy refresh's draws (default CUDA generator)
     hist = []
     for i in range(steps):
-        o, d, t = _rays(256, 100 + i, host)
+        o, d, t = _rays(256, 100 + i, ("packed" if i % 2 else True) if host else False)
         out = tr.step(o, d, t, step=i)
         hist.append({k: v.clone() for k, v in out.items()})
     torch.cuda.synchronize()
@@ -83,7 +86,8 @@ def test_graph_step_is_bitwise_the_eager_step():
 
 def test_graph_step_takes_pinned_host_inputs():
     """Pinned host rays and targets (copied by the step, in graph mode straight into the graph's
-    input buffers) give the bits of device inputs."""
+    input buffers; separate tensors and slices of one packed tensor alternate) give the bits of
+    device inputs."""
     from voxneus_b200 import ops
 
     ops.set_deterministic(True)

@@ -243,7 +243,8 @@ class FusedTrainer:
     def _graph_step(self, rays_o, rays_d, target, step: int) -> Dict[str, torch.Tensor]:
         amplify = step >= self.s_warmup_steps
         g = self._graphs.get(amplify)
-        if g is not None and (g.o.shape != rays_o.shape or g.d.shape != rays_d.shape or g.t.shape != target.shape):
+        if g is not None and (g.o.shape != rays_o.shape or g.d.shape != rays_d.shape or g.t.shape != target.shape
+                              or g.io.dtype != rays_o.dtype):
             g = None  # a new batch shape: capture again
         if g is None:
             self._graphs.clear()  # one captured variant at a time (amplification switches on once)
@@ -277,9 +278,10 @@ class _StepGraph:
         m = tr.model
         self.tr = tr
         self.amplify = amplify
-        self.o = torch.empty(rays_o.shape, dtype=rays_o.dtype, device=dev)
-        self.d = torch.empty(rays_d.shape, dtype=rays_d.dtype, device=dev)
-        self.t = torch.empty(target.shape, dtype=target.dtype, device=dev)
+        # the inputs as one (3, N, 3) buffer: a caller whose rays and targets are the three slices of
+        # one host tensor is served with a single copy
+        self.io = torch.empty((3,) + tuple(rays_o.shape), dtype=rays_o.dtype, device=dev)
+        self.o, self.d, self.t = self.io[0], self.io[1], self.io[2]
         self.grid_opt = tr.optimizers["sdf_optimizer"]
         self.net_opt = tr.optimizers["net_optimizer"]
         if not isinstance(self.grid_opt, SparseGridAdam) or not isinstance(self.net_opt, FusedAdam):
@@ -355,9 +357,15 @@ class _StepGraph:
         return torch.tensor(row, dtype=torch.float32)
 
     def run(self, rays_o, rays_d, target, step: int) -> None:
-        self.o.copy_(rays_o, non_blocking=True)
-        self.d.copy_(rays_d, non_blocking=True)
-        self.t.copy_(target, non_blocking=True)
+        b = rays_o._base
+        if (b is not None and rays_d._base is b and target._base is b and b.shape == self.io.shape
+                and b.dtype == self.io.dtype and b.is_contiguous() and rays_o.data_ptr() == b[0].data_ptr()
+                and rays_d.data_ptr() == b[1].data_ptr() and target.data_ptr() == b[2].data_ptr()):
+            self.io.copy_(b, non_blocking=True)
+        else:
+            self.o.copy_(rays_o, non_blocking=True)
+            self.d.copy_(rays_d, non_blocking=True)
+            self.t.copy_(target, non_blocking=True)
         s = self.slot
         self.slot = (s + 1) % _SCALAR_SLOTS
         if self.slot_events[s] is not None:
