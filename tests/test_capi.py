@@ -78,3 +78,26 @@ def test_kernel_calls_fail_loudly_without_cuda(monkeypatch):
 
     with pytest.raises(RuntimeError):
         ops.near_far_from_sphere(torch.zeros(2, 3), torch.ones(2, 3))
+
+
+def test_adam_step_scalar_helpers_match_the_update_formulas():
+    """The host helpers behind the graph-replayed optimizer steps: torch.optim.Adam's scalars
+    (lr / (1 - b1^t), 1 / sqrt(1 - b2^t), double rounded to float) and the reference formula's
+    step size lr * sqrt(1 - b2^t) / (1 - b1^t) (adam_upd_kernel.cu:50, evaluated in float)."""
+    import math
+
+    import numpy as np
+
+    from voxneus_b200 import ops
+
+    for step in (1, 2, 7, 100, 5000, 40000):
+        for b1, b2, lr in ((0.9, 0.999, 1e-2), (0.9, 0.99, 0.1), (0.9, 0.999, 5e-4 * 5.0)):
+            ss, inv = ops.adam_torch_step_scalars(step, b1, b2, lr)
+            f = np.float32
+            lr32, b132, b232 = float(f(lr)), float(f(b1)), float(f(b2))
+            assert ss == float(f(lr32 / (1.0 - b132 ** step)))
+            assert inv == float(f(1.0 / math.sqrt(1.0 - b232 ** step)))
+            ref = ops.adam_reference_step_size(step, b1, b2, lr)
+            want = lr32 * math.sqrt(1.0 - b232 ** step) / (1.0 - b132 ** step)
+            # float evaluation: 1 - b^t cancels (b^t near 1 carries ~6e-8 absolute error)
+            assert abs(ref - want) <= 1e-4 * abs(want)
