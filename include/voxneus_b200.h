@@ -286,11 +286,12 @@ int vx_tensor_core_timeouts(void);
 /* Adjoint of vx_radiance_mlp_forward (recomputes the hidden layer): d_colors (n,3) -> d_hash (n,32)
  * (gradient of input columns 0..31), d_normal (n,3) (columns 48..50), and the weight gradients
  * dW0, db0, dW1, db1 (written, not accumulated; summed over blocks in a fixed order).
- * partials: >= vx_mlp_blocks(n) * vx_mlp_partial_floats() floats. */
+ * colors: the forward's outputs (n,3) for the sigmoid's derivative, or NULL to recompute them
+ * (the same bits either way). partials: >= vx_mlp_blocks(n) * vx_mlp_partial_floats() floats. */
 int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int in_dim, int hidden, int out_dim,
                              const float* W0, const float* b0, const float* W1, const float* b1, const float* d_colors,
-                             float* d_hash, float* d_normal, float* dW0, float* db0, float* dW1, float* db1,
-                             float* partials, int64_t n_partial_floats, void* stream);
+                             const float* colors, float* d_hash, float* d_normal, float* dW0, float* db0, float* dW1,
+                             float* db1, float* partials, int64_t n_partial_floats, void* stream);
 
 /* ---------------------------------------------------------- render (per ray) --------------- */
 

@@ -489,6 +489,27 @@ def test_fused_mlp_matches_oracle(p, ld):
     assert _lib.query("vx_tensor_core_timeouts") == 0
 
 
+def test_mlp_adjoint_with_forward_colours_is_bitwise_the_recompute():
+    """The adjoint reading the forward's colours (for the sigmoid's derivative) instead of
+    recomputing the output layer gives the same bits: same MMAs, same partial sums."""
+    from voxneus_b200 import ops
+
+    torch.manual_seed(5)
+    p = 3001  # a partial last tile
+    rows = torch.randn(p, 52, device=DEV)[:, :51]  # 51 features in 52-float rows, as the render keeps them
+    W0 = 0.2 * torch.randn(64, 51, device=DEV)
+    b0 = 0.1 * torch.randn(64, device=DEV)
+    W1 = 0.2 * torch.randn(3, 64, device=DEV)
+    b1 = 0.1 * torch.randn(3, device=DEV)
+    colors = ops.mlp_forward(rows, W0, b0, W1, b1)
+    g = torch.randn(p, 3, device=DEV)
+    a = ops.mlp_backward(rows, W0, b0, W1, b1, g)
+    b = ops.mlp_backward(rows, W0, b0, W1, b1, g, colors)
+    torch.cuda.synchronize()
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
+
+
 def test_huber_loss_and_gradient():
     """Fused Huber colour loss (value 1e-5, gradient 1e-4) vs the oracle's torch ops; both branches,
     exact ties and a size that is not a multiple of the block."""

@@ -535,6 +535,7 @@ __device__ __forceinline__ uint32_t wt_off(int f, int n) {
 template <bool kBulk>
 __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__ X, int64_t ldx, int xvec, int64_t P,
                                                       MlpW w, const float* __restrict__ d_out,
+                                                      const float* __restrict__ y_in,
                                                       float* __restrict__ d_hash, float* __restrict__ d_normal,
                                                       float* __restrict__ partials) {
   extern __shared__ __align__(1024) uint8_t smem[];
@@ -610,12 +611,15 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   bool first_w = true, failed = false;
   uint32_t phase = 0;
   float4 pre[7];  // !kBulk: this tile's row chunks, loaded during the previous tile
-  float dy[NO];
+  float dy[NO], yv[NO] = {0.0f, 0.0f, 0.0f};  // dL/dcolour and (y_in) the forward's colour of this sample
   if ((int64_t)blockIdx.x < ntiles) {
     const int64_t m0 = (int64_t)blockIdx.x * TM;
     if (!kBulk) load_row_chunks(X, ldx, xvec != 0, P, m0, m, hh, pre);
 #pragma unroll
-    for (int c = 0; c < NO; ++c) dy[c] = m0 + m < P ? d_out[(m0 + m) * NO + c] : 0.0f;
+    for (int c = 0; c < NO; ++c) {
+      dy[c] = m0 + m < P ? d_out[(m0 + m) * NO + c] : 0.0f;
+      if (y_in) yv[c] = m0 + m < P ? y_in[(m0 + m) * NO + c] : 0.0f;
+    }
   }
   for (int64_t t = blockIdx.x; t < ntiles; t += gridDim.x) {
     const int64_t m0 = t * TM;
@@ -694,21 +698,26 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     tc::fence_after_sync();
     float z[32];
     tmem_ld_sum32(tbase + lane_base + 32 * hh, z);
-    {
-      float p0, p1, p2;
-      colour_partial(z, hh, B0, W1s, p0, p1, p2);
-      float* r = RED + (hh * TM + m) * 4;
-      r[0] = p0;
-      r[1] = p1;
-      r[2] = p2;
-    }
-    __syncthreads();
     float d[NO];
+    if (y_in) {  // the forward's colours: the same bits as the recomputation below
 #pragma unroll
-    for (int c = 0; c < NO; ++c) {
-      const float o = (B1[c] + RED[m * 4 + c]) + RED[(TM + m) * 4 + c];
-      const float y = sigmoidf_ref(o);
-      d[c] = dy[c] * ((1.0f - y) * y);  // dL/d(pre-sigmoid); 0 on rows past P
+      for (int c = 0; c < NO; ++c) d[c] = dy[c] * ((1.0f - yv[c]) * yv[c]);  // 0 on rows past P
+    } else {     // block-uniform branch: every thread takes the same side of the barrier
+      {
+        float p0, p1, p2;
+        colour_partial(z, hh, B0, W1s, p0, p1, p2);
+        float* r = RED + (hh * TM + m) * 4;
+        r[0] = p0;
+        r[1] = p1;
+        r[2] = p2;
+      }
+      __syncthreads();
+#pragma unroll
+      for (int c = 0; c < NO; ++c) {
+        const float o = (B1[c] + RED[m * 4 + c]) + RED[(TM + m) * 4 + c];
+        const float y = sigmoidf_ref(o);
+        d[c] = dy[c] * ((1.0f - y) * y);  // dL/d(pre-sigmoid); 0 on rows past P
+      }
     }
     if (hh == 0) {
 #pragma unroll
@@ -804,7 +813,10 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
       const int64_t mn = (t + gridDim.x) * TM;
       if (!kBulk) load_row_chunks(X, ldx, xvec != 0, P, mn, m, hh, pre);
 #pragma unroll
-      for (int c = 0; c < NO; ++c) dy[c] = mn + m < P ? d_out[(mn + m) * NO + c] : 0.0f;
+      for (int c = 0; c < NO; ++c) {
+        dy[c] = mn + m < P ? d_out[(mn + m) * NO + c] : 0.0f;
+        if (y_in) yv[c] = mn + m < P ? y_in[(mn + m) * NO + c] : 0.0f;
+      }
     }
     // dX readout while the dW0 MMAs run
     if (hh == 0) {
@@ -1148,8 +1160,8 @@ int vx_radiance_mlp_forward(const float* x, int64_t ldx, int64_t n_points, int i
 
 int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int in_dim, int hidden, int out_dim,
                              const float* W0, const float* b0, const float* W1, const float* b1, const float* d_colors,
-                             float* d_hash, float* d_normal, float* dW0, float* db0, float* dW1, float* db1,
-                             float* partials, int64_t n_partial_floats, void* stream) {
+                             const float* colors, float* d_hash, float* d_normal, float* dW0, float* db0, float* dW1,
+                             float* db1, float* partials, int64_t n_partial_floats, void* stream) {
   VX_REQUIRE(in_dim == KIN && hidden == NH && out_dim == NO, "the fused MLP is %d -> %d -> %d", KIN, NH, NO);
   VX_REQUIRE(n_points >= 0 && ldx >= KIN, "bad sizes");
   VX_REQUIRE(x && W0 && b0 && W1 && b1 && d_colors && d_hash && d_normal && dW0 && db0 && dW1 && db1 && partials,
@@ -1167,7 +1179,7 @@ int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int 
     auto kern = bulk ? k_mlp_bwd_tc<true> : k_mlp_bwd_tc<false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "radiance_mlp_backward: %s", cudaGetErrorString(e));
-    kern<<<nb, 256, smem, st>>>(x, ldx, xvec, n_points, w, d_colors, d_hash, d_normal, partials);
+    kern<<<nb, 256, smem, st>>>(x, ldx, xvec, n_points, w, d_colors, colors, d_hash, d_normal, partials);
   } else {
     cudaMemsetAsync(partials, 0, sizeof(float) * WG, st);
   }

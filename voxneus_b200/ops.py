@@ -554,9 +554,15 @@ def mlp_forward(rows: torch.Tensor, W0, b0, W1, b1) -> torch.Tensor:
     return out
 
 
-def mlp_backward(rows, W0, b0, W1, b1, d_colors):
+def mlp_backward(rows, W0, b0, W1, b1, d_colors, colors=None):
+    """colors: the forward's (P, 3) outputs (the adjoint then skips recomputing the output layer),
+    or None."""
     dev = rows.device
     p = rows.shape[0]
+    if colors is not None:
+        check_tensor(colors, "colors", device=dev)
+        if colors.numel() != 3 * p:
+            raise RuntimeError(f"colors has {colors.numel()} elements, need {3 * p}")
     nb = int(L.query("vx_mlp_blocks", p))
     nf = int(L.query("vx_mlp_partial_floats"))
     sc = Scratch.get(dev)
@@ -567,8 +573,8 @@ def mlp_backward(rows, W0, b0, W1, b1, d_colors):
     dW0, db0, dW1, db1 = (torch.empty_like(t) for t in (W0, b0, W1, b1))
     call("vx_radiance_mlp_backward", ptr(rows), rows.stride(0), p, rows.shape[1], W0.shape[0], W1.shape[0],
          ptr(W0.detach()), ptr(b0.detach()), ptr(W1.detach()), ptr(b1.detach()),
-         ptr(check_tensor(d_colors.contiguous(), "d_colors")), ptr(d_hash), ptr(d_normal), ptr(dW0), ptr(db0),
-         ptr(dW1), ptr(db1), ptr(sc.mlp_partials), sc.mlp_partials.numel(), stream_ptr(dev))
+         ptr(check_tensor(d_colors.contiguous(), "d_colors")), ptr(colors), ptr(d_hash), ptr(d_normal), ptr(dW0),
+         ptr(db0), ptr(dW1), ptr(db1), ptr(sc.mlp_partials), sc.mlp_partials.numel(), stream_ptr(dev))
     return d_hash, d_normal, dW0, db0, dW1, db1
 
 
@@ -627,6 +633,7 @@ class AppearanceMLPFn(torch.autograd.Function):
             rows = rows[:, :width]
         ctx.save_for_backward(rays_o, rays_d, mid, W0, b0, W1, b1)
         ctx.rows = rows
+        ctx.colors = colors if rows is not None else None  # the adjoint's sigmoid derivative reads them
         ctx.handoff = handoff
         ctx.meta = (xyz_min, xyz_max, cfg, active_levels, embeddings.shape, normals.shape)
         return colors.reshape(nr, ns, 3)
@@ -636,11 +643,11 @@ class AppearanceMLPFn(torch.autograd.Function):
         rays_o, rays_d, mid, W0, b0, W1, b1 = ctx.saved_tensors
         xyz_min, xyz_max, cfg, active_levels, eshape, nshape = ctx.meta
         nr, ns = mid.shape
-        rows = ctx.rows
-        ctx.rows = None
+        rows, colors = ctx.rows, ctx.colors
+        ctx.rows = ctx.colors = None
         if rows is None:
             raise RuntimeError("AppearanceMLPFn: forward ran with keep_rows=False; no adjoint input kept")
-        d_hash, d_normal, dW0, db0, dW1, db1 = mlp_backward(rows, W0, b0, W1, b1, g.reshape(-1, 3))
+        d_hash, d_normal, dW0, db0, dW1, db1 = mlp_backward(rows, W0, b0, W1, b1, g.reshape(-1, 3), colors)
         d_emb = None
         if ctx.needs_input_grad[0]:
             d_emb = torch.zeros(eshape, device=g.device)
