@@ -194,12 +194,14 @@ int vx_render_geometry_forward(const float* grid, const int32_t res[3], const fl
 
 /* Adjoint of vx_render_geometry_forward: recomputes positions and normals and accumulates into
  * grid_grad the SDF term (d_sdf) and the Eq.7 term from d_normal (n,3) + d_normal2 (row stride
- * ld2, e.g. the normal columns of the radiance-MLP input gradient) + d_grad; each nullable. */
+ * ld2, e.g. the normal columns of the radiance-MLP input gradient) + d_grad; each nullable.
+ * grad_fwd: the forward's `grad` output (n,3), read instead of recomputing the Eq.7 gradient for
+ * the normalisation's adjoint (the same values), or NULL. */
 int vx_render_geometry_backward(const float* grid, const int32_t res[3], const float xyz_min[3],
                                 const float xyz_max[3], const float* rays_o, const float* rays_d, const float* mid,
                                 int64_t n_rays, int n_samples, const float* d_sdf, const float* d_normal,
-                                const float* d_normal2, int64_t ld2, const float* d_grad, float* grid_grad,
-                                void* stream);
+                                const float* d_normal2, int64_t ld2, const float* d_grad, const float* grad_fwd,
+                                float* grid_grad, void* stream);
 
 /* Radiance-MLP input rows (models/voxneus.py:147-157): hash features (models/radiance_hash.py:71-166,
  * 2 per level, NeuS2 level weights level_weights (nullable = all 1)) in columns [0, 2L), degree-4 SH

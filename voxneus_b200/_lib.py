@@ -45,7 +45,7 @@ _PROTOS = {
     "vx_up_sample": [P, P, P, P, I64, I32, I32, F32, P, P, P, I32, HF3, HF3, P, P],
     "vx_sample_pdf": [P, P, P, I64, I32, I32, P, P, P, P, P],
     "vx_render_geometry_forward": [P, HI3, HF3, HF3, P, P, P, I64, I32, P, P, P, P, P],
-    "vx_render_geometry_backward": [P, HI3, HF3, HF3, P, P, P, I64, I32, P, P, P, I64, P, P, P],
+    "vx_render_geometry_backward": [P, HI3, HF3, HF3, P, P, P, I64, I32, P, P, P, I64, P, P, P, P],
     "vx_appearance_forward": [P, I32, I32, I32, HI3, HF3, P, P, P, P, I32, HF3, HF3, I64, P, I64, I32, P, I64, I32,
                               P, I32, P],
     "vx_hash_encode_backward": [P, I32, I32, I32, HI3, HF3, P, P, P, P, I32, HF3, HF3, I64, P, I64, P],

@@ -363,8 +363,11 @@ class RenderGeometryFn(torch.autograd.Function):
         sdf = torch.empty(nr, ns, device=dev)
         nrm = torch.empty(nr, ns, 3, device=dev)
         gr = torch.empty(nr, ns, 3, device=dev) if want_grad else None
+        # kept for the adjoint (its normalisation term) when the caller does not receive it
+        gkeep = torch.empty(nr, ns, 3, device=dev) if gr is None and ctx.needs_input_grad[0] else None
         call("vx_render_geometry_forward", ptr(g), i3(res), f3(xyz_min), f3(xyz_max), ptr(rays_o), ptr(rays_d),
-             ptr(mid), nr, ns, ptr(sdf), ptr(nrm), ptr(gr), ptr(bitmap), stream_ptr(dev))
+             ptr(mid), nr, ns, ptr(sdf), ptr(nrm), ptr(gr if gr is not None else gkeep), ptr(bitmap), stream_ptr(dev))
+        ctx.gkeep = gkeep
         ctx.save_for_backward(grid, rays_o, rays_d, mid)
         ctx.bounds = (xyz_min, xyz_max)
         ctx.handoff = handoff
@@ -386,7 +389,8 @@ class RenderGeometryFn(torch.autograd.Function):
         gg = torch.zeros(res, device=mid.device)
         d_sdf = None if d_sdf is None else d_sdf.contiguous()
         d_nrm = None if d_nrm is None else d_nrm.contiguous()
-        geometry_backward(g, res, ctx.bounds, rays_o, rays_d, mid, d_sdf, d_nrm, gg, d_nrm2)
+        gkeep, ctx.gkeep = ctx.gkeep, None
+        geometry_backward(g, res, ctx.bounds, rays_o, rays_d, mid, d_sdf, d_nrm, gg, d_nrm2, gkeep)
         return gg.reshape(grid.shape), None, None, None, None, None, None, None, None
 
 
@@ -414,8 +418,9 @@ def _workspace(dev, nbytes: int) -> torch.Tensor:
     return ws
 
 
-def geometry_backward(g, res, bounds, rays_o, rays_d, mid, d_sdf, d_normal, out, d_normal2=None):
-    """d_normal2: a second dL/dnormal source, (P, 3) contiguous, added to d_normal in the kernel."""
+def geometry_backward(g, res, bounds, rays_o, rays_d, mid, d_sdf, d_normal, out, d_normal2=None, grad_fwd=None):
+    """d_normal2: a second dL/dnormal source, (P, 3) contiguous, added to d_normal in the kernel.
+    grad_fwd: the forward's Eq.7 gradients (P, 3), read instead of recomputed (atomic path)."""
     nr, ns = mid.shape
     dev = mid.device
     if d_normal2 is not None:
@@ -432,7 +437,8 @@ def geometry_backward(g, res, bounds, rays_o, rays_d, mid, d_sdf, d_normal, out,
              ws.numel(), stream_ptr(dev))
     else:
         call("vx_render_geometry_backward", ptr(g), i3(res), f3(bounds[0]), f3(bounds[1]), ptr(rays_o), ptr(rays_d),
-             ptr(mid), nr, ns, ptr(d_sdf), ptr(d_normal), ptr(d_normal2), 3, None, ptr(out), stream_ptr(dev))
+             ptr(mid), nr, ns, ptr(d_sdf), ptr(d_normal), ptr(d_normal2), 3, None, ptr(grad_fwd), ptr(out),
+             stream_ptr(dev))
 
 
 def hash_backward(d_emb, cfg, active_levels, pts, rays_o, rays_d, mid, n_samples, xyz_min, xyz_max, n_points,
