@@ -354,7 +354,7 @@ class VoxNeuS(nn.Module):
             _, dists, mid = ops.sample_multistep(self.sdf_grid.grid.detach(), lo, hi, o, d, near, far, ns, ni,
                                                  up_sample_steps, perturb, t_rand, u, occ.occupancy_mask,
                                                  *occ.bounds(), want_z=False)
-        handoff = ops.NormalGradHandoff() if fused_mlp else None
+        handoff = ops.NormalGradHandoff(torch.is_grad_enabled()) if fused_mlp else None
         sdf, normal, gsamp = ops.RenderGeometryFn.apply(self.sdf_grid.grid, o, d, mid, lo, hi, vr_bitmap, extras,
                                                         handoff)
         if fused_mlp:

@@ -347,8 +347,9 @@ class NormalGradHandoff:
     (the same single addition autograd would make, without its (P, 3) sum kernel). The geometry
     adjoint runs after both consumers of the normals, so the hand-off is complete by then."""
 
-    def __init__(self):
+    def __init__(self, training: bool = True):
         self.d_normal = None
+        self.training = training  # the caller's grad mode (Function.forward itself runs without grad)
 
 
 class RenderGeometryFn(torch.autograd.Function):
@@ -363,8 +364,10 @@ class RenderGeometryFn(torch.autograd.Function):
         sdf = torch.empty(nr, ns, device=dev)
         nrm = torch.empty(nr, ns, 3, device=dev)
         gr = torch.empty(nr, ns, 3, device=dev) if want_grad else None
-        # kept for the adjoint (its normalisation term) when the caller does not receive it
-        gkeep = torch.empty(nr, ns, 3, device=dev) if gr is None and ctx.needs_input_grad[0] else None
+        # kept for the adjoint (its normalisation term) when the caller does not receive it; only in
+        # training (needs_input_grad stays True under no_grad)
+        keep = gr is None and ctx.needs_input_grad[0] and handoff is not None and handoff.training
+        gkeep = torch.empty(nr, ns, 3, device=dev) if keep else None
         call("vx_render_geometry_forward", ptr(g), i3(res), f3(xyz_min), f3(xyz_max), ptr(rays_o), ptr(rays_d),
              ptr(mid), nr, ns, ptr(sdf), ptr(nrm), ptr(gr if gr is not None else gkeep), ptr(bitmap), stream_ptr(dev))
         ctx.gkeep = gkeep
