@@ -403,13 +403,14 @@ int64_t vx_reg_stencil_workspace(const int32_t res[3]);
  * called by training/trainer.py:268-319), gather form (deterministic, no atomics), accumulated into
  * grad_grid with weights w_eik and w_curv and scale 2/|V_R|. bitmap is the filtered pair written by
  * vx_vr_count; counts selects its relax half (the reference applies the relax filter only when a
- * vertex passes it) and gives |V_R|. band is unused (applied by vx_vr_count); counter is unused
- * (may be NULL). partials: >= vx_reg_stencil_workspace(res) doubles.
- * losses (device float[2], nullable) receives the monitoring losses. */
+ * vertex passes it) and gives |V_R|. band is applied by vx_vr_count (here it only selects which
+ * count n_active reports); counter is unused (may be NULL). partials: >=
+ * vx_reg_stencil_workspace(res) doubles. losses (device float[2], nullable) receives the monitoring
+ * losses; n_active (device int64, nullable) |V_R| after the relax and band filters. */
 int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[3], const float xyz_min[3],
                    const float xyz_max[3], float relax_radius, float band, const unsigned long long* counts,
                    float w_eik, float w_curv, float* grad_grid, double* partials, int64_t n_partials,
-                   unsigned int* counter, float* losses, void* stream);
+                   unsigned int* counter, float* losses, int64_t* n_active, void* stream);
 
 /* ------------------------------------------------------------ occupancy grid ------------- */
 

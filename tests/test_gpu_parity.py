@@ -368,7 +368,9 @@ def test_fused_stencil_matches_oracle(band, res):
     counts = ops.vr_count(bm, gd, res, lo, hi, 1.2, bnd, filtered=fb)
     assert int(ops.final_count(counts, 1.2, bnd)) == v.shape[0]
     out = torch.zeros(res, device=DEV)
-    losses = ops.reg_stencil(gd, fb, res, lo, hi, 1.2, bnd, counts, 0.1, 5e-4, out)
+    n_active = torch.zeros((), dtype=torch.int64, device=DEV)
+    losses = ops.reg_stencil(gd, fb, res, lo, hi, 1.2, bnd, counts, 0.1, 5e-4, out, n_active=n_active)
+    assert int(n_active) == int(ops.final_count(counts, 1.2, bnd)) == v.shape[0]
     assert_close(out, ge + gc, GRAD_TOL, "fused stencil grad")
     assert abs(losses[0].item() - le.item()) <= 1e-5 * max(le.item(), 1e-12)
     assert abs(losses[1].item() - lc.item()) <= 1e-5 * max(lc.item(), 1e-12)

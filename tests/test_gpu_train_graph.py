@@ -119,3 +119,15 @@ def test_graph_mode_falls_back_to_eager_with_explicit_randoms():
     randoms = m.draw_sampler_randoms(128, 16, 16, 4, DEV)
     out = tr.step(o, d, t, step=3, randoms=randoms)
     assert tr.graph() is None and torch.isfinite(out["loss_rgb"]).all()
+
+
+def test_sampler_draws_are_the_separate_draws():
+    """The per-step uniforms drawn in place into one tensor equal separate draws stacked (the same
+    generator offsets: the reference's draw order is kept)."""
+    m = _model()
+    g1 = torch.Generator(device=DEV).manual_seed(21)
+    t1, u1 = m.draw_sampler_randoms(300, 64, 64, 4, DEV, generator=g1)
+    g2 = torch.Generator(device=DEV).manual_seed(21)
+    t2 = torch.rand((300, 64), device=DEV, generator=g2)
+    u2 = torch.stack([torch.rand((300, 16), device=DEV, generator=g2) for _ in range(4)])
+    assert torch.equal(t1, t2) and torch.equal(u1, u2)

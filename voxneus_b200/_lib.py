@@ -79,7 +79,7 @@ _PROTOS = {
     "vx_vr_compact_noalloc": [P, P, HI3, HF3, HF3, F32, F32, P, P, P, I64, P],
     "vx_reg_stencil_blocks": [HI3],
     "vx_reg_stencil_workspace": [HI3],
-    "vx_reg_stencil": [P, P, HI3, HF3, HF3, F32, F32, P, F32, F32, P, P, I64, P, P, P],
+    "vx_reg_stencil": [P, P, HI3, HF3, HF3, F32, F32, P, F32, F32, P, P, I64, P, P, P, P],
     "vx_grid_upsample": [P, HI3, P, HI3, P],
     "vx_occupancy_workspace": [I64],
     "vx_adam_torch": [P, I32, F32, F32, F32, P],

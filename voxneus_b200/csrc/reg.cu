@@ -425,9 +425,12 @@ __global__ void __launch_bounds__(256) k_reg_stencil(StencilArgs a, const uint8_
   }
 }
 
-// Mean losses over interior vertices from the per-block partials, fixed reduction order.
+// Mean losses over interior vertices from the per-block partials, fixed reduction order; and
+// |V_R| after the filters (relax sphere when it keeps any vertex, band) for n_active.
 __global__ void __launch_bounds__(256) k_reg_finalize(const double* __restrict__ partials, int nblocks,
-                                                      float* __restrict__ losses) {
+                                                      float* __restrict__ losses,
+                                                      const unsigned long long* __restrict__ counts, int relax,
+                                                      int band, long long* __restrict__ n_active) {
   __shared__ double red[3][8];
   double a = 0, b = 0, k = 0;
   for (int i = threadIdx.x; i < nblocks; i += blockDim.x) {
@@ -451,8 +454,14 @@ __global__ void __launch_bounds__(256) k_reg_finalize(const double* __restrict__
       b += red[1][w];
       k += red[2][w];
     }
-    losses[0] = k > 0 ? (float)(a / k) : 0.0f;
-    losses[1] = k > 0 ? (float)(b / k) : 0.0f;
+    if (losses) {
+      losses[0] = k > 0 ? (float)(a / k) : 0.0f;
+      losses[1] = k > 0 ? (float)(b / k) : 0.0f;
+    }
+    if (n_active) {
+      const bool relax_on = relax && counts[1] > 0;
+      *n_active = (long long)(band ? (relax_on ? counts[3] : counts[2]) : (relax_on ? counts[1] : counts[0]));
+    }
   }
 }
 
@@ -527,7 +536,7 @@ int64_t vx_reg_stencil_workspace(const int32_t res[3]) {
 int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[3], const float xyz_min[3],
                    const float xyz_max[3], float relax_radius, float band, const unsigned long long* counts,
                    float w_eik, float w_curv, float* grad_grid, double* partials, int64_t n_partials,
-                   unsigned int* counter, float* losses, void* stream) {
+                   unsigned int* counter, float* losses, int64_t* n_active, void* stream) {
   if (int s = check_reg(res)) return s;
   VX_REQUIRE(grid && bitmap && counts && grad_grid && partials && xyz_min && xyz_max, "null pointer");
   const int64_t nb = vx_reg_stencil_blocks(res);
@@ -541,7 +550,6 @@ int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[
   a.g = make_grid(res, xyz_min, xyz_max);
   a.counts = counts;
   a.relax_r = relax_radius;
-  (void)band;
   a.w_eik = w_eik;
   a.w_curv = w_curv;
   a.gg = grad_grid;
@@ -554,8 +562,10 @@ int vx_reg_stencil(const float* grid, const uint32_t* bitmap, const int32_t res[
   cudaStream_t st = (cudaStream_t)stream;
   k_tile_flags<<<grid_for(ntiles, 256), 256, 0, st>>>(a, (int)ntiles, flags);
   k_reg_stencil<<<(unsigned)nb, 256, 0, st>>>(a, flags, partials, (int)ntiles);
-  if (losses) k_reg_finalize<<<1, 256, 0, st>>>(partials, (int)nb, losses);
-  count_launches(losses ? 3 : 2);
+  if (losses || n_active)
+    k_reg_finalize<<<1, 256, 0, st>>>(partials, (int)nb, losses, counts, relax_radius > 0.0f ? 1 : 0,
+                                      band > 0.0f ? 1 : 0, reinterpret_cast<long long*>(n_active));
+  count_launches(losses || n_active ? 3 : 2);
   return check_launch("reg_stencil");
 }
 

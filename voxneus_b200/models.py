@@ -324,8 +324,10 @@ class VoxNeuS(nn.Module):
         t_rand = torch.rand((n_rays, n_samples), device=device, generator=generator)
         per = max(n_importance // steps, 1) if (n_importance > 0 and steps > 0) else 0
         u = None
-        if per:
-            u = torch.stack([torch.rand((n_rays, per), device=device, generator=generator) for _ in range(steps)])
+        if per:  # each step's draw written in place into its slice (the same values as separate tensors)
+            u = torch.empty((steps, n_rays, per), device=device)
+            for k in range(steps):
+                torch.rand((n_rays, per), device=device, generator=generator, out=u[k])
         return t_rand, u
 
     def render(self, rays_o, rays_d, sampler, near=None, far=None, background_rgb=None, cos_anneal_ratio=0.0,

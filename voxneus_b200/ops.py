@@ -996,8 +996,11 @@ def reg_list(kind: str, grid3, verts, eps, weight, grad_out):
 
 
 def reg_stencil(grid, filtered, res, xyz_min, xyz_max, relax_radius, band, counts, w_eik, w_curv, grad_out,
-                losses=None):
-    """Fused eikonal + curvature into grad_out; `filtered` and `counts` come from vr_count."""
+                losses=None, n_active=None):
+    """Fused eikonal + curvature into grad_out; `filtered` and `counts` come from vr_count.
+    n_active: an int64 device scalar receiving |V_R| after the filters (final_count's value)."""
+    if n_active is not None:
+        check_tensor(n_active, "n_active", dtype=torch.int64, device=grid.device)
     dev = grid.device
     bitmap = filtered
     sc = Scratch.get(dev)
@@ -1006,7 +1009,7 @@ def reg_stencil(grid, filtered, res, xyz_min, xyz_max, relax_radius, band, count
         losses = torch.zeros(2, device=dev)
     call("vx_reg_stencil", ptr(grid), ptr(bitmap), i3(res), f3(xyz_min), f3(xyz_max), float(relax_radius),
          float(band), ptr(counts), float(w_eik), float(w_curv), ptr(grad_out), ptr(partials), partials.numel(),
-         ptr(sc.counter(COUNTER_STENCIL)), ptr(losses), stream_ptr(dev))
+         ptr(sc.counter(COUNTER_STENCIL)), ptr(losses), ptr(n_active), stream_ptr(dev))
     return losses
 
 

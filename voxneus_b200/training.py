@@ -149,6 +149,7 @@ class FusedTrainer:
         self.filtered = ops.new_filtered(self.res, dev)
         self.counts = torch.zeros(4, dtype=torch.int64, device=dev)
         self.reg_losses = torch.zeros(2, device=dev)
+        self.n_active = torch.zeros((), dtype=torch.int64, device=dev)  # |V_R| after the filters
         self.amp_flag = torch.zeros(1, dtype=torch.int32, device=dev)
         # training/trainer.py:171-173: occupancy refresh every `occupancy_update_interval` steps
         # (0 disables). Data-parallel ranks draw the cells from one shared seed so that their
@@ -213,9 +214,9 @@ class FusedTrainer:
         ops.vr_count(self.bitmap, grid.detach(), self.res, lo, hi, self.relax_radius, self.band, self.counts,
                      self.filtered)
         ops.reg_stencil(grid.detach(), self.filtered, self.res, lo, hi, self.relax_radius, self.band, self.counts,
-                        self.w_eik, self.w_curv, grid.grad, self.reg_losses)
+                        self.w_eik, self.w_curv, grid.grad, self.reg_losses, self.n_active)
         return {"loss_rgb": loss.detach(), "loss_eik": self.reg_losses[0], "loss_curv": self.reg_losses[1],
-                "n_active": ops.final_count(self.counts, self.relax_radius, self.band), "rgb": out["rgb"].detach()}
+                "n_active": self.n_active, "rgb": out["rgb"].detach()}
 
     def _eager_step(self, rays_o, rays_d, target, step: int, randoms) -> Dict[str, torch.Tensor]:
         m = self.model
