@@ -131,3 +131,34 @@ def test_sampler_draws_are_the_separate_draws():
     t2 = torch.rand((300, 64), device=DEV, generator=g2)
     u2 = torch.stack([torch.rand((300, 16), device=DEV, generator=g2) for _ in range(4)])
     assert torch.equal(t1, t2) and torch.equal(u1, u2)
+
+
+def test_graph_mode_recaptures_on_a_new_batch_shape():
+    """A new ray count mid-run captures the step again; the steps stay the eager steps' bits."""
+    from voxneus_b200 import ops
+    from voxneus_b200.rendering import RaySampler
+    from voxneus_b200.training import FusedTrainer
+
+    sizes = [192, 192, 192, 256, 256, 192]
+
+    def run(cuda_graph):
+        m = _model()
+        tr = FusedTrainer(m, RaySampler(16, 16, perturb=True), band_voxels=3.0, cuda_graph=cuda_graph)
+        torch.manual_seed(13)
+        outs = []
+        for i, n in enumerate(sizes):
+            o, d, t = _rays(n, 200 + i)
+            outs.append(tr.step(o, d, t, step=i)["loss_rgb"].clone())
+        torch.cuda.synchronize()
+        return m, tr, outs
+
+    ops.set_deterministic(True)
+    try:
+        me, _, le = run(False)
+        mg, tg, lg = run(True)
+    finally:
+        ops.set_deterministic(False)
+    assert tg.graph() is not None and tg.graph().o.shape[0] == sizes[-1]
+    assert all(torch.equal(a, b) for a, b in zip(le, lg))
+    for pa, pb in zip(me.parameters(), mg.parameters()):
+        assert torch.equal(pa, pb)
