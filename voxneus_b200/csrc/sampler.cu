@@ -203,7 +203,7 @@ struct SamplerArgs {
   float* mid;
 };
 
-__global__ void __launch_bounds__(128) k_sample_multistep(SamplerArgs a, const float* __restrict__ fgrid, Grid g, Occ oc) {
+__global__ void __launch_bounds__(128, 9) k_sample_multistep(SamplerArgs a, const float* __restrict__ fgrid, Grid g, Occ oc) {
   extern __shared__ float smem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
@@ -418,7 +418,7 @@ int vx_sample_multistep(const float* grid, const int32_t res[3], const float xyz
   Occ oc = make_occ(occupancy, occ_res, occ_min, occ_max);
   const int threads = 128;
   const size_t smem = (size_t)(threads / 32) * (6 * total + 64) * sizeof(float);
-  k_sample_multistep<<<grid_for(n_rays * 32, threads, 8), threads, smem, (cudaStream_t)stream>>>(a, grid, g, oc);
+  k_sample_multistep<<<grid_for(n_rays * 32, threads, 9), threads, smem, (cudaStream_t)stream>>>(a, grid, g, oc);
   count_launches(1);
   return check_launch("sample_multistep");
 }
