@@ -339,7 +339,8 @@ class VoxNeuS(nn.Module):
         near/far None: computed from the unit sphere inside the sampler kernel. randoms:
         (t_rand, u) uniforms for a perturbed sampler (drawn in the reference order when None).
         vr_bitmap: V_R bitmap receiving every sample's Eq.7 corners. extras: also return pts,
-        sdf_samples, corner_indices, grad_samples, normal_samples like the reference.
+        sdf_samples, corner_indices, grad_samples, normal_samples like the reference; with
+        extras=False the per-sample weights, alpha and transmittance are not written (None).
         """
         dev = rays_o.device
         o = rays_o.contiguous()
@@ -370,7 +371,8 @@ class VoxNeuS(nn.Module):
             colors = self.radiance_mlp.forward_rows(x).reshape(nr, mid.shape[1], 3)
         out_t = ops.CompositeFn.apply(colors, sdf, normal, self.variance_net.variance, d, mid, dists, None, o, True,
                                       self.variance_net._s_max, sphere_radius if sphere_radius else 0.0,
-                                      background_rgb, use_iter_cos_annealing, cos_anneal_ratio, amplify_k, amp_flag)
+                                      background_rgb, use_iter_cos_annealing, cos_anneal_ratio, amplify_k, amp_flag,
+                                      extras)
         keys = ("rgb", "depth", "normal", "opacity", "weights", "alpha", "transmittance")
         out = dict(zip(keys, out_t))
         out["dists"] = dists

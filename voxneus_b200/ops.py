@@ -755,7 +755,7 @@ class CompositeFn(torch.autograd.Function):
 
     @staticmethod
     def forward(ctx, colors, sdf, normals, s_param, dirs, z, dists, pts, rays_o, s_is_variance, s_max, radius,
-                background, iter_cos, cos_anneal, amplify_k, amp_flag):
+                background, iter_cos, cos_anneal, amplify_k, amp_flag, per_sample=True):
         nr, ns = z.shape
         dev = z.device
         colors_c = check_tensor(colors.detach().reshape(nr, ns, 3).contiguous(), "colors")
@@ -771,9 +771,10 @@ class CompositeFn(torch.autograd.Function):
             bg = check_tensor(background.detach().contiguous(), "background")
             bg_per_ray = 1 if bg.dim() == 2 else 0
         ptsc = None if pts is None else check_tensor(pts.detach().reshape(nr, ns, 3).contiguous(), "pts")
+        # per_sample=False: the (N, S) weights, alpha and transmittance are neither written nor returned
         outs = [torch.empty(nr, 3, device=dev), torch.empty(nr, 1, device=dev), torch.empty(nr, 3, device=dev),
-                torch.empty(nr, 1, device=dev), torch.empty(nr, ns, device=dev), torch.empty(nr, ns, device=dev),
-                torch.empty(nr, ns, device=dev)]
+                torch.empty(nr, 1, device=dev)]
+        outs += [torch.empty(nr, ns, device=dev) if per_sample else None for _ in range(3)]
         call("vx_composite_forward", ptr(colors_c), ptr(sdf_c), ptr(nrm_c), ptr(d), drs, dss, ptr(z), ptr(dists),
              ptr(ptsc), ptr(rays_o), ptr(s_c), int(s_is_variance), float(s_max), float(radius), ptr(bg), bg_per_ray,
              int(iter_cos), float(cos_anneal), nr, ns, *[ptr(t) for t in outs], stream_ptr(dev))
@@ -810,7 +811,7 @@ class CompositeFn(torch.autograd.Function):
              ptr(d_colors), ptr(d_sdf), ptr(d_n), ptr(partials), int(partials.numel()),
              ptr(sc.counter(COUNTER_COMPOSITE)), ptr(d_s), amp_k, ptr(amp_flag), stream_ptr(dev))
         return (d_colors.reshape(c_shape), d_sdf.reshape(sdf_shape), d_n.reshape(n_shape), d_s.reshape(s_shape),
-                None, None, None, None, None, None, None, None, None, None, None, None, None)
+                None, None, None, None, None, None, None, None, None, None, None, None, None, None)
 
 
 class NeusAlphaFn(torch.autograd.Function):
