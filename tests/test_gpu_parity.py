@@ -491,14 +491,16 @@ def test_fused_mlp_matches_oracle(p, ld):
     assert _lib.query("vx_tensor_core_timeouts") == 0
 
 
-def test_mlp_adjoint_with_forward_colours_is_bitwise_the_recompute():
+@pytest.mark.parametrize("ld", [52, 56])
+def test_mlp_adjoint_with_forward_colours_is_bitwise_the_recompute(ld):
     """The adjoint reading the forward's colours (for the sigmoid's derivative) instead of
-    recomputing the output layer gives the same bits: same MMAs, same partial sums."""
+    recomputing the output layer gives the same bits: same MMAs, same partial sums (52-float rows
+    take the bulk-copy kernels, other strides the register-prefetch ones)."""
     from voxneus_b200 import ops
 
     torch.manual_seed(5)
     p = 3001  # a partial last tile
-    rows = torch.randn(p, 52, device=DEV)[:, :51]  # 51 features in 52-float rows, as the render keeps them
+    rows = torch.randn(p, ld, device=DEV)[:, :51]  # 51 features in ld-float rows
     W0 = 0.2 * torch.randn(64, 51, device=DEV)
     b0 = 0.1 * torch.randn(64, device=DEV)
     W1 = 0.2 * torch.randn(3, 64, device=DEV)
