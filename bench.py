@@ -64,20 +64,8 @@ def config(args, world):
 
 def make_scene(res, device, seed=0):
     from voxneus_b200 import synthetic
-    from voxneus_b200.models import VoxNeuS
 
-    torch.manual_seed(seed)
-    m = VoxNeuS(grid_res=res // 2, occupancy_res=128).to(device)
-    with torch.no_grad():
-        m.sdf_grid.grid.copy_(synthetic.shapes_grid(res // 2, seed=seed).to(device))
-        m.radiance_hash.encoder.embeddings.uniform_(-1e-2, 1e-2)
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record()
-    m.sdf_grid.scale_volume_grid(res)  # trilinear 128^3 -> 256^3 on the device
-    t1.record()
-    torch.cuda.synchronize()
-    return m, t0.elapsed_time(t1)
+    return synthetic.throughput_scene(res, device, seed=seed)
 
 
 class ClockSampler:

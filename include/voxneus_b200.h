@@ -97,6 +97,12 @@ typedef struct vx_adam_segment {
 } vx_adam_segment;
 int vx_adam_torch(const vx_adam_segment* segs, int n_segs, float beta1, float beta2, float eps, void* stream);
 
+/* SparseGridAdam's vectorised torch path (training/optimizer.py:86-113, the plain-PyTorch mode of
+ * the grid optimizer): the torch formula above, and elements whose gradient is exactly 0 keep p, m
+ * and v. Same segments as vx_adam_torch (step_scalars/lr_flag optional). */
+int vx_masked_adam_torch(const vx_adam_segment* segs, int n_segs, float beta1, float beta2, float eps,
+                         void* stream);
+
 /* Host helpers giving exactly the scalars the updates above compute from (step, lr): the
  * reference formula's step size lr * sqrt(1 - b2^t) / (1 - b1^t) in float, and torch's
  * {lr / (1 - b1^t), 1 / sqrt(1 - b2^t)} in double rounded to float. */

@@ -106,7 +106,7 @@ def interpolate_gradients(grid5, coords, eps, res):
 
 def query_normals(grid5, xyz, xyz_min, xyz_max):
     """models/sdf_grid.py:122-160 (interpolated mode)."""
-    res = torch.tensor(grid5.shape[-3:], dtype=torch.float32)
+    res = torch.tensor(grid5.shape[-3:], dtype=torch.float32, device=grid5.device)
     coords = world_to_grid(xyz, xyz_min, xyz_max, res)
     eps = voxel_size(xyz_min, xyz_max, res)
     return interpolate_gradients(grid5, coords, eps, [int(r) for r in res])
@@ -139,11 +139,12 @@ def sample_pdf(bins, weights, n_samples: int, det: bool, u=None, eps: float = 1e
     cdf = torch.cat([torch.zeros_like(cdf[..., :1]), cdf], dim=-1)
     lead = list(cdf.shape[:-1])
     if det:
-        u = torch.linspace(0.5 / n_samples, 1.0 - 0.5 / n_samples, steps=n_samples, dtype=cdf.dtype)
+        u = torch.linspace(0.5 / n_samples, 1.0 - 0.5 / n_samples, steps=n_samples, dtype=cdf.dtype,
+                           device=cdf.device)
         u = u.expand(lead + [n_samples]).contiguous()
     else:
         if u is None:
-            u = torch.rand(lead + [n_samples], dtype=cdf.dtype)
+            u = torch.rand(lead + [n_samples], dtype=cdf.dtype, device=cdf.device)
         u = u.to(cdf.dtype).contiguous()
     idx = torch.searchsorted(cdf, u, right=True)
     below = torch.clamp(idx - 1, min=0)
@@ -163,7 +164,7 @@ def sample_pdf(bins, weights, n_samples: int, det: bool, u=None, eps: float = 1e
 
 def sample_stratified(near, far, n_samples: int, perturb: bool, t_rand=None):
     """rendering/sampler.py:85-125.  ``t_rand`` replaces the rand_like draw (sampler.py:117)."""
-    t = torch.linspace(0.0, 1.0, steps=n_samples, dtype=near.dtype)
+    t = torch.linspace(0.0, 1.0, steps=n_samples, dtype=near.dtype, device=near.device)
     z = near * (1.0 - t) + far * t
     if perturb:
         mids = 0.5 * (z[..., 1:] + z[..., :-1])
@@ -228,7 +229,7 @@ def up_sample(o, d, z, sdf, n_importance: int, inv_s: float, det: bool, occ_fn=N
     z0, z1 = z[:, :-1], z[:, 1:]
     fm = (f0 + f1) * 0.5
     cos = (f1 - f0) / (z1 - z0 + 1e-5)
-    prev = torch.cat([torch.zeros([nr, 1], dtype=z.dtype), cos[:, :-1]], dim=-1)
+    prev = torch.cat([torch.zeros([nr, 1], dtype=z.dtype, device=z.device), cos[:, :-1]], dim=-1)
     cos = torch.min(torch.stack([prev, cos], dim=-1), dim=-1)[0]
     cos = cos.clip(-1e3, 0.0) * inside
     dist = z1 - z0
@@ -237,7 +238,8 @@ def up_sample(o, d, z, sdf, n_importance: int, inv_s: float, det: bool, occ_fn=N
     c0 = torch.sigmoid(e0 * inv_s)
     c1 = torch.sigmoid(e1 * inv_s)
     alpha = (c0 - c1 + 1e-5) / (c0 + 1e-5)
-    trans = torch.cumprod(torch.cat([torch.ones([nr, 1], dtype=z.dtype), 1.0 - alpha + 1e-7], -1), -1)[:, :-1]
+    trans = torch.cumprod(torch.cat([torch.ones([nr, 1], dtype=z.dtype, device=z.device), 1.0 - alpha + 1e-7], -1),
+                          -1)[:, :-1]
     w = alpha * trans
     if occ_fn is not None:
         zm = (z0 + z1) * 0.5
@@ -329,7 +331,8 @@ def composite_weights(alpha, eps: float = 1e-7):
     """
     n = alpha.shape[0]
     q = torch.clamp(1.0 - alpha + eps, min=0.0, max=1.0)
-    t = torch.cumprod(torch.cat([torch.ones([n, 1], dtype=alpha.dtype), q], dim=-1), dim=-1)[:, :-1]
+    t = torch.cumprod(torch.cat([torch.ones([n, 1], dtype=alpha.dtype, device=alpha.device), q], dim=-1),
+                      dim=-1)[:, :-1]
     w = alpha * t
     w = torch.where(t < 1e-4, torch.zeros_like(w), w)
     return w, t
@@ -412,15 +415,15 @@ def hash_encode(norm_xyz, embeddings, resolutions: Sequence[int], active_levels=
     lead = x.shape[:-1]
     xf = x.reshape(-1, 3)
     n_levels, tsize, nf = embeddings.shape
-    primes = torch.tensor(HASH_PRIMES, dtype=torch.int64)
+    primes = torch.tensor(HASH_PRIMES, dtype=torch.int64, device=xf.device)
     outs = []
     sel = [(a, b, c) for a in (0, 1) for b in (0, 1) for c in (0, 1)]
     for lvl in range(n_levels):
         lw = level_weight(lvl, active_levels)
         if lw == 0.0:
-            outs.append(torch.zeros((xf.shape[0], nf), dtype=embeddings.dtype))
+            outs.append(torch.zeros((xf.shape[0], nf), dtype=embeddings.dtype, device=xf.device))
             continue
-        sx = xf * torch.tensor(resolutions[lvl], dtype=torch.float32).to(xf.dtype)
+        sx = xf * torch.tensor(resolutions[lvl], dtype=torch.float32, device=xf.device).to(xf.dtype)
         lo = torch.floor(sx).to(torch.int64)
         up = lo + 1
         dd = sx - lo.to(sx.dtype)
@@ -511,13 +514,13 @@ def eikonal(grid, verts, eps, res, weight: float = 1.0, eps_norm: float = 1e-8):
     """
     f = grid.reshape(grid.shape[-3:])
     res = tuple(int(r) for r in res)
-    g = torch.zeros(res, dtype=f.dtype)
+    g = torch.zeros(res, dtype=f.dtype, device=f.device)
     nv = verts.shape[0]
     if nv == 0:
-        return torch.tensor(0.0, dtype=f.dtype), g
+        return torch.tensor(0.0, dtype=f.dtype, device=f.device), g
     v = verts[_interior(verts, res)]
     if v.shape[0] == 0:
-        return torch.tensor(0.0, dtype=f.dtype), g
+        return torch.tensor(0.0, dtype=f.dtype, device=f.device), g
     i, j, k = v[:, 0], v[:, 1], v[:, 2]
     dx, dy, dz = 2.0 * eps[0], 2.0 * eps[1], 2.0 * eps[2]
     nx = (f[i + 1, j, k] - f[i - 1, j, k]) / dx
@@ -541,13 +544,13 @@ def curvature(grid, verts, eps, res, weight: float = 1.0):
     """Closed-form Laplacian curvature loss and gradient (Eq.12-14).  regularization/curvature.py:100-165."""
     f = grid.reshape(grid.shape[-3:])
     res = tuple(int(r) for r in res)
-    g = torch.zeros(res, dtype=f.dtype)
+    g = torch.zeros(res, dtype=f.dtype, device=f.device)
     nv = verts.shape[0]
     if nv == 0:
-        return torch.tensor(0.0, dtype=f.dtype), g
+        return torch.tensor(0.0, dtype=f.dtype, device=f.device), g
     v = verts[_interior(verts, res)]
     if v.shape[0] == 0:
-        return torch.tensor(0.0, dtype=f.dtype), g
+        return torch.tensor(0.0, dtype=f.dtype, device=f.device), g
     i, j, k = v[:, 0], v[:, 1], v[:, 2]
     e2 = (eps[0] * eps[0], eps[1] * eps[1], eps[2] * eps[2])
     fc = f[i, j, k]
@@ -580,8 +583,16 @@ def upsample_grid(grid5: torch.Tensor, new_res) -> torch.Tensor:
 # ---------------------------------------------------------------------------------------
 
 
-def sparse_adam_step(p, grad, state, lr, betas=(0.9, 0.99), eps=1e-8):
-    """SparseGridAdam's torch path (training/optimizer.py:86-113): update only grad != 0 entries."""
+def sparse_adam_step(p, grad, state, lr, betas=(0.9, 0.99), eps=1e-8, formula: str = "torch"):
+    """SparseGridAdam (training/optimizer.py:32-116): update only the grad != 0 entries.
+
+    formula="torch": the vectorised torch path (optimizer.py:86-113),
+        p -= lr/(1-b1^t) * m / (sqrt(v)/sqrt(1-b2^t) + eps).
+    formula="cuda": the extension kernel the reference's optimizer dispatches to on a GPU
+        (optimizer.py:64-77 -> cuda/adam_upd_kernel.cu:23-38 with the step size of
+        cuda/adam_upd.cpp), p -= lr*sqrt(1-b2^t)/(1-b1^t) * m / (sqrt(v) + eps).
+    The two differ only in where eps enters (by sqrt(1-b2^t)).
+    """
     b1, b2 = betas
     if not state:
         state["step"] = 0
@@ -598,13 +609,25 @@ def sparse_adam_step(p, grad, state, lr, betas=(0.9, 0.99), eps=1e-8):
         v = state["exp_avg_sq"][mask] * b2 + (1.0 - b2) * (g * g)
         state["exp_avg"][mask] = m
         state["exp_avg_sq"][mask] = v
-        step_size = lr / (1.0 - b1 ** t)
-        den = torch.sqrt(v) / math.sqrt(1.0 - b2 ** t) + eps
+        if formula == "cuda":
+            step_size = lr * math.sqrt(1.0 - b2 ** t) / (1.0 - b1 ** t)
+            den = torch.sqrt(v) + eps
+        else:
+            step_size = lr / (1.0 - b1 ** t)
+            den = torch.sqrt(v) / math.sqrt(1.0 - b2 ** t) + eps
         p[mask] -= step_size * (m / den)
 
 
+def lr_factor(step: int, total_steps: int) -> float:
+    """Cosine decay of the hash and MLP learning rates to 0.05 (training/trainer.py:333)."""
+    return (math.cos(math.pi * step / max(total_steps, 1)) + 1.0) * 0.5 * (1.0 - 0.05) + 0.05
+
+
 class OracleScene:
-    """Parameters of one scene with the reference's state_dict naming (models/voxneus.py:21-92)."""
+    """Parameters of one scene with the reference's state_dict naming (models/voxneus.py:21-92).
+
+    The tensors may live on any device: the oracle's ops follow the device of the grid.
+    """
 
     def __init__(self, grid5, variance, embeddings, w0, b0, w1, b1, occupancy=None,
                  xyz_min=(-1.0, -1.0, -1.0), xyz_max=(1.0, 1.0, 1.0), s_max=300.0):
@@ -613,8 +636,9 @@ class OracleScene:
         self.embeddings = embeddings
         self.w0, self.b0, self.w1, self.b1 = w0, b0, w1, b1
         self.occupancy = occupancy
-        self.xyz_min = torch.tensor(xyz_min, dtype=grid5.dtype)
-        self.xyz_max = torch.tensor(xyz_max, dtype=grid5.dtype)
+        self.device = grid5.device
+        self.xyz_min = torch.tensor(xyz_min, dtype=grid5.dtype, device=self.device)
+        self.xyz_max = torch.tensor(xyz_max, dtype=grid5.dtype, device=self.device)
         self.s_max = s_max
         self.resolutions = hash_level_resolutions(embeddings.shape[0])
 
@@ -625,7 +649,8 @@ class OracleScene:
         return [int(r) for r in self.grid.shape[-3:]]
 
     def eps(self):
-        return voxel_size(self.xyz_min, self.xyz_max, torch.tensor(self.res(), dtype=torch.float32))
+        return voxel_size(self.xyz_min, self.xyz_max, torch.tensor(self.res(), dtype=torch.float32,
+                                                                   device=self.device))
 
     def sdf_fn(self, p):
         return query_sdf(self.grid, p, self.xyz_min, self.xyz_max).squeeze(-1)
@@ -634,11 +659,19 @@ class OracleScene:
         return is_occupied(self.occupancy, p, self.xyz_min, self.xyz_max)
 
     def render(self, o, d, near, far, n_samples=64, n_importance=64, steps=4, perturb=False,
-               t_rand=None, us=None, active_levels=None, background=None):
-        """models/voxneus.py:169-260 (pass 1 sampler, pass 2 midpoints, pass 3 compositing)."""
-        z, dists, mid = sample_multistep_sdf(o, d, near, far, self.sdf_fn, n_samples, n_importance, steps,
-                                             perturb, self.occ_fn if self.occupancy is not None else None,
-                                             t_rand=t_rand, us=us)
+               t_rand=None, us=None, active_levels=None, background=None, z_vals=None):
+        """models/voxneus.py:169-260 (pass 1 sampler, pass 2 midpoints, pass 3 compositing).
+
+        z_vals: the sampler's output for these rays, given instead of running the sampler (its
+        dists and midpoints are then formed as in rendering/sampler.py:197-202)."""
+        if z_vals is None:
+            z, dists, mid = sample_multistep_sdf(o, d, near, far, self.sdf_fn, n_samples, n_importance, steps,
+                                                 perturb, self.occ_fn if self.occupancy is not None else None,
+                                                 t_rand=t_rand, us=us)
+        else:
+            z = z_vals
+            dists = torch.cat([z[..., 1:] - z[..., :-1], z[..., -1:] - z[..., -2:-1]], dim=-1)
+            mid = z + dists * 0.5
         pts = o.unsqueeze(1) + d.unsqueeze(1) * mid.unsqueeze(-1)
         dirs = d.unsqueeze(1).expand_as(pts)
         sdf = query_sdf(self.grid, pts, self.xyz_min, self.xyz_max)
@@ -653,10 +686,20 @@ class OracleScene:
         return out
 
     def train_step(self, o, d, target, w_eik=0.1, w_curv=5e-4, band_voxels=None, amplify_k=None,
-                   huber_delta=0.1, optimize=False, **render_kw):
-        """The timed unit: training/trainer.py:188-326 without the optimizer step.
+                   huber_delta=0.1, optimize=False, step=None, total_steps=40000, s_warmup_steps=5000,
+                   lr_sdf=0.1, lr_hash=0.01, lr_mlp=0.001, lr_variance=0.0005, grid_adam="torch", **render_kw):
+        """The timed unit: training/trainer.py:166-393 (render, Huber loss, backward, V_R with the
+        relax filter, eikonal + curvature into grid.grad, s amplification, optimizer steps).
 
-        Returns a dict with losses, |V_R| and the gradients of every parameter.
+        step=None: the amplification runs when amplify_k is given and the learning rates are the
+        base ones. step=k: the trainer's rules at step k: amplification (k = amplify_k or 5) only
+        when step >= s_warmup_steps (:311-315), the hash and MLP learning rates scaled by the
+        cosine factor and the variance learning rate multiplied by k when the gradient was
+        amplified (:317-329). optimize=True runs SparseGridAdam(0.9, 0.99) on the grid (formula
+        `grid_adam`, see sparse_adam_step) and torch.optim.Adam(0.9, 0.999) on the rest
+        (training/optimizer.py:119-154); the state persists across calls on this scene.
+        Returns the losses, |V_R|, the V_R linear indices, the amplification flag and the
+        gradients of every parameter (after the amplification).
         """
         for p in self.params():
             p.grad = None
@@ -675,19 +718,31 @@ class OracleScene:
             self.grid.grad.add_(ge.reshape(self.grid.shape))
             self.grid.grad.add_(gc.reshape(self.grid.shape))
         amplified = False
-        if amplify_k is not None:
-            amplified = amplify_s_gradient(self.variance, amplify_k)
+        k = 5.0 if amplify_k is None else float(amplify_k)
+        if step is None:
+            if amplify_k is not None:
+                amplified = amplify_s_gradient(self.variance, k)
+            lrs = (lr_hash, lr_mlp, lr_variance)
+        else:
+            if step >= s_warmup_steps:
+                amplified = amplify_s_gradient(self.variance, k)
+            f = lr_factor(step, total_steps)
+            lrs = (lr_hash * f, lr_mlp * f, lr_variance * (k if amplified else 1.0))
+        grads = {"grid": self.grid.grad.clone(), "variance": self.variance.grad.clone(),
+                 "embeddings": self.embeddings.grad.clone(), "w0": self.w0.grad.clone(),
+                 "b0": self.b0.grad.clone(), "w1": self.w1.grad.clone(), "b1": self.b1.grad.clone()}
         if optimize:
-            # training/optimizer.py:119-154: SparseGridAdam(0.9, 0.99) for the grid, Adam for the rest
             if not hasattr(self, "_opt_state"):
                 self._opt_state = {}
-                self._net_opt = torch.optim.Adam([{"params": [self.embeddings], "lr": 0.01},
-                                                  {"params": [self.w0, self.b0, self.w1, self.b1], "lr": 0.001},
-                                                  {"params": [self.variance], "lr": 0.0005}], betas=(0.9, 0.999))
-            sparse_adam_step(self.grid, self.grid.grad, self._opt_state, lr=0.1)
+                self._net_opt = torch.optim.Adam([{"params": [self.embeddings], "lr": lr_hash},
+                                                  {"params": [self.w0, self.b0, self.w1, self.b1], "lr": lr_mlp},
+                                                  {"params": [self.variance], "lr": lr_variance}],
+                                                 betas=(0.9, 0.999), eps=1e-8)
+            for grp, lr in zip(self._net_opt.param_groups, lrs):
+                grp["lr"] = lr
+            sparse_adam_step(self.grid, self.grid.grad, self._opt_state, lr=lr_sdf, formula=grid_adam)
             self._net_opt.step()
+        r1, r2 = self.res()[1], self.res()[2]
+        lin = verts[:, 0] * (r1 * r2) + verts[:, 1] * r2 + verts[:, 2]
         return {"loss_rgb": loss.detach(), "loss_eik": le, "loss_curv": lc, "n_active": verts.shape[0],
-                "amplified": amplified, "render": out,
-                "grads": {"grid": self.grid.grad.clone(), "variance": self.variance.grad.clone(),
-                          "embeddings": self.embeddings.grad.clone(), "w0": self.w0.grad.clone(),
-                          "b0": self.b0.grad.clone(), "w1": self.w1.grad.clone(), "b1": self.b1.grad.clone()}}
+                "vr_linear": lin, "amplified": amplified, "render": out, "grads": grads}

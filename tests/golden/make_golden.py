@@ -1,8 +1,9 @@
 """Generate golden vectors from the reference implementation (rishidevde/VoxNeus).
 
-Run in a container where the reference source tree is available (read-only):
+Run in a container where the reference source tree is available (read-only), pointing at the
+reference's ``Code/`` directory by argument or by the VOXNEUS_REFERENCE environment variable:
 
-    python tests/golden/make_golden.py --reference /root/reference/Code
+    python tests/golden/make_golden.py --reference <reference>/Code [--only NAME ...]
 
 It imports the reference's own Python modules in their pure-PyTorch mode (the reference's
 optional CUDA extension is not built, so every call takes its plain torch path), runs each
@@ -126,24 +127,27 @@ def gen_sampler(R):
     save("sampler.npz", bins=bins, weights=weights, det=det, u=u, sto=sto, rays_o=o, rays_d=d, near=near, far=far)
 
 
-def gen_render(R, perturb: bool, name: str):
+def gen_render(R, perturb: bool, name: str, n_samples: int = 16, n_importance: int = 16, grid_res: int = 24,
+               hash_log2: int = 8, n_rays: int = 24):
     torch.manual_seed(4)
-    model = R["VoxNeuS"](grid_res=24, hash_n_levels=16, hash_log2_size=8, occupancy_res=8, force_pytorch=True)
+    model = R["VoxNeuS"](grid_res=grid_res, hash_n_levels=16, hash_log2_size=hash_log2, occupancy_res=8,
+                         force_pytorch=True)
     with torch.no_grad():
         model.sdf_grid.grid.add_(torch.randn_like(model.sdf_grid.grid) * 0.01)
         model.radiance_hash.encoder.embeddings.uniform_(-0.5, 0.5)
         occ = torch.rand(8, 8, 8) > 0.3
         model.occupancy_grid.occupancy_mask.copy_(occ)
-    o, d = hemisphere_rays(24, seed=5)
+    o, d = hemisphere_rays(n_rays, seed=5)
     near, far = R["rays"].near_far_from_sphere(o, d, radius=1.0)
-    sampler = R["sampler"].RaySampler(n_samples=16, n_importance=16, perturb=perturb)
-    target = torch.rand(24, 3)
+    sampler = R["sampler"].RaySampler(n_samples=n_samples, n_importance=n_importance, perturb=perturb)
+    target = torch.rand(n_rays, 3)
+    per = n_importance // 4
     torch.manual_seed(6)
-    t_rand = torch.rand(24, 16) if perturb else torch.zeros(0)
-    us = [torch.rand(24, 4) for _ in range(4)] if perturb else []
+    t_rand = torch.rand(n_rays, n_samples) if perturb else torch.zeros(0)
+    us = [torch.rand(n_rays, per) for _ in range(4)] if perturb else []
     torch.manual_seed(6)
     z, dists, mid = sampler.sample_multistep_sdf(o, d, near, far, lambda p: model.sdf_grid.query_sdf(p).squeeze(-1),
-                                                 n_samples=16, n_importance=16, up_sample_steps=4,
+                                                 n_samples=n_samples, n_importance=n_importance, up_sample_steps=4,
                                                  occupancy_grid=model.occupancy_grid)
     torch.manual_seed(6)
     out = model.render(o, d, sampler, near, far, up_sample_steps=4, sphere_radius=1.0)
@@ -249,11 +253,130 @@ def gen_occupancy(R):
     save("occupancy.npz", **out)
 
 
+class _FixedBatch:
+    """Dataset stand-in for the reference trainer: every sample_rays call returns the same batch
+    and draws no random numbers, so the sampler's draws are the only ones inside a step."""
+
+    def __init__(self, o, d, rgb):
+        self.o, self.d, self.rgb = o, d, rgb
+        self.test_views = []
+
+    def sample_rays(self, batch_size):
+        return {"rays_o": self.o, "rays_d": self.d, "rgb": self.rgb}
+
+
+def _trainer_snapshot(prefix, model, trainer, out):
+    """Parameters, gradients and both optimizers' Adam moments, keyed by the state_dict names."""
+    named = dict(model.named_parameters())
+    for k, p in named.items():
+        out[f"{prefix}param/{k}"] = p.detach().clone()
+        if p.grad is not None:
+            out[f"{prefix}grad/{k}"] = p.grad.detach().clone()
+    for opt in trainer.optimizers.values():
+        for k, p in named.items():
+            st = opt.state.get(p)
+            if st:
+                out[f"{prefix}exp_avg/{k}"] = st["exp_avg"].clone()
+                out[f"{prefix}exp_avg_sq/{k}"] = st["exp_avg_sq"].clone()
+                out[f"{prefix}adam_step/{k}"] = torch.tensor(float(st["step"]))
+
+
+def gen_train_step(R):
+    """Steps 1 and 2 of the reference's own VoxNeuSTrainer.train_step (training/trainer.py:166-393):
+    render with RaySampler(64, 64, perturb=True), Huber loss, backward, V_R in the relax sphere,
+    eikonal + curvature into grid.grad at the scheduler's weights, the k = 5 s amplification
+    (s_warmup_steps = 0, so it is live), the cosine learning rates and the amplified variance rate,
+    SparseGridAdam(0.9, 0.99) on the grid (its torch path) and Adam on the rest. Steps 1 and 2 draw
+    no occupancy cells (the refresh runs at multiples of 16). The targets are the first seeded ones
+    whose s gradient is negative (amplified) at step 1 and positive at step 2, so both branches of
+    the rule are pinned. The sampler's uniforms of each step are regenerated from its seed and
+    saved, with the z it returned. The trainer state after step 2 is also written with the
+    reference's own save_checkpoint (checkpoint_step2.pt), with a deterministic render of that
+    model."""
+    import contextlib
+    import io
+    import tempfile
+
+    from voxneus.training.checkpoint import save_checkpoint
+    from voxneus.training.trainer import VoxNeuSTrainer
+
+    n_rays, ns, ni = 32, 64, 64
+    o, d = hemisphere_rays(n_rays, seed=9)
+    cfg = {"training": {"total_steps": 40000, "batch_size": n_rays, "loss_type": "Huber",
+                        "occupancy_update_interval": 16, "progressive_hash": False, "save_interval": 10 ** 9},
+           "sampler": {"n_samples": ns, "n_importance": ni, "perturb": True, "up_sample_steps": 4},
+           "scheduler": {"s_warmup_steps": 0, "s_amplification_k": 5.0},
+           "optimizer": {"lr_sdf": 0.1, "lr_hash": 0.01, "lr_mlp": 0.001, "lr_variance": 0.0005},
+           "model": {}, "logging": {"dashboard_interval": 10 ** 9, "print_interval": 10 ** 9}}
+
+    def build(target_seed):
+        torch.manual_seed(8)
+        model = R["VoxNeuS"](grid_res=20, hash_n_levels=16, hash_log2_size=7, occupancy_res=8, force_pytorch=True)
+        with torch.no_grad():
+            model.sdf_grid.grid.add_(torch.randn_like(model.sdf_grid.grid) * 0.01)
+            model.radiance_hash.encoder.embeddings.uniform_(-0.5, 0.5)
+            model.occupancy_grid.occupancy_mask.copy_(torch.rand(8, 8, 8) > 0.3)
+        tgt = torch.rand(n_rays, 3, generator=torch.Generator().manual_seed(target_seed))
+        tr = VoxNeuSTrainer(model, _FixedBatch(o, d, tgt), cfg, output_dir=tempfile.mkdtemp(prefix="vx_golden_"),
+                            device=torch.device("cpu"))
+        return model, tr, tgt
+
+    def run(model, tr, out, steps=(1, 2)):
+        _trainer_snapshot("init/", model, tr, out)
+        seen = {}
+        sample = tr.sampler.sample_multistep_sdf
+
+        def recording(*args, **kw):  # keeps the sampler's z of the step (behaviour unchanged)
+            r = sample(*args, **kw)
+            seen["z"] = r[0].detach().clone()
+            return r
+
+        tr.sampler.sample_multistep_sdf = recording
+        for k in steps:
+            torch.manual_seed(100 + k)
+            out[f"step{k}/t_rand"] = torch.rand(n_rays, ns)
+            out[f"step{k}/us"] = torch.stack([torch.rand(n_rays, ni // 4) for _ in range(4)])
+            torch.manual_seed(100 + k)
+            met = tr.train_step(k)
+            for key in ("loss_rgb", "loss_eik", "loss_curv", "w_eik", "w_curv", "lr_hash", "lr_mlp", "lr_s"):
+                out[f"step{k}/{key}"] = torch.tensor(float(met[key]), dtype=torch.float64)
+            out[f"step{k}/s_amplified"] = torch.tensor(bool(met["s_amplified"]))
+            out[f"step{k}/z"] = seen["z"]
+            _trainer_snapshot(f"step{k}/", model, tr, out)
+
+    for seed in range(64):  # the first target whose s gradient is negative at step 1 and positive at step 2
+        model, tr, tgt = build(seed)
+        out = {"rays_o": o, "rays_d": d, "target": tgt, "occupancy": model.occupancy_grid.occupancy_mask.clone(),
+               "target_seed": torch.tensor(seed)}
+        with contextlib.redirect_stdout(io.StringIO()):
+            run(model, tr, out)
+        if bool(out["step1/s_amplified"]) and not bool(out["step2/s_amplified"]):
+            break
+    else:
+        raise RuntimeError("no target seed gives both s-gradient signs")
+    save("train_step.npz", **out)
+    path = os.path.join(HERE, "checkpoint_step2.pt")
+    save_checkpoint(path, 2, model, tr.optimizers, {"note": "golden fixture"},
+                    {"loss_rgb": float(out["step2/loss_rgb"])})
+    ro, rd = hemisphere_rays(16, seed=21)
+    near, far = R["rays"].near_far_from_sphere(ro, rd, radius=1.0)
+    with torch.no_grad():
+        rend = model.render(ro, rd, R["sampler"].RaySampler(n_samples=ns, n_importance=ni, perturb=False), near, far,
+                            up_sample_steps=4, sphere_radius=1.0)
+    save("checkpoint_render.npz", rays_o=ro, rays_d=rd, rgb=rend["rgb"], depth=rend["depth"], normal=rend["normal"],
+         opacity=rend["opacity"])
+    print(f"wrote checkpoint_step2.pt ({os.path.getsize(path)} bytes)")
+
+
 GENERATORS = {
     "field_query": gen_field_query,
     "sampler": gen_sampler,
     "render_det": lambda R: gen_render(R, perturb=False, name="render_det.npz"),
     "render_perturb": lambda R: gen_render(R, perturb=True, name="render_perturb.npz"),
+    # the throughput workload's sampler: 64 stratified + 4 x 16 upsampled = 128 samples per ray
+    "render_128": lambda R: gen_render(R, perturb=True, name="render_128.npz", n_samples=64, n_importance=64,
+                                       grid_res=20, hash_log2=7, n_rays=24),
+    "train_step": gen_train_step,
     "regularizers": gen_regularizers,
     "upsample": gen_upsample,
     "hash": gen_hash,
@@ -264,9 +387,12 @@ GENERATORS = {
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference/Code")
+    ap.add_argument("--reference", default=os.environ.get("VOXNEUS_REFERENCE"),
+                    help="the reference's Code/ directory (default: $VOXNEUS_REFERENCE)")
     ap.add_argument("--only", nargs="*", choices=sorted(GENERATORS), help="fixtures to write (default: all)")
     args = ap.parse_args()
+    if not args.reference:
+        ap.error("give --reference <reference>/Code or set VOXNEUS_REFERENCE")
     torch.set_num_threads(1)
     R = _import_reference(args.reference)
     for name in args.only or list(GENERATORS):

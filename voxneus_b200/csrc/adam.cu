@@ -4,7 +4,8 @@
 //   SparseGridAdam, training/optimizer.py:32-116):
 //       step_size = lr * sqrt(1 - b2^t) / (1 - b1^t);  p -= step_size * m / (sqrt(v) + eps)
 //     masked: elements whose gradient is exactly 0 keep p, m and v.
-//   torch formula (torch.optim.Adam, the network optimizer of training/optimizer.py:119-154):
+//   torch formula (torch.optim.Adam, the network optimizer of training/optimizer.py:119-154, and
+//   SparseGridAdam's vectorised torch path, optimizer.py:86-113, when masked):
 //       p -= (lr / (1 - b1^t)) * m / (sqrt(v) / sqrt(1 - b2^t) + eps)
 //     (the division by sqrt(1 - b2^t) is a multiplication by its reciprocal, formed on the host)
 //   both with m = b1 m + (1 - b1) g, v = b2 v + (1 - b2) g^2.
@@ -151,14 +152,17 @@ unsigned adam_blocks(int64_t total) {
 }
 
 int launch_adam(const AdamArgs& a, bool masked, bool torch_formula, int64_t total, cudaStream_t stream) {
-  if (torch_formula)
+  if (torch_formula && masked)
+    k_adam<true, true><<<adam_blocks<true, true>(total), 256, 0, stream>>>(a);
+  else if (torch_formula)
     k_adam<false, true><<<adam_blocks<false, true>(total), 256, 0, stream>>>(a);
   else if (masked)
     k_adam<true, false><<<adam_blocks<true, false>(total), 256, 0, stream>>>(a);
   else
     k_adam<false, false><<<adam_blocks<false, false>(total), 256, 0, stream>>>(a);
   count_launches(1);
-  return check_launch(torch_formula ? "adam_torch" : (masked ? "masked_adam_upd" : "adam_upd"));
+  return check_launch(torch_formula ? (masked ? "masked_adam_torch" : "adam_torch")
+                                    : (masked ? "masked_adam_upd" : "adam_upd"));
 }
 
 // The reference's step size, evaluated on the host in float (adam_upd_kernel.cu:50).
@@ -229,7 +233,13 @@ int vx_masked_adam_upd_dev(float* param, const float* grad, float* exp_avg, floa
   return adam_reference(true, param, grad, exp_avg, exp_avg_sq, n, 0, beta1, beta2, 0.0f, eps, stream, step_size);
 }
 
-int vx_adam_torch(const vx_adam_segment* segs, int n_segs, float beta1, float beta2, float eps, void* stream) {
+}  // extern "C"
+
+namespace vx {
+namespace {
+
+int adam_torch_segments(const vx_adam_segment* segs, int n_segs, float beta1, float beta2, float eps, bool masked,
+                        void* stream) {
   VX_REQUIRE(n_segs >= 0, "n_segs < 0");
   if (n_segs == 0) return VX_OK;
   VX_REQUIRE(segs, "null pointer");
@@ -264,9 +274,22 @@ int vx_adam_torch(const vx_adam_segment* segs, int n_segs, float beta1, float be
       total += in.n;
     }
     if (a.n_segs == 0) continue;
-    if (int st = launch_adam(a, false, true, total, (cudaStream_t)stream)) return st;
+    if (int st = launch_adam(a, masked, true, total, (cudaStream_t)stream)) return st;
   }
   return VX_OK;
+}
+
+}  // namespace
+}  // namespace vx
+
+extern "C" {
+
+int vx_adam_torch(const vx_adam_segment* segs, int n_segs, float beta1, float beta2, float eps, void* stream) {
+  return adam_torch_segments(segs, n_segs, beta1, beta2, eps, false, stream);
+}
+
+int vx_masked_adam_torch(const vx_adam_segment* segs, int n_segs, float beta1, float beta2, float eps, void* stream) {
+  return adam_torch_segments(segs, n_segs, beta1, beta2, eps, true, stream);
 }
 
 }  // extern "C"

@@ -1027,8 +1027,10 @@ def grid_upsample(grid: torch.Tensor, new_res) -> torch.Tensor:
     return dst
 
 
-def adam_torch(segments, beta1: float, beta2: float, eps: float):
-    """torch.optim.Adam's update over [(param, grad, exp_avg, exp_avg_sq, step, lr), ...] in place.
+def adam_torch(segments, beta1: float, beta2: float, eps: float, masked: bool = False):
+    """torch.optim.Adam's update over [(param, grad, exp_avg, exp_avg_sq, step, lr), ...] in place;
+    masked=True skips the elements whose gradient is exactly 0 (SparseGridAdam's torch path,
+    training/optimizer.py:86-113).
 
     A segment may carry two more items, (..., scalars, flag): a float32 device tensor of 3 values
     {lr / (1 - b1^t), 1 / sqrt(1 - b2^t), the step size used when flag is nonzero} read by the
@@ -1056,8 +1058,8 @@ def adam_torch(segments, beta1: float, beta2: float, eps: float):
             check_tensor(flag, "flag", dtype=torch.int32, device=dev)
         arr[k] = L.AdamSegment(p.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), p.numel(), int(step), float(lr),
                                None if scal is None else scal.data_ptr(), None if flag is None else flag.data_ptr())
-    call("vx_adam_torch", ctypes.cast(arr, ctypes.c_void_p), len(segments), float(beta1), float(beta2), float(eps),
-         stream_ptr(dev))
+    call("vx_masked_adam_torch" if masked else "vx_adam_torch", ctypes.cast(arr, ctypes.c_void_p), len(segments),
+         float(beta1), float(beta2), float(eps), stream_ptr(dev))
 
 
 def adam_update(param, grad, exp_avg, exp_avg_sq, step, beta1, beta2, lr, eps, masked):

@@ -99,13 +99,28 @@ class SceneStore:
             p.requires_grad_(False)
         self.scenes[name] = model
 
-    def load_checkpoint(self, name: str, path: str, **model_kw) -> None:
-        """Load a reference checkpoint (training/checkpoint.py:11-33 layout) into the store."""
-        ck = torch.load(path, map_location="cpu", weights_only=False)
-        res = ck.get("grid_res", None)
-        m = VoxNeuS(grid_res=res if res is not None else 96, **model_kw)
-        m.load_state_dict(ck["model_state"])
+    def load_checkpoint(self, name: str, path: str, **model_kw) -> int:
+        """Load a checkpoint written by the reference's save_checkpoint (training/checkpoint.py:11-33:
+        {"step", "model_state", "grid_res", ...}) into the store; returns its step.
+
+        The grid resolution comes from "grid_res" (else the grid's shape), the hash table's levels,
+        features and size, the MLP width and the occupancy resolution from the state_dict's shapes
+        (the reference's load_checkpoint rescales a model built at another resolution,
+        :48-54; here the model is built at the saved one). Only tensors and plain containers are
+        unpickled (weights_only). model_kw overrides the inferred constructor arguments."""
+        ck = torch.load(path, map_location="cpu", weights_only=True)
+        sd = ck["model_state"]
+        emb = sd["radiance_hash.encoder.embeddings"]
+        res = ck.get("grid_res") or list(sd["sdf_grid.grid"].shape[-3:])
+        kw = dict(grid_res=[int(r) for r in res], hash_n_levels=int(emb.shape[0]), hash_n_features=int(emb.shape[2]),
+                  hash_log2_size=int(emb.shape[1]).bit_length() - 1,
+                  mlp_hidden_dim=int(sd["radiance_mlp.net.0.weight"].shape[0]),
+                  occupancy_res=int(sd["occupancy_grid.occupancy_mask"].shape[0]))
+        kw.update(model_kw)
+        m = VoxNeuS(**kw)
+        m.load_state_dict(sd)
         self.add(name, m)
+        return int(ck.get("step", 0))
 
     def bytes(self) -> int:
         return sum(sum(t.numel() * t.element_size() for t in m.state_dict().values()) for m in self.scenes.values())

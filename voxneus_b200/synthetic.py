@@ -117,3 +117,25 @@ def bumpy_spheres_grid(res: int, n_spheres: int = 32, seed: int = 0, device="cpu
             fi = dc - r * (1.0 + a * torch.exp(-dp / (s * s)))
             f[i0:i0 + 64] = torch.minimum(f[i0:i0 + 64], fi)
     return f.reshape(1, 1, res, res, res)
+
+
+def throughput_scene(res: int, device, seed: int = 0, hash_log2_size: int = 19, occupancy_res: int = 128):
+    """The training-throughput scene: a (res/2)^3 union of 8 random spheres/boxes + N(0, 0.005),
+    upsampled on the device to res^3 by trilinear interpolation (geometry/upsample.py:12-39), a
+    16-level hash table of 2^hash_log2_size entries initialised U(-1e-2, 1e-2), default MLP and s.
+
+    Returns (model, milliseconds of the upsampling launch)."""
+    from .models import VoxNeuS
+
+    torch.manual_seed(seed)
+    m = VoxNeuS(grid_res=res // 2, hash_log2_size=hash_log2_size, occupancy_res=occupancy_res).to(device)
+    with torch.no_grad():
+        m.sdf_grid.grid.copy_(shapes_grid(res // 2, seed=seed).to(device))
+        m.radiance_hash.encoder.embeddings.uniform_(-1e-2, 1e-2)
+    t0 = torch.cuda.Event(enable_timing=True)
+    t1 = torch.cuda.Event(enable_timing=True)
+    t0.record()
+    m.sdf_grid.scale_volume_grid(res)
+    t1.record()
+    torch.cuda.synchronize()
+    return m, t0.elapsed_time(t1)

@@ -40,12 +40,23 @@ def amplify_s_gradient(variance_param: torch.nn.Parameter, k: float = 5.0) -> bo
 
 
 class SparseGridAdam(Optimizer):
-    """Adam that skips grad == 0 voxels (training/optimizer.py:15-116) on the masked Adam kernel."""
+    """Adam that skips grad == 0 voxels (training/optimizer.py:15-116) on the masked Adam kernel.
 
-    def __init__(self, params, lr: float = 1e-1, betas=(0.9, 0.999), eps: float = 1e-8, weight_decay: float = 0.0):
+    formula="torch" (default): the reference optimizer's vectorised PyTorch path
+    (optimizer.py:86-113), p -= lr/(1-b1^t) * m / (sqrt(v)/sqrt(1-b2^t) + eps).
+    formula="cuda": the update of the reference's extension kernel, which its optimizer
+    dispatches to when that extension is built (optimizer.py:64-77, adam_upd_kernel.cu),
+    p -= lr*sqrt(1-b2^t)/(1-b1^t) * m / (sqrt(v) + eps). They differ only in where eps enters.
+    """
+
+    def __init__(self, params, lr: float = 1e-1, betas=(0.9, 0.999), eps: float = 1e-8, weight_decay: float = 0.0,
+                 formula: str = "torch"):
         if weight_decay != 0.0:
             raise ValueError("weight decay is not on the masked kernel path")
+        if formula not in ("torch", "cuda"):
+            raise ValueError(f"formula must be 'torch' or 'cuda', not {formula!r}")
         super().__init__(params, dict(lr=lr, betas=betas, eps=eps, weight_decay=weight_decay))
+        self.formula = formula
         self.last_updated_count = 0
 
     @torch.no_grad()
@@ -61,8 +72,12 @@ class SparseGridAdam(Optimizer):
                     st["exp_avg"] = torch.zeros_like(p)
                     st["exp_avg_sq"] = torch.zeros_like(p)
                 st["step"] += 1
-                ops.adam_update(p, p.grad.contiguous(), st["exp_avg"], st["exp_avg_sq"], st["step"], b1, b2,
-                                group["lr"], group["eps"], masked=True)
+                if self.formula == "torch":
+                    ops.adam_torch([(p, p.grad.contiguous(), st["exp_avg"], st["exp_avg_sq"], st["step"], group["lr"])],
+                                   b1, b2, group["eps"], masked=True)
+                else:
+                    ops.adam_update(p, p.grad.contiguous(), st["exp_avg"], st["exp_avg_sq"], st["step"], b1, b2,
+                                    group["lr"], group["eps"], masked=True)
         return None
 
 
@@ -107,9 +122,11 @@ class FusedAdam(Optimizer):
         return loss
 
 
-def create_optimizer(model: VoxNeuS, lr_sdf=0.1, lr_hash=1e-2, lr_mlp=1e-3, lr_variance=1e-2, use_sparse_sdf=True):
+def create_optimizer(model: VoxNeuS, lr_sdf=0.1, lr_hash=1e-2, lr_mlp=1e-3, lr_variance=1e-2, use_sparse_sdf=True,
+                     grid_formula: str = "torch"):
     """Optimizer suite (training/optimizer.py:119-154)."""
-    sdf_opt = (SparseGridAdam([model.sdf_grid.grid], lr=lr_sdf, betas=(0.9, 0.99)) if use_sparse_sdf
+    sdf_opt = (SparseGridAdam([model.sdf_grid.grid], lr=lr_sdf, betas=(0.9, 0.99), formula=grid_formula)
+               if use_sparse_sdf
                else torch.optim.Adam([model.sdf_grid.grid], lr=lr_sdf, betas=(0.9, 0.99)))
     net_opt = FusedAdam([{"params": model.radiance_hash.parameters(), "lr": lr_hash},
                          {"params": model.radiance_mlp.parameters(), "lr": lr_mlp},
@@ -126,7 +143,8 @@ class FusedTrainer:
                  amplify_k: float = 5.0, s_warmup_steps: int = 5000, total_steps: int = 40000, lr_sdf: float = 0.1,
                  lr_hash: float = 0.01, lr_mlp: float = 0.001, lr_variance: float = 0.0005, up_sample_steps: int = 4,
                  huber_delta: float = 0.1, optimize: bool = True, exchange=None,
-                 occupancy_update_interval: int = 16, occupancy_seed: int = 0, cuda_graph: bool = False):
+                 occupancy_update_interval: int = 16, occupancy_seed: int = 0, cuda_graph: bool = False,
+                 grid_adam: str = "torch"):
         self.model = model
         self.exchange = exchange  # dataparallel.GradExchange for world_size > 1
         self.sampler = sampler or RaySampler(64, 64, perturb=True)
@@ -139,7 +157,8 @@ class FusedTrainer:
         self.huber_delta = huber_delta
         self.lr_hash, self.lr_mlp, self.lr_variance = lr_hash, lr_mlp, lr_variance
         self.optimize = optimize
-        self.optimizers = create_optimizer(model, lr_sdf, lr_hash, lr_mlp, lr_variance) if optimize else {}
+        self.optimizers = (create_optimizer(model, lr_sdf, lr_hash, lr_mlp, lr_variance, grid_formula=grid_adam)
+                           if optimize else {})
         dev = model.sdf_grid.grid.device
         self.res = [int(r) for r in model.sdf_grid.res]
         eps = model.sdf_grid.voxel_size_host()
@@ -269,8 +288,9 @@ class _StepGraph:
     """One captured training step (render .. optimizer) of a FusedTrainer.
 
     Static inputs: rays_o, rays_d, target buffers (the caller's tensors are copied in) and a device
-    table of optimizer scalars: [grid step size, then per network parameter {lr/(1-b1^t),
-    1/sqrt(1-b2^t), step size when amplified}]. The sampler's uniforms come from torch's default
+    table of optimizer scalars, three per parameter, the grid's first: {step size (lr/(1-b1^t) for
+    the torch formula, lr*sqrt(1-b2^t)/(1-b1^t) for the extension's), 1/sqrt(1-b2^t), step size when
+    the s gradient was amplified (the variance only)}. The sampler's uniforms come from torch's default
     CUDA generator inside the graph (torch advances its offset per replay, so the draws are the
     eager step's). Gradients live in the graph's memory pool and are rewritten by every replay.
     """
@@ -293,7 +313,7 @@ class _StepGraph:
                 for p in grp["params"]:
                     if not opt.state.get(p):
                         raise RuntimeError("graph mode starts after an eager step has created the optimizer state")
-        n = 1 + 3 * len(self.net_params)
+        n = 3 + 3 * len(self.net_params)
         self.scalars = torch.zeros(n, device=dev)
         self.host = torch.zeros(_SCALAR_SLOTS, n).pin_memory()
         self.slot_events = [None] * _SCALAR_SLOTS
@@ -315,8 +335,12 @@ class _StepGraph:
         grid = m.sdf_grid.grid
         b1, b2 = self.grid_opt.param_groups[0]["betas"]
         st = self.grid_opt.state[grid]
-        ops.masked_adam_update_dev(grid, grid.grad, st["exp_avg"], st["exp_avg_sq"], self.scalars[0:1], b1, b2,
-                                   self.grid_opt.param_groups[0]["eps"])
+        if self.grid_opt.formula == "torch":
+            ops.adam_torch([(grid, grid.grad, st["exp_avg"], st["exp_avg_sq"], 0, 0.0, self.scalars[0:3], None)],
+                           b1, b2, self.grid_opt.param_groups[0]["eps"], masked=True)
+        else:
+            ops.masked_adam_update_dev(grid, grid.grad, st["exp_avg"], st["exp_avg_sq"], self.scalars[0:1], b1, b2,
+                                       self.grid_opt.param_groups[0]["eps"])
         flag = self.tr.amp_flag if self.amplify else None
         batches: Dict[tuple, list] = {}
         for k, (gi, p) in enumerate(self.net_params):
@@ -326,7 +350,7 @@ class _StepGraph:
             st = self.net_opt.state[p]
             b1, b2 = grp["betas"]
             batches.setdefault((float(b1), float(b2), float(grp["eps"])), []).append(
-                (p, p.grad, st["exp_avg"], st["exp_avg_sq"], 0, 0.0, self.scalars[1 + 3 * k:4 + 3 * k],
+                (p, p.grad, st["exp_avg"], st["exp_avg_sq"], 0, 0.0, self.scalars[3 + 3 * k:6 + 3 * k],
                  flag if gi == 2 else None))
         for (b1, b2, eps), segs in batches.items():
             ops.adam_torch(segs, b1, b2, eps)
@@ -340,7 +364,11 @@ class _StepGraph:
         st = self.grid_opt.state[tr.model.sdf_grid.grid]
         st["step"] += 1
         b1, b2 = grp["betas"]
-        row[0] = ops.adam_reference_step_size(st["step"], b1, b2, grp["lr"])
+        if self.grid_opt.formula == "torch":
+            ss, inv = ops.adam_torch_step_scalars(st["step"], b1, b2, grp["lr"])
+            row[0:3] = [ss, inv, ss]
+        else:
+            row[0] = ops.adam_reference_step_size(st["step"], b1, b2, grp["lr"])
         f = tr.lr_factor(step)
         lrs = [tr.lr_hash * f, tr.lr_mlp * f, tr.lr_variance]
         for gi, lr in enumerate(lrs):
@@ -354,7 +382,7 @@ class _StepGraph:
             amp = ss
             if gi == 2 and self.amplify:
                 amp = ops.adam_torch_step_scalars(st["step"], b1, b2, tr.lr_variance * tr.amplify_k)[0]
-            row[1 + 3 * k:4 + 3 * k] = [ss, inv, amp]
+            row[3 + 3 * k:6 + 3 * k] = [ss, inv, amp]
         return torch.tensor(row, dtype=torch.float32)
 
     def run(self, rays_o, rays_d, target, step: int) -> None:
