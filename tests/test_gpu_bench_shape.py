@@ -1,0 +1,310 @@
+"""Parity at the benchmarked configuration (the training-throughput workload's shapes).
+
+A 256^3 grid (trilinear from a 128^3 union of 8 shapes), a 16-level hash table of 2^19 entries,
+64 stratified + 4 x 16 perturbed upsampled samples per ray (128 per ray), V_R in the 1.2 relax
+sphere and the |f| < 3 voxel narrow band, eikonal 0.1 and curvature 5e-4, both optimizers, the
+cosine learning-rate rule and the k = 5 s amplification live (s_warmup_steps = 0), an occupancy
+mask after one EMA refresh. 1024 rays from the 64-camera rig (the CPU oracle's step takes a few
+seconds); the sampler's uniforms are the ones the GPU step drew from torch's CUDA generator,
+redrawn from the saved generator state and handed to the oracle.
+
+The sampler (S0-S7) is conditioned badly at the 1e-5 level on a few percent of rays: its
+occupancy lookups, inside-sphere tests and flat CDF stretches are discontinuous, so a one-ulp
+difference in an SDF value or a sigmoid can move a later sample by up to an interval. The float32
+oracle itself differs from a float64 run of the same algorithm on ~14% of these rays, and from a
+float32 run whose grid moved by one ulp on ~1%. The sampler test therefore checks: the stratified
+samples bit for bit; each upsampling step started from the GPU's own previous samples (teacher
+forced), with at most 0.5% of rays outside 1e-5; and end to end, that the GPU is no further from
+the float64 oracle than the float32 oracle is, and differs from the float32 oracle on at most a
+quarter as many rays as the float32 oracle differs from float64.
+
+Each training step is compared with the oracle's step (training/trainer.py:166-393) on the GPU
+sampler's samples of that step and from the GPU's own parameters and Adam state (teacher
+forcing), so every step is checked on identical inputs:
+* losses within 1e-5 relative; |V_R| and the V_R linear indices bit-exact; the amplification flag;
+* every gradient within 1e-4 of its largest magnitude;
+* the Adam moments within 1e-4 of the scale the gradient gives them ((1-b1) max|g|, (1-b2) max|g|^2);
+* the parameters after the optimizers equal to the Adam update (the oracle's formulas in float64)
+  of the GPU's state and gradients, to float32 rounding. Together with the gradient check this pins
+  the step: Adam divides by sqrt(v), so where |g| is near eps a gradient difference inside the
+  tolerance moves the update by up to the learning rate, and the parameters are not compared with
+  the oracle's own post-step parameters elementwise (their largest difference is printed).
+"""
+
+import math
+
+import pytest
+import torch
+
+from oracle import reference_path as O
+
+pytestmark = pytest.mark.gpu
+
+DEV = torch.device("cuda", 0)
+RES = 256
+N_RAYS = 1024
+NS, NI, STEPS = 64, 64, 4
+VAL_TOL = 1e-5
+GRAD_TOL = 1e-4
+
+
+def _close(a, b, tol, what, scale=None):
+    a = torch.as_tensor(a).detach().double().cpu()
+    b = torch.as_tensor(b).detach().double().cpu()
+    assert a.shape == b.shape, (what, a.shape, b.shape)
+    if scale is None:
+        scale = float(b.abs().max()) if b.numel() else 0.0
+    err = (a - b).abs()
+    bad = err > tol * (b.abs() + max(scale, 1e-30))
+    assert not bool(bad.any()), f"{what}: max err {float(err.max()):.3e} vs scale {scale:.3e} ({int(bad.sum())} bad)"
+    return float(err.max()) / max(scale, 1e-30)
+
+
+def _bad_rays(a, b, tol=VAL_TOL):
+    """Rays (rows) with any sample outside tol * (|b| + max|b|)."""
+    a, b = a.double().cpu(), b.double().cpu()
+    return ((a - b).abs() > tol * (b.abs() + float(b.abs().max()))).any(dim=1)
+
+
+@pytest.fixture(scope="module")
+def scene_state():
+    """The throughput scene after one occupancy refresh, as CPU tensors (rebuilt per test)."""
+    from voxneus_b200 import _lib, synthetic
+
+    _lib.load()
+    m, _ = synthetic.throughput_scene(RES, DEV, seed=0)
+    torch.manual_seed(5)
+    m.update_occupancy_grid(subsample_ratio=0.25)
+    sd = {k: v.detach().cpu().clone() for k, v in m.state_dict().items()}
+    pool = synthetic.RayPool(seed=100)
+    batches = []
+    g = torch.Generator().manual_seed(101)
+    for _ in range(3):
+        o, d = pool.sample(N_RAYS)
+        batches.append((o, d, torch.rand(N_RAYS, 3, generator=g)))
+    del m
+    torch.cuda.empty_cache()
+    return sd, batches
+
+
+def _model(sd):
+    from voxneus_b200.models import VoxNeuS
+
+    m = VoxNeuS(grid_res=RES, occupancy_res=128).to(DEV)
+    m.load_state_dict({k: v.to(DEV) for k, v in sd.items()})
+    return m
+
+
+def _params(m):
+    l0, l1 = m.radiance_mlp.net[0], m.radiance_mlp.net[2]
+    return {"grid": m.sdf_grid.grid, "variance": m.variance_net.variance,
+            "embeddings": m.radiance_hash.encoder.embeddings, "w0": l0.weight, "b0": l0.bias, "w1": l1.weight,
+            "b1": l1.bias}
+
+
+_SD_NAMES = {"grid": "sdf_grid.grid", "variance": "variance_net.variance",
+             "embeddings": "radiance_hash.encoder.embeddings", "w0": "radiance_mlp.net.0.weight",
+             "b0": "radiance_mlp.net.0.bias", "w1": "radiance_mlp.net.2.weight", "b1": "radiance_mlp.net.2.bias"}
+
+
+def _oracle_scene(sd, dtype=torch.float32):
+    p = {k: sd[v].to(dtype).clone().requires_grad_(True) for k, v in _SD_NAMES.items()}
+    return O.OracleScene(p["grid"], p["variance"], p["embeddings"], p["w0"], p["b0"], p["w1"], p["b1"],
+                         occupancy=sd["occupancy_grid.occupancy_mask"].clone())
+
+
+def _gpu_samples(m, o, d, t_rand, u, k):
+    """The GPU sampler's z after k upsampling steps of 16 (the first k steps of the 4-step run)."""
+    from voxneus_b200 import ops
+
+    lo, hi = m.sdf_grid.bounds()
+    occ = m.occupancy_grid
+    z, _, _ = ops.sample_multistep(m.sdf_grid.grid.detach(), lo, hi, o.to(DEV), d.to(DEV), None, None, NS, 16 * k, k,
+                                   True, t_rand, u[:k].contiguous() if k else None, occ.occupancy_mask, *occ.bounds(),
+                                   want_z=True)
+    return z.cpu()
+
+
+def test_sampler_128_samples_matches_oracle(scene_state):
+    """S0-S7 at 64 + 4 x 16: the multi-tile merge of up to 112 + 16 samples and the scans over
+    more than 32 entries (rendering/sampler.py:127-204, 243-320)."""
+    sd, batches = scene_state
+    m = _model(sd)
+    o, d, _ = batches[0]
+    gen = torch.Generator(device=DEV).manual_seed(7)
+    t_rand, u = m.draw_sampler_randoms(N_RAYS, NS, NI, STEPS, DEV, generator=gen)
+    tr, uc = t_rand.cpu(), u.cpu()
+    sc = _oracle_scene(sd)
+    near, far = O.near_far_from_sphere(o, d)
+    zs = [_gpu_samples(m, o, d, t_rand, u, k) for k in range(STEPS + 1)]
+    # S1 + S0: near/far and the stratified samples, bit for bit
+    z0, _ = O.sample_stratified(near, far, NS, True, t_rand=tr)
+    assert torch.equal(zs[0], z0), f"stratified z differs, max {float((zs[0] - z0).abs().max()):.3e}"
+    # S4-S6 per step, from the GPU's previous samples
+    for k in range(1, STEPS + 1):
+        zin = zs[k - 1]
+        pts = o[:, None, :] + d[:, None, :] * zin[..., None]
+        sdf = sc.sdf_fn(pts.reshape(-1, 3)).reshape(zin.shape)
+        nz = O.up_sample(o, d, zin, sdf, NI // STEPS, 64.0 * 2 ** (k - 1), det=False, occ_fn=sc.occ_fn, u=uc[k - 1])
+        zr, _ = O.cat_z_vals(o, d, zin, nz, sdf, sc.sdf_fn, last=True)
+        bad = _bad_rays(zs[k], zr)
+        exact = float((zs[k] == zr).all(dim=1).float().mean())
+        print(f"upsampling step {k} (teacher forced): {int(bad.sum())} of {N_RAYS} rays outside 1e-5, "
+              f"{exact:.3f} of rays bit-exact, max |dz| {float((zs[k] - zr).abs().max()):.2e}")
+        assert int(bad.sum()) <= N_RAYS // 200, f"step {k}: {int(bad.sum())} rays outside 1e-5"
+        assert zs[k].shape == (N_RAYS, NS + 16 * k) and bool((zs[k][:, 1:] >= zs[k][:, :-1]).all())
+    # end to end, against the float32 and the float64 oracle
+    z32, d32, m32 = O.sample_multistep_sdf(o, d, near, far, sc.sdf_fn, NS, NI, STEPS, True, sc.occ_fn, t_rand=tr,
+                                           us=[uc[k] for k in range(STEPS)])
+    sc64 = _oracle_scene(sd, torch.float64)
+    n64, f64 = O.near_far_from_sphere(o.double(), d.double())
+    z64, _, _ = O.sample_multistep_sdf(o.double(), d.double(), n64, f64, sc64.sdf_fn, NS, NI, STEPS, True,
+                                       sc64.occ_fn, t_rand=tr.double(), us=[uc[k].double() for k in range(STEPS)])
+    n_gpu32 = int(_bad_rays(zs[STEPS], z32).sum())
+    n_gpu64 = int(_bad_rays(zs[STEPS], z64).sum())
+    n_3264 = int(_bad_rays(z32, z64).sum())
+    print(f"end to end, rays outside 1e-5: GPU vs float32 oracle {n_gpu32}, GPU vs float64 oracle {n_gpu64}, "
+          f"float32 vs float64 oracle {n_3264} (of {N_RAYS})")
+    assert n_gpu64 <= n_3264 + N_RAYS // 100
+    assert n_gpu32 <= max(n_3264 // 4, N_RAYS // 100)
+    # the full call's dists and midpoints follow from its z (S7)
+    from voxneus_b200 import ops
+
+    lo, hi = m.sdf_grid.bounds()
+    occ = m.occupancy_grid
+    z, dists, mid = ops.sample_multistep(m.sdf_grid.grid.detach(), lo, hi, o.to(DEV), d.to(DEV), None, None, NS, NI,
+                                         STEPS, True, t_rand, u, occ.occupancy_mask, *occ.bounds(), want_z=True)
+    assert torch.equal(z.cpu(), zs[STEPS])
+    zc = z.cpu()
+    dr = torch.cat([zc[:, 1:] - zc[:, :-1], zc[:, -1:] - zc[:, -2:-1]], dim=-1)
+    assert torch.equal(dists.cpu(), dr) and torch.equal(mid.cpu(), zc + dr * 0.5)
+
+
+def _adam64(p, g, m, v, t, lr, b1, b2, eps, masked):
+    """The torch formula in float64 (training/optimizer.py:86-113; torch.optim.Adam)."""
+    p, g, m, v = (x.detach().double().cpu() for x in (p, g, m, v))
+    m2 = b1 * m + (1 - b1) * g
+    v2 = b2 * v + (1 - b2) * g * g
+    p2 = p - (lr / (1 - b1 ** t)) * m2 / (v2.sqrt() / math.sqrt(1 - b2 ** t) + eps)
+    if masked:
+        keep = g == 0
+        m2 = torch.where(keep, m, m2)
+        v2 = torch.where(keep, v, v2)
+        p2 = torch.where(keep, p, p2)
+    return p2, m2, v2
+
+
+def _gpu_state(tr, m):
+    """GPU parameters and Adam state (CPU copies), keyed like the oracle's parameters."""
+    out = {}
+    opts = tr.optimizers
+    for k, p in _params(m).items():
+        opt = opts["sdf_optimizer"] if k == "grid" else opts["net_optimizer"]
+        st = opt.state.get(p, {})
+        out[k] = (p.detach().cpu().clone(), int(st["step"]) if st else 0,
+                  st["exp_avg"].cpu().clone() if st else torch.zeros_like(p, device="cpu"),
+                  st["exp_avg_sq"].cpu().clone() if st else torch.zeros_like(p, device="cpu"))
+    return out
+
+
+def _teacher_force(sc, state):
+    """Give the oracle scene the GPU's parameters and Adam state."""
+    for k, (p, t, mo, vo) in state.items():
+        with torch.no_grad():
+            getattr(sc, k).copy_(p)
+    if not hasattr(sc, "_opt_state"):
+        sc._opt_state = {}
+        sc._net_opt = torch.optim.Adam([{"params": [sc.embeddings], "lr": 0.01},
+                                        {"params": [sc.w0, sc.b0, sc.w1, sc.b1], "lr": 0.001},
+                                        {"params": [sc.variance], "lr": 0.0005}], betas=(0.9, 0.999), eps=1e-8)
+    p, t, mo, vo = state["grid"]
+    if t:
+        sc._opt_state.update({"step": t, "exp_avg": mo.clone(), "exp_avg_sq": vo.clone()})
+    for k in ("embeddings", "w0", "b0", "w1", "b1", "variance"):
+        p, t, mo, vo = state[k]
+        if t:
+            sc._net_opt.state[getattr(sc, k)] = {"step": torch.tensor(float(t)), "exp_avg": mo.clone(),
+                                                 "exp_avg_sq": vo.clone()}
+
+
+@pytest.mark.parametrize("graph", [False, True], ids=["eager", "graph"])
+def test_training_step_matches_oracle(scene_state, graph):
+    """FusedTrainer.step at the benchmarked shape against OracleScene.train_step, three steps
+    (the third one a CUDA graph replay in graph mode), the s amplification live."""
+    from voxneus_b200 import ops
+    from voxneus_b200.rendering import RaySampler
+    from voxneus_b200.training import FusedTrainer
+
+    sd, batches = scene_state
+    m = _model(sd)
+    tr = FusedTrainer(m, RaySampler(NS, NI, perturb=True), band_voxels=3.0, s_warmup_steps=0,
+                      occupancy_update_interval=0, cuda_graph=graph)
+    sc = _oracle_scene(sd)
+    lo, hi = m.sdf_grid.bounds()
+    res = [RES] * 3
+    torch.manual_seed(23)
+    seen_amp = set()
+    for k in range(3):
+        o, d, t = batches[k]
+        before = _gpu_state(tr, m)
+        _teacher_force(sc, before)
+        grid_before = m.sdf_grid.grid.detach().clone()
+        rng = torch.cuda.get_rng_state()
+        out = tr.step(o.to(DEV), d.to(DEV), t.to(DEV), step=k)
+        torch.cuda.synchronize()
+        after_rng = torch.cuda.get_rng_state()
+        torch.cuda.set_rng_state(rng)
+        t_rand, u = m.draw_sampler_randoms(N_RAYS, NS, NI, STEPS, DEV)
+        torch.cuda.set_rng_state(after_rng)
+        if graph and k == 2:
+            assert tr.graph() is not None, "the third step should be a graph replay"
+        # the samples this step trained on: the same sampler launch on the pre-step grid
+        occ = m.occupancy_grid
+        z, _, _ = ops.sample_multistep(grid_before, lo, hi, o.to(DEV), d.to(DEV), None, None, NS, NI, STEPS, True,
+                                       t_rand, u, occ.occupancy_mask, *occ.bounds(), want_z=True)
+        ref = sc.train_step(o, d, t, w_eik=0.1, w_curv=5e-4, band_voxels=3.0, amplify_k=5.0, optimize=True, step=k,
+                            total_steps=tr.total_steps, s_warmup_steps=0, grid_adam="torch", z_vals=z.cpu())
+        tag = f"step {k} ({'graph' if graph and k == 2 else 'eager'})"
+        assert int(out["n_active"]) == ref["n_active"], (tag, int(out["n_active"]), ref["n_active"])
+        counts = ops.vr_count(tr.bitmap, grid_before, res, lo, hi, tr.relax_radius, tr.band,
+                              filtered=ops.new_filtered(res, DEV))
+        n = int(ops.final_count(counts, tr.relax_radius, tr.band))
+        _, lin = ops.vr_compact(tr.bitmap, grid_before, res, lo, hi, tr.relax_radius, tr.band, counts, n)
+        assert torch.equal(lin.cpu(), ref["vr_linear"]), f"{tag}: V_R differs"
+        _close(out["loss_rgb"], ref["loss_rgb"], VAL_TOL, f"{tag} loss_rgb")
+        _close(out["loss_eik"], ref["loss_eik"], VAL_TOL, f"{tag} loss_eik")
+        _close(out["loss_curv"], ref["loss_curv"], VAL_TOL, f"{tag} loss_curv")
+        amp = bool(tr.amp_flag.item())
+        assert amp == ref["amplified"], (tag, amp, ref["amplified"])
+        seen_amp.add(amp)
+        gp = _params(m)
+        errs = {}
+        for name, p in gp.items():
+            errs[name] = _close(p.grad, ref["grads"][name], GRAD_TOL, f"{tag} grad {name}")
+        # optimizers: the GPU's update equals Adam (float64) of its own state and gradients
+        f = tr.lr_factor(k)
+        lrs = {"grid": tr.optimizers["sdf_optimizer"].param_groups[0]["lr"], "embeddings": tr.lr_hash * f,
+               "variance": tr.lr_variance * (tr.amplify_k if amp else 1.0)}
+        div = {}
+        for name, p in gp.items():
+            p0, t0, m0, v0 = before[name]
+            b1, b2 = (0.9, 0.99) if name == "grid" else (0.9, 0.999)
+            lr = lrs.get(name, tr.lr_mlp * f)
+            pe, me, ve = _adam64(p0, p.grad, m0, v0, t0 + 1, lr, b1, b2, 1e-8, masked=(name == "grid"))
+            opt = tr.optimizers["sdf_optimizer" if name == "grid" else "net_optimizer"]
+            st = opt.state[p]
+            assert int(st["step"]) == t0 + 1
+            _close(st["exp_avg"], me, 1e-6, f"{tag} exp_avg {name} (Adam of the GPU gradient)")
+            _close(st["exp_avg_sq"], ve, 1e-5, f"{tag} exp_avg_sq {name} (Adam of the GPU gradient)")
+            _close(p, pe, 1e-6, f"{tag} param {name} (Adam of the GPU gradient)",
+                   scale=float(p0.abs().max()) + lr)
+            gmax = float(ref["grads"][name].abs().max())
+            ost = sc._opt_state if name == "grid" else sc._net_opt.state[getattr(sc, name)]
+            _close(st["exp_avg"], ost["exp_avg"], GRAD_TOL, f"{tag} exp_avg {name} vs oracle", scale=(1 - b1) * gmax)
+            _close(st["exp_avg_sq"], ost["exp_avg_sq"], 3 * GRAD_TOL, f"{tag} exp_avg_sq {name} vs oracle",
+                   scale=(1 - b2) * gmax * gmax)
+            div[name] = float((p.detach().cpu().double() - getattr(sc, name).detach().double()).abs().max()) / lr
+        print(f"{tag}: loss {float(out['loss_rgb']):.6f} |V_R| {int(out['n_active'])} amplified {amp}; "
+              f"grad errs {', '.join(f'{k} {v:.1e}' for k, v in errs.items())}; "
+              f"max |p - p_oracle| / lr {', '.join(f'{k} {v:.1e}' for k, v in div.items())}")
+    print(f"amplification seen: {sorted(seen_amp)}")

@@ -145,7 +145,8 @@ def test_lattice_query():
 def _scene_from(g):
     from voxneus_b200.models import VoxNeuS
 
-    m = VoxNeuS(grid_res=24, hash_n_levels=16, hash_log2_size=8, occupancy_res=8).to(DEV)
+    m = VoxNeuS(grid_res=list(g["grid"].shape[-3:]), hash_n_levels=16,
+                hash_log2_size=int(g["embeddings"].shape[1]).bit_length() - 1, occupancy_res=8).to(DEV)
     sd = m.state_dict()
     sd["sdf_grid.grid"] = to(g["grid"])
     sd["variance_net.variance"] = to(g["variance"])
@@ -234,13 +235,16 @@ def test_up_sample_single_step():
 # ------------------------------------------------------------------ render forward / backward
 
 
-@pytest.mark.parametrize("name,perturb", [("render_det.npz", False), ("render_perturb.npz", True)])
-def test_render_matches_golden(golden, name, perturb):
+@pytest.mark.parametrize("name,perturb,ns", [("render_det.npz", False, 16), ("render_perturb.npz", True, 16),
+                                             ("render_128.npz", True, 64)])
+def test_render_matches_golden(golden, name, perturb, ns):
+    """The whole render and its gradients against the reference's; render_128 is the throughput
+    workload's sampler (64 stratified + 4 x 16 upsampled samples per ray)."""
     from voxneus_b200.rendering import RaySampler, compute_huber_color_loss
 
     g = golden(name)
     m = _scene_from(g)
-    s = RaySampler(16, 16, perturb=perturb)
+    s = RaySampler(ns, ns, perturb=perturb)
     randoms = (to(g["t_rand"]), to(g["us"])) if perturb else None
     out = m.render(to(g["rays_o"]), to(g["rays_d"]), s, to(g["near"]), to(g["far"]), randoms=randoms)
     for k in ("rgb", "depth", "normal", "opacity", "weights", "alpha", "transmittance", "pts", "sdf_samples",
@@ -257,7 +261,7 @@ def test_render_matches_golden(golden, name, perturb):
         assert_close(v, g[k + "_grad"], GRAD_TOL, k + " grad")
     from voxneus_b200.regularization import extract_active_vertices
 
-    verts, lin = extract_active_vertices(out["corner_indices"], [24, 24, 24])
+    verts, lin = extract_active_vertices(out["corner_indices"], list(g["grid"].shape[-3:]))
     assert torch.equal(verts.cpu(), g["vr_verts"]) and torch.equal(lin.cpu(), g["vr_linear"])
 
 

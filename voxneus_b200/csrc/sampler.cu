@@ -9,14 +9,16 @@
 
 namespace vx {
 
-// rendering/rays.py:102-128
+// rendering/rays.py:102-128. Every product and sum rounded separately, in the order of the
+// reference's float32 ops (torch.sum over the 3 components adds them left to right), so near
+// and far are bit-identical to it (no fused multiply-adds).
 __device__ __forceinline__ void near_far(float ox, float oy, float oz, float dx, float dy, float dz, float radius,
                                          float& nearv, float& farv) {
-  const float a = dx * dx + dy * dy + dz * dz;
-  const float b = 2.0f * (ox * dx + oy * dy + oz * dz);
-  const float mid = 0.5f * (-b) / a;
-  nearv = fmaxf(mid - radius, 0.05f);
-  farv = fmaxf(mid + radius, nearv + 0.1f);
+  const float a = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+  const float b = __fmul_rn(2.0f, __fadd_rn(__fadd_rn(__fmul_rn(ox, dx), __fmul_rn(oy, dy)), __fmul_rn(oz, dz)));
+  const float mid = __fdiv_rn(__fmul_rn(0.5f, -b), a);
+  nearv = fmaxf(__fsub_rn(mid, radius), 0.05f);
+  farv = fmaxf(__fadd_rn(mid, radius), __fadd_rn(nearv, 0.1f));
 }
 
 struct WarpArrays {

@@ -333,7 +333,7 @@ class VoxNeuS(nn.Module):
     def render(self, rays_o, rays_d, sampler, near=None, far=None, background_rgb=None, cos_anneal_ratio=0.0,
                use_iter_cos_annealing=False, active_levels=None, up_sample_steps=4, sphere_radius=1.0,
                *, randoms=None, vr_bitmap=None, extras=True, amplify_k=0.0, amp_flag=None,
-               fused_mlp=True) -> Dict[str, torch.Tensor]:
+               fused_mlp=True, z_vals=None) -> Dict[str, torch.Tensor]:
         """Fused render (models/voxneus.py:169-260).
 
         near/far None: computed from the unit sphere inside the sampler kernel. randoms:
@@ -341,6 +341,9 @@ class VoxNeuS(nn.Module):
         vr_bitmap: V_R bitmap receiving every sample's Eq.7 corners. extras: also return pts,
         sdf_samples, corner_indices, grad_samples, normal_samples like the reference; with
         extras=False the per-sample weights, alpha and transmittance are not written (None).
+        z_vals: (N_rays, S) sorted sample depths to render instead of running the sampler (as the
+        reference sampler returns them); their dists and midpoints are formed as in
+        rendering/sampler.py:197-202.
         """
         dev = rays_o.device
         o = rays_o.contiguous()
@@ -350,13 +353,20 @@ class VoxNeuS(nn.Module):
         ns, ni = sampler.n_samples, sampler.n_importance
         perturb = sampler.perturb
         t_rand = u = None
-        if perturb:
-            t_rand, u = randoms if randoms is not None else self.draw_sampler_randoms(nr, ns, ni, up_sample_steps, dev)
-        occ = self.occupancy_grid
-        with torch.no_grad():
-            _, dists, mid = ops.sample_multistep(self.sdf_grid.grid.detach(), lo, hi, o, d, near, far, ns, ni,
-                                                 up_sample_steps, perturb, t_rand, u, occ.occupancy_mask,
-                                                 *occ.bounds(), want_z=False)
+        if z_vals is not None:
+            with torch.no_grad():
+                z = z_vals.detach().to(torch.float32).contiguous()
+                dists = torch.cat([z[:, 1:] - z[:, :-1], z[:, -1:] - z[:, -2:-1]], dim=-1)
+                mid = z + dists * 0.5
+        else:
+            if perturb:
+                t_rand, u = (randoms if randoms is not None
+                             else self.draw_sampler_randoms(nr, ns, ni, up_sample_steps, dev))
+            occ = self.occupancy_grid
+            with torch.no_grad():
+                _, dists, mid = ops.sample_multistep(self.sdf_grid.grid.detach(), lo, hi, o, d, near, far, ns, ni,
+                                                     up_sample_steps, perturb, t_rand, u, occ.occupancy_mask,
+                                                     *occ.bounds(), want_z=False)
         handoff = ops.NormalGradHandoff(torch.is_grad_enabled()) if fused_mlp else None
         sdf, normal, gsamp = ops.RenderGeometryFn.apply(self.sdf_grid.grid, o, d, mid, lo, hi, vr_bitmap, extras,
                                                         handoff)

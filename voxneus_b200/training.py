@@ -187,16 +187,18 @@ class FusedTrainer:
         """Cosine decay to 0.05 of the base LR (training/trainer.py:378-385)."""
         return (math.cos(math.pi * step / max(self.total_steps, 1)) + 1.0) * 0.5 * (1.0 - 0.05) + 0.05
 
-    def step(self, rays_o, rays_d, target, step: int = 0, randoms=None) -> Dict[str, torch.Tensor]:
+    def step(self, rays_o, rays_d, target, step: int = 0, randoms=None, z_vals=None) -> Dict[str, torch.Tensor]:
         """One training step. rays_o, rays_d, target may be device tensors or (pinned) host tensors,
         which are copied to the device on the current stream: in graph mode straight into the
         graph's input buffers. In graph mode the returned tensors are the graph's outputs,
-        overwritten by the next step (copy them to keep them)."""
+        overwritten by the next step (copy them to keep them). randoms: the sampler's (t_rand, u)
+        uniforms; z_vals: sample depths to train on instead of running the sampler (VoxNeuS.render);
+        either makes the step eager."""
         m = self.model
         if [int(r) for r in m.sdf_grid.res] != self.res:
             raise RuntimeError("grid resolution changed; build a new FusedTrainer after scale_volume_grid")
         graphable = (self.cuda_graph and self.exchange is None and self.optimize and randoms is None
-                     and torch.is_grad_enabled())
+                     and z_vals is None and torch.is_grad_enabled())
         if graphable and self._eager_steps >= GRAPH_WARMUP_STEPS:
             return self._graph_step(rays_o, rays_d, target, step)
         self._graphs.clear()  # an eager step owns fresh gradients; replays would no longer see them
@@ -204,13 +206,15 @@ class FusedTrainer:
         dev = self.bitmap.device
         rays_o, rays_d, target = (t if t.device == dev else t.to(dev, non_blocking=True)
                                   for t in (rays_o, rays_d, target))
-        return self._eager_step(rays_o, rays_d, target, step, randoms)
+        if z_vals is not None and z_vals.device != dev:
+            z_vals = z_vals.to(dev, non_blocking=True)
+        return self._eager_step(rays_o, rays_d, target, step, randoms, z_vals)
 
     def _refresh_occupancy(self, step: int) -> None:
         if self.occupancy_update_interval > 0 and step % self.occupancy_update_interval == 0:
             self.model.update_occupancy_grid(subsample_ratio=0.25, generator=self.occ_generator)
 
-    def _render_backward_regularize(self, rays_o, rays_d, target, amp_k: float, randoms=None):
+    def _render_backward_regularize(self, rays_o, rays_d, target, amp_k: float, randoms=None, z_vals=None):
         """Render, loss, backward, gradient exchange, V_R and the regularizer stencil."""
         m = self.model
         self.bitmap.zero_()
@@ -218,7 +222,7 @@ class FusedTrainer:
         ex = self.exchange
         out = m.render(rays_o, rays_d, self.sampler, None, None, up_sample_steps=self.up_sample_steps,
                        sphere_radius=1.0, randoms=randoms, vr_bitmap=self.bitmap, extras=False,
-                       amplify_k=0.0 if ex is not None else amp_k, amp_flag=self.amp_flag)
+                       amplify_k=0.0 if ex is not None else amp_k, amp_flag=self.amp_flag, z_vals=z_vals)
         loss = compute_huber_color_loss(out["rgb"], target, self.huber_delta)
         loss.backward()
         if ex is not None:
@@ -237,7 +241,7 @@ class FusedTrainer:
         return {"loss_rgb": loss.detach(), "loss_eik": self.reg_losses[0], "loss_curv": self.reg_losses[1],
                 "n_active": self.n_active, "rgb": out["rgb"].detach()}
 
-    def _eager_step(self, rays_o, rays_d, target, step: int, randoms) -> Dict[str, torch.Tensor]:
+    def _eager_step(self, rays_o, rays_d, target, step: int, randoms, z_vals=None) -> Dict[str, torch.Tensor]:
         m = self.model
         for opt in self.optimizers.values():
             opt.zero_grad(set_to_none=True)
@@ -246,7 +250,7 @@ class FusedTrainer:
                 p.grad = None
         self._refresh_occupancy(step)
         amp_k = self.amplify_k if step >= self.s_warmup_steps else 0.0
-        res = self._render_backward_regularize(rays_o, rays_d, target, amp_k, randoms)
+        res = self._render_backward_regularize(rays_o, rays_d, target, amp_k, randoms, z_vals)
         if self.optimize:
             lr_factor = self.lr_factor(step)
             net = self.optimizers["net_optimizer"]
