@@ -25,7 +25,8 @@ forcing), so every step is checked on identical inputs:
 * every gradient within 1e-4 of its largest magnitude;
 * the Adam moments within 1e-4 of the scale the gradient gives them ((1-b1) max|g|, (1-b2) max|g|^2);
 * the parameters after the optimizers equal to the Adam update (the oracle's formulas in float64)
-  of the GPU's state and gradients, to float32 rounding. Together with the gradient check this pins
+  of the GPU's state and gradients, to float32 rounding (1e-6 of the parameter's scale plus the
+  largest update, lr / (1 - b1^t)). Together with the gradient check this pins
   the step: Adam divides by sqrt(v), so where |g| is near eps a gradient difference inside the
   tolerance moves the update by up to the learning rate, and the parameters are not compared with
   the oracle's own post-step parameters elementwise (their largest difference is printed).
@@ -297,7 +298,7 @@ def test_training_step_matches_oracle(scene_state, graph):
             _close(st["exp_avg"], me, 1e-6, f"{tag} exp_avg {name} (Adam of the GPU gradient)")
             _close(st["exp_avg_sq"], ve, 1e-5, f"{tag} exp_avg_sq {name} (Adam of the GPU gradient)")
             _close(p, pe, 1e-6, f"{tag} param {name} (Adam of the GPU gradient)",
-                   scale=float(p0.abs().max()) + lr)
+                   scale=float(p0.abs().max()) + lr / (1 - b1 ** (t0 + 1)))
             gmax = float(ref["grads"][name].abs().max())
             ost = sc._opt_state if name == "grid" else sc._net_opt.state[getattr(sc, name)]
             _close(st["exp_avg"], ost["exp_avg"], GRAD_TOL, f"{tag} exp_avg {name} vs oracle", scale=(1 - b1) * gmax)

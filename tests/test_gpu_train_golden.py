@@ -14,7 +14,8 @@ reference's sampler produced (FusedTrainer.step(z_vals=...)); the fused sampler 
 those samples separately, on the same uniforms. Tolerances: losses 1e-5 relative, gradients 1e-4
 of their largest magnitude, the flag exact, the Adam moments 1e-4 of the scale the gradient gives
 them, and the parameters equal to Adam (float64, the reference optimizer's torch formulas) of the
-fused step's own state and gradients to float32 rounding (Adam divides by sqrt(v), so where |g| is
+fused step's own state and gradients to float32 rounding (1e-6 of the parameter's scale plus the
+largest update, lr / (1 - b1^t); Adam divides by sqrt(v), so where |g| is
 near eps an allowed gradient difference moves the update by up to the learning rate).
 """
 
@@ -152,7 +153,8 @@ def test_step_matches_reference_trainer(fx, k):
         pe, me, ve = _adam64(p0, p.grad, m0, v0, t0 + 1, lr, b1, b2, 1e-8, masked=grid)
         _close(st["exp_avg"], me, 1e-6, f"step {k} exp_avg {n} (Adam of the fused gradient)")
         _close(st["exp_avg_sq"], ve, 1e-5, f"step {k} exp_avg_sq {n} (Adam of the fused gradient)")
-        _close(p, pe, 1e-6, f"step {k} param {n} (Adam of the fused gradient)", scale=float(p0.abs().max()) + lr)
+        _close(p, pe, 1e-6, f"step {k} param {n} (Adam of the fused gradient)",
+               scale=float(p0.abs().max()) + lr / (1 - b1 ** (t0 + 1)))
         gmax = float(g_ref.abs().max())
         _close(st["exp_avg"], fx[f"step{k}/exp_avg/{n}"], GRAD_TOL, f"step {k} exp_avg {n}", scale=(1 - b1) * gmax)
         _close(st["exp_avg_sq"], fx[f"step{k}/exp_avg_sq/{n}"], 3 * GRAD_TOL, f"step {k} exp_avg_sq {n}",
