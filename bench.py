@@ -35,6 +35,9 @@ METRIC = "fwd+bwd rays/s at 256^3 grid (fused training step)"
 UNIT = "rays/s"
 N_SAMPLES, N_IMPORTANCE, STEPS_UP = 64, 64, 4
 CPU_SAMPLE_RAYS = 1024
+# the timed steps are numbered from here: past the trainer's s_warmup_steps (5000), so the k = 5
+# s-gradient amplification and its variance learning-rate rule are live, as in 35k of the 40k steps
+STEP0 = 5000
 
 
 def parse():
@@ -58,6 +61,7 @@ def config(args, world):
             "grid": args.res, "rays_per_gpu": args.rays, "global_rays": args.rays * world,
             "samples_per_ray": N_SAMPLES + N_IMPORTANCE, "hash": "16 levels x 2 x 2^19", "mlp": "51-64-3",
             "band_voxels": 3, "w_eik": 0.1, "w_curv": 5e-4, "perturb": True, "optimizer_step": True,
+            "steps_from": STEP0, "s_amplification": "live (k = 5, steps past the 5000-step warm-up)",
             "parallelism": f"dp{world}" if world > 1 else "single",
             "l2": "working set (grid, hash table, grads, Adam state > 700 MiB) exceeds the 126 MB L2"}
 
@@ -268,6 +272,133 @@ def cpu_baseline(args, n_rays=CPU_SAMPLE_RAYS, steps=3):
                       f"(oracle: the reference's torch ops restated, float32 on CPU)"}, med
 
 
+def _oracle_scene_of(m, device, grad=True):
+    """The oracle's scene holding copies of a fused model's parameters and occupancy mask."""
+    from oracle import reference_path as O
+
+    l0, l1 = m.radiance_mlp.net[0], m.radiance_mlp.net[2]
+    ps = [t.detach().to(device).clone().requires_grad_(grad) for t in (
+        m.sdf_grid.grid, m.variance_net.variance, m.radiance_hash.encoder.embeddings, l0.weight, l0.bias, l1.weight,
+        l1.bias)]
+    return O.OracleScene(*ps, occupancy=m.occupancy_grid.occupancy_mask.detach().to(device).clone())
+
+
+def parity_leg(m, batch, dev, n_rays=CPU_SAMPLE_RAYS):
+    """The timed step's numbers against the oracle's (the checker, on the host cores) on a
+    n_rays slice of a timed batch, with the fused model's parameters after the timed steps:
+    one fused training step without the optimizers (s amplification live) and the oracle's step
+    on the samples the fused sampler drew, plus the end-to-end sampler agreement."""
+    from oracle import reference_path as O
+    from voxneus_b200 import ops
+    from voxneus_b200.rendering import RaySampler
+    from voxneus_b200.training import FusedTrainer
+
+    o, d, t = (x[:n_rays].contiguous() for x in batch)
+    tr = FusedTrainer(m, RaySampler(N_SAMPLES, N_IMPORTANCE, perturb=True), band_voxels=3.0, s_warmup_steps=0,
+                      optimize=False, occupancy_update_interval=0)
+    gen = torch.Generator(device=dev).manual_seed(1234)
+    t_rand, u = m.draw_sampler_randoms(n_rays, N_SAMPLES, N_IMPORTANCE, STEPS_UP, dev, generator=gen)
+    out = tr.step(o, d, t, step=0, randoms=(t_rand, u))
+    lo, hi = m.sdf_grid.bounds()
+    occ = m.occupancy_grid
+    z, _, _ = ops.sample_multistep(m.sdf_grid.grid.detach(), lo, hi, o, d, None, None, N_SAMPLES, N_IMPORTANCE,
+                                   STEPS_UP, True, t_rand, u, occ.occupancy_mask, *occ.bounds(), want_z=True)
+    torch.cuda.synchronize()
+    sc = _oracle_scene_of(m, "cpu")
+    oc, dc, tc = o.cpu(), d.cpu(), t.cpu()
+    ref = sc.train_step(oc, dc, tc, band_voxels=3.0, amplify_k=5.0, step=0, s_warmup_steps=0, z_vals=z.cpu())
+    near, far = O.near_far_from_sphere(oc, dc)
+    zr, _, _ = O.sample_multistep_sdf(oc, dc, near, far, sc.sdf_fn, N_SAMPLES, N_IMPORTANCE, STEPS_UP, True, sc.occ_fn,
+                                      t_rand=t_rand.cpu(), us=[u[k].cpu() for k in range(STEPS_UP)])
+    zd, zrd = z.cpu().double(), zr.double()
+    outside = int(((zd - zrd).abs() > 1e-5 * (zrd.abs() + float(zrd.abs().max()))).any(dim=1).sum())
+
+    def rel(a, b):
+        a, b = torch.as_tensor(a).detach().double().cpu(), torch.as_tensor(b).detach().double().cpu()
+        return float((a - b).abs().max() / max(float(b.abs().max()), 1e-30))
+
+    l0, l1 = m.radiance_mlp.net[0], m.radiance_mlp.net[2]
+    gp = {"grid": m.sdf_grid.grid, "variance": m.variance_net.variance,
+          "embeddings": m.radiance_hash.encoder.embeddings, "w0": l0.weight, "b0": l0.bias, "w1": l1.weight,
+          "b1": l1.bias}
+    grads = {k: rel(p.grad, ref["grads"][k]) for k, p in gp.items()}
+    losses = {k: rel(out[k], ref[k]) for k in ("loss_rgb", "loss_eik", "loss_curv")}
+    amp = bool(tr.amp_flag.item())
+    res = {"rays": n_rays, "loss_rel_err": losses, "grad_rel_err": grads,
+           "n_active": [int(out["n_active"]), int(ref["n_active"])], "amplified": [amp, bool(ref["amplified"])],
+           "sampler_rays_outside_1e-5": outside,
+           "tolerance": {"loss": 1e-5, "grad": 1e-4, "n_active": "equal", "amplified": "equal"},
+           "how": "one training step without the optimizers on a slice of a timed batch, parameters after the "
+                  "timed steps; the oracle (float32, host cores) steps on the fused sampler's samples; "
+                  "sampler_rays_outside_1e-5 compares the two samplers end to end on the same uniforms"}
+    res["within_tolerance"] = (max(losses.values()) <= 1e-5 and max(grads.values()) <= 1e-4
+                               and res["n_active"][0] == res["n_active"][1] and amp == bool(ref["amplified"]))
+    for p in gp.values():
+        p.grad = None
+    return res
+
+
+def same_gpu_torch_leg(m, batches, dev, steps=3, step0=0):
+    """The reference's plain PyTorch training step on this GPU: its torch ops as the oracle
+    restates them (the golden-pinned checker, here the baseline being timed, never the product)
+    on a copy of the fused scene, the full workload (all rays of a batch, 64 + 4 x 16 samples, the
+    narrow band, both optimizers), FP32 with TF32 off. Median of `steps` CUDA-event-timed steps
+    after one warm-up step."""
+    from oracle import reference_path as O
+
+    prev = torch.backends.cuda.matmul.allow_tf32, torch.backends.cudnn.allow_tf32
+    torch.backends.cuda.matmul.allow_tf32 = False
+    torch.backends.cudnn.allow_tf32 = False
+    try:
+        sc = _oracle_scene_of(m, dev)
+        n = batches[0][0].shape[0]
+        times = []
+        for i in range(steps + 1):
+            o, d, t = batches[i % len(batches)]
+            t_rand, us = O.sampler_draws(n, N_SAMPLES, N_IMPORTANCE, STEPS_UP, True, device=dev)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            torch.cuda.synchronize()
+            e0.record()
+            sc.train_step(o, d, t, band_voxels=3.0, amplify_k=5.0, optimize=True, step=step0 + i, n_samples=N_SAMPLES,
+                          n_importance=N_IMPORTANCE, steps=STEPS_UP, perturb=True, t_rand=t_rand, us=us)
+            e1.record()
+            torch.cuda.synchronize()
+            if i > 0:
+                times.append(e0.elapsed_time(e1))
+        ms = statistics.median(times)
+        del sc
+        torch.cuda.empty_cache()
+    finally:
+        torch.backends.cuda.matmul.allow_tf32, torch.backends.cudnn.allow_tf32 = prev
+    return {"value": n / (ms / 1e3), "unit": UNIT, "ms_per_step": ms, "steps": steps, "warmup": 1,
+            "what": "the reference's plain PyTorch training step (its torch ops as the oracle restates them, "
+                    "golden-pinned) on this GPU at the full workload, FP32, TF32 off"}
+
+
+# Render forward per ray, the unit of the "render kernel" target: sampler 4,444 B (112 SDF queries x
+# 32 B + occupancy + z) + Eq.7 stencil 128 x 128 B + appearance hand-off 128 x 36 B + ray I/O 64 B
+RENDER_BYTES_PER_RAY = 4444 + 16384 + 4608 + 64
+HASH_FWD_BYTES_PER_RAY = (N_SAMPLES + N_IMPORTANCE) * 16 * 8 * 2 * 4  # 16 levels x 8 corners x 2 features
+RENDER_KERNELS = ("vx_sample_multistep", "vx_render_geometry_forward", "vx_composite_forward")
+
+
+def render_roofline(per_kernel, n_rays, peak, peak_kind):
+    """Render-forward bytes per ray over the summed device time of its kernels (one step's
+    attribution pass), without and with the appearance forward (hash gathers + MLP)."""
+    ms = sum(per_kernel.get(k, 0.0) for k in RENDER_KERNELS)
+    out = {"bound": "hbm", "kernels": list(RENDER_KERNELS), "bytes_per_ray": RENDER_BYTES_PER_RAY, "ms": ms,
+           "peak": peak, "peak_kind": peak_kind, "unit": "GB/s"}
+    if ms > 0:
+        out["achieved"] = n_rays * RENDER_BYTES_PER_RAY / (ms / 1e3) / 1e9
+        out["frac"] = out["achieved"] / peak
+    app = per_kernel.get("vx_appearance_mlp_forward")
+    if app and ms > 0:
+        b = RENDER_BYTES_PER_RAY + HASH_FWD_BYTES_PER_RAY
+        ach = n_rays * b / ((ms + app) / 1e3) / 1e9
+        out["with_appearance"] = {"bytes_per_ray": b, "ms": ms + app, "achieved": ach, "frac": ach / peak}
+    return out
+
+
 def run_reference(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -335,7 +466,7 @@ def run_fused(args):
         elif graph_mode and dom_timer is not None and tr.graph() is None:
             _lib.set_timer(dom_timer)  # this step captures the graph
         o, d, t = batches[i % nb]
-        tr.step(o, d, t, step=i)
+        tr.step(o, d, t, step=STEP0 + i)
         _lib.set_timer(None)
         if i == attr_at:
             torch.cuda.synchronize()
@@ -368,7 +499,7 @@ def run_fused(args):
             o, d, t = batches[i % nb]
             if graph_timer is not None:
                 graph_timer.arm(i)
-            tr.step(o, d, t, step=n_warm + i)
+            tr.step(o, d, t, step=STEP0 + n_warm + i)
         _lib.set_timer(None)
         ev1.record()
         torch.cuda.synchronize()
@@ -433,7 +564,7 @@ def run_fused(args):
     t0 = time.perf_counter()
     for i in range(args.steps):
         ho, hd, ht = host[i % nb]
-        out = tr.step(ho, hd, ht, step=n_warm + args.steps + i)
+        out = tr.step(ho, hd, ht, step=STEP0 + n_warm + args.steps + i)
         slots[i % 2:i % 2 + 1].copy_(out["loss_rgb"].reshape(1), non_blocking=True)
         evts[i % 2].record()
         if i >= 1:
@@ -460,9 +591,13 @@ def run_fused(args):
 
             dist.destroy_process_group()
         return
-    cb = None
+    cb = parity = same_gpu = None
     if world == 1 and not args.no_cpu_baseline:
         cb, _ = cpu_baseline(args)
+        parity = parity_leg(m, batches[0], dev)
+        same_gpu = same_gpu_torch_leg(m, batches, dev, step0=STEP0 + n_warm)
+        same_gpu["fused_over_same_gpu_torch"] = value / same_gpu["value"]
+        same_gpu["fused_e2e_over_same_gpu_torch"] = e2e["value"] / same_gpu["value"]
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, rays and targets)",
@@ -472,7 +607,9 @@ def run_fused(args):
             "roofline": roofline, "roofline_hbm": roofline_hbm,
             "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(per_kernel.items(), key=lambda x: -x[1])},
             "mlp_tensor": mlp_tensor(per_kernel, args.rays * (N_SAMPLES + N_IMPORTANCE)),
-            "grid_upsample_128_to_256_ms": up_ms, "clocks": clk.summary(), "cpu_baseline": cb}
+            "roofline_render": render_roofline(per_kernel, args.rays, peak, peak_kind),
+            "grid_upsample_128_to_256_ms": up_ms, "clocks": clk.summary(), "cpu_baseline": cb,
+            "same_gpu_torch": same_gpu, "parity": parity}
     print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
