@@ -291,6 +291,15 @@ int vx_mlp_partial_floats(void);
  * a CUDA error. Synchronises the device (diagnostic only). No counterpart in the reference. */
 int vx_tensor_core_timeouts(void);
 
+/* The wait policy of this thread's later MLP launches (vx_radiance_mlp_forward/backward,
+ * vx_appearance_mlp_forward[_chunked]): at most wait_polls mbarrier polls per wait on the tensor
+ * core (negative: the default, 2^22), and a device int (status, may be NULL) that every block
+ * which gave up on a wait increments atomically, so the caller can test its step's status without
+ * a synchronisation. A block that gives up lets the copy or MMA it waited for finish (bounded)
+ * before it frees tensor memory and exits; its outputs are invalid. The arguments are baked into
+ * launches captured in a CUDA graph. Thread-local; no counterpart in the reference. */
+int vx_tc_guard(int* status, int64_t wait_polls);
+
 /* Adjoint of vx_radiance_mlp_forward (recomputes the hidden layer): d_colors (n,3) -> d_hash (n,32)
  * (gradient of input columns 0..31), d_normal (n,3) (columns 48..50), and the weight gradients
  * dW0, db0, dW1, db1 (written, not accumulated; summed over blocks in a fixed order).

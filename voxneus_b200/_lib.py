@@ -84,6 +84,7 @@ _PROTOS = {
     "vx_occupancy_workspace": [I64],
     "vx_adam_torch": [P, I32, F32, F32, F32, P],
     "vx_masked_adam_torch": [P, I32, F32, F32, F32, P],
+    "vx_tc_guard": [P, I64],
     "vx_adam_reference_step_size": [I32, F32, F32, F32],
     "vx_adam_torch_step_scalars": [I64, F32, F32, F32, HF3],
     "vx_masked_adam_upd_dev": [P, P, P, P, I64, P, F32, F32, F32, P],

@@ -33,12 +33,31 @@ constexpr int NH = 64;   // hidden units
 constexpr int NO = 3;    // colours
 constexpr int TM = 128;  // samples per tile (TMEM lanes)
 constexpr int WG = NH * KP + NO * NH + NH + NO;  // per-block weight-gradient partial size
-constexpr uint32_t kWaitLimit = 1u << 22;       // mbarrier polls before a tile gives up
+constexpr uint32_t kWaitLimit = 1u << 22;       // default mbarrier polls before a tile gives up
+// After a block gives up on a wait, the copy or MMA it waited for may still be running: the
+// block waits for it (at most this many polls) before it frees tensor memory and exits, so no
+// asynchronous write lands in memory that another block owns next.
+constexpr uint32_t kDrainLimit = 1u << 22;
 
 constexpr uint32_t kXBytes = 16 * 16 * 128;  // one tf32 part of X (or DZ)
 constexpr uint32_t kWBytes = 16 * 16 * 128;  // W0 (or W0^T) as [hi; lo]
 
 __device__ int g_tc_timeouts = 0;
+
+// The wait policy of the MMA kernels: polls per mbarrier wait, and a caller's device status word
+// (nullable) that every block which gave up increments.
+struct TcGuard {
+  int* status;
+  uint32_t limit;
+};
+
+// The guard the host launchers of this thread pass (vx_tc_guard).
+thread_local TcGuard t_guard{nullptr, kWaitLimit};
+
+__device__ __forceinline__ void report_timeout(int* status) {
+  atomicAdd(&g_tc_timeouts, 1);
+  if (status) atomicAdd(status, 1);
+}
 
 struct MlpW {
   const float* W0;  // (64, 51)
@@ -196,7 +215,8 @@ __device__ __forceinline__ void colour_partial(const float z[32], int hh, const 
 // hidden columns 32*(w/4)..; the two column halves meet in shared memory.
 template <bool kHashIn, bool kRowsOut>
 __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* __restrict__ X, int64_t ldx, int xvec,
-                                                       int64_t P, MlpW w, float* __restrict__ colors) {
+                                                       int64_t P, MlpW w, float* __restrict__ colors,
+                                                       TcGuard g) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* XH = smem;
   uint8_t* XL = XH + kXBytes;
@@ -298,12 +318,15 @@ __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* 
     }
     if (!kHashIn && t + gridDim.x < ntiles)  // next tile's rows fly during the MMA and the epilogue
       load_row_chunks(X, ldx, xvec != 0, P, (t + gridDim.x) * TM, tid & (TM - 1), tid >> 7, pre);
-    const bool ok = tc::mbar_wait(bar, phase, kWaitLimit);
-    phase ^= 1u;
+    const bool ok = tc::mbar_wait(bar, phase, g.limit);
     if (__syncthreads_or(!ok)) {
-      if (tid == 0) atomicAdd(&g_tc_timeouts, 1);
+      if (tid == 0) {
+        if (!ok) tc::mbar_wait(bar, phase, kDrainLimit);  // this tile's Z MMA, before TMEM is freed
+        report_timeout(g.status);
+      }
       break;
     }
+    phase ^= 1u;
     tc::fence_after_sync();
     float z[32];
     tmem_ld_sum32(tbase + ((uint32_t)(32 * q) << 16) + 32 * hh, z);
@@ -351,7 +374,7 @@ __device__ __forceinline__ void slot_sync(int slot) {
 }
 
 __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restrict__ X, int64_t P, MlpW w,
-                                                         float* __restrict__ colors) {
+                                                         float* __restrict__ colors, TcGuard g) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* W2 = smem;
   float* B0 = reinterpret_cast<float*>(W2 + kWBytes);
@@ -404,6 +427,7 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
     tc::bulk_g2s(ROWS, X + m0 * KP, bytes, bar_rows);
   };
   bool rows_pending = false;  // slot thread 0: a rows copy is in flight
+  bool mma_pending = false;   // slot thread 0: its wait on the slot's MMA gave up
   if (stid == 0 && t0 < ntiles) {
     fetch_rows(t0);
     rows_pending = true;
@@ -412,12 +436,15 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
   for (int64_t t = t0; t < ntiles; t += tstride) {
     const int64_t m0 = t * TM;
     const bool valid = m0 + m < P;
-    const bool got = tc::mbar_wait(bar_rows, rphase, kWaitLimit);
-    rphase ^= 1u;
-    if (!got) s_fail[slot] = 1;
+    const bool got = tc::mbar_wait(bar_rows, rphase, g.limit);
+    if (got) {  // on a give-up, rphase still names the copy in flight
+      rphase ^= 1u;
+      if (stid == 0) rows_pending = false;
+    } else {
+      s_fail[slot] = 1;
+    }
     slot_sync(slot);
     if (s_fail[slot]) break;
-    if (stid == 0) rows_pending = false;
     {  // rows -> X_hi (TMEM) and X_lo (sample rows); column 51 zero (the padding column may hold anything)
       const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * (KP * 4));
       const int c0 = hh ? 7 : 0;
@@ -463,9 +490,13 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
         rows_pending = true;
       }
     }
-    const bool ok = tc::mbar_wait(bar, phase, kWaitLimit);
-    phase ^= 1u;
-    if (!ok) s_fail[slot] = 1;
+    const bool ok = tc::mbar_wait(bar, phase, g.limit);
+    if (ok) {
+      phase ^= 1u;
+    } else {
+      s_fail[slot] = 1;
+      if (stid == 0) mma_pending = true;
+    }
     slot_sync(slot);
     if (s_fail[slot]) break;
     tc::fence_after_sync();
@@ -488,9 +519,11 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
     }
   }
   if (stid == 0 && s_fail[slot]) {
-    atomicAdd(&g_tc_timeouts, 1);
-    // a rows copy may still be landing in this slot's buffer: wait for it (bounded) before leaving
-    if (rows_pending) tc::mbar_wait(bar_rows, rphase, kWaitLimit);
+    // this slot's MMA and a rows copy into its buffer may still run: let them finish (bounded)
+    // before TMEM and shared memory are released
+    if (mma_pending) tc::mbar_wait(bar, phase, kDrainLimit);
+    if (rows_pending) tc::mbar_wait(bar_rows, rphase, kDrainLimit);
+    report_timeout(g.status);
   }
   tc::fence_before_sync();
   __syncthreads();
@@ -537,7 +570,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
                                                       MlpW w, const float* __restrict__ d_out,
                                                       const float* __restrict__ y_in,
                                                       float* __restrict__ d_hash, float* __restrict__ d_normal,
-                                                      float* __restrict__ partials) {
+                                                      float* __restrict__ partials, TcGuard g) {
   extern __shared__ __align__(1024) uint8_t smem[];
   uint8_t* W2 = smem;
   uint8_t* WT2 = W2 + kWBytes;
@@ -609,6 +642,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   }
   float sb[NO] = {0.0f, 0.0f, 0.0f};
   bool first_w = true, failed = false;
+  bool mma_pending = false;  // thread 0: its wait on an MMA gave up
   uint32_t phase = 0;
   float4 pre[7];  // !kBulk: this tile's row chunks, loaded during the previous tile
   float dy[NO], yv[NO] = {0.0f, 0.0f, 0.0f};  // dL/dcolour and (y_in) the forward's colour of this sample
@@ -625,13 +659,15 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     const int64_t m0 = t * TM;
     const bool valid = m0 + m < P;
     if (kBulk) {
-      const bool got = tc::mbar_wait(bar_rows, rphase, kWaitLimit);
-      rphase ^= 1u;
+      const bool got = tc::mbar_wait(bar_rows, rphase, g.limit);
+      if (got) {  // on a give-up, rphase still names the copy in flight
+        rphase ^= 1u;
+        if (tid == 0) rows_pending = false;
+      }
       if (__syncthreads_or(!got)) {
         failed = true;
         break;
       }
-      if (tid == 0) rows_pending = false;
     }
     // rows -> X_hi (TMEM, sample lanes), X_lo (sample rows, R1) and X^T (feature rows); column 51
     // = 1 on real rows (db0)
@@ -689,8 +725,11 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
         rows_pending = true;
       }
     }
-    bool ok = tc::mbar_wait(bar, phase, kWaitLimit);
-    phase ^= 1u;
+    bool ok = tc::mbar_wait(bar, phase, g.limit);
+    if (ok)
+      phase ^= 1u;
+    else if (tid == 0)
+      mma_pending = true;
     if (__syncthreads_or(!ok)) {
       failed = true;
       break;
@@ -778,8 +817,11 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
       issue_split_ts(tbase, tbase + kAhiCol, r1 + kXBytes, wt2, 8);
       tc::commit(bar);
     }
-    ok = tc::mbar_wait(bar, phase, kWaitLimit);
-    phase ^= 1u;
+    ok = tc::mbar_wait(bar, phase, g.limit);
+    if (ok)
+      phase ^= 1u;
+    else if (tid == 0)
+      mma_pending = true;
     if (__syncthreads_or(!ok)) {
       failed = true;
       break;
@@ -841,8 +883,11 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
         d_normal[(m0 + m) * 3 + 2] = v[2];
       }
     }
-    ok = tc::mbar_wait(bar, phase, kWaitLimit);  // R1 and X^T are rewritten by the next tile
-    phase ^= 1u;
+    ok = tc::mbar_wait(bar, phase, g.limit);  // R1 and X^T are rewritten by the next tile
+    if (ok)
+      phase ^= 1u;
+    else if (tid == 0)
+      mma_pending = true;
     tc::fence_before_sync();
     if (__syncthreads_or(!ok)) {
       failed = true;
@@ -851,9 +896,11 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     tc::fence_after_sync();
   }
   if (failed && tid == 0) {
-    atomicAdd(&g_tc_timeouts, 1);
-    // a rows copy may still be landing in shared memory: wait for it (bounded) before leaving
-    if (kBulk && rows_pending) tc::mbar_wait(bar_rows, rphase, kWaitLimit);
+    // the MMAs and a rows copy may still run: let them finish (bounded) before tensor memory is
+    // read and freed and the block leaves
+    if (mma_pending) tc::mbar_wait(bar, phase, kDrainLimit);
+    if (kBulk && rows_pending) tc::mbar_wait(bar_rows, rphase, kDrainLimit);
+    report_timeout(g.status);
   }
   // weight-gradient partials of this block
   const bool have = blockIdx.x < ntiles && !failed;  // every block with a tile issued the dW0 MMAs
@@ -861,6 +908,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   float* R2 = reinterpret_cast<float*>(R1);           // [64][64]: dW0 rows of DZ_lo x X_hi
   float* RW1 = R2 + 64 * 64;                          // [4 q][2 hh][3][32] dW1, then [4][3] db1
   __syncthreads();
+  tc::fence_after_sync();  // thread 0's drain (after a give-up) before this block reads tensor memory
   if (q >= 2) {
     float v[32];
     tc::tmem_ld32(tbase + lane_base + 128 + 32 * hh, v);
@@ -1034,7 +1082,7 @@ int launch_fwd(const HashArgs& a, const float* X, int64_t ldx, int64_t P, const 
     if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "mlp forward: %s", cudaGetErrorString(e));
     const int64_t pairs = (tiles + 1) / 2;
     const unsigned blocks = (unsigned)(pairs < (int64_t)kSMs ? pairs : (int64_t)kSMs);
-    k_mlp_fwd_rows2<<<blocks, 512, kFwd2Smem, st>>>(X, P, w, colors);
+    k_mlp_fwd_rows2<<<blocks, 512, kFwd2Smem, st>>>(X, P, w, colors, t_guard);
     return VX_OK;
   }
   auto kern = k_mlp_fwd_tc<kHashIn, kRowsOut>;
@@ -1042,7 +1090,7 @@ int launch_fwd(const HashArgs& a, const float* X, int64_t ldx, int64_t P, const 
   if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "mlp forward: %s", cudaGetErrorString(e));
   const unsigned blocks = (unsigned)(tiles < (int64_t)kSMs * 2 ? tiles : (int64_t)kSMs * 2);
   const int xvec = X && (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
-  kern<<<blocks, 256, kFwdSmem, st>>>(a, X, ldx, xvec, P, w, colors);
+  kern<<<blocks, 256, kFwdSmem, st>>>(a, X, ldx, xvec, P, w, colors, t_guard);
   return VX_OK;
 }
 
@@ -1135,6 +1183,13 @@ int vx_mlp_blocks(int64_t n_points) {
 
 int vx_mlp_partial_floats(void) { return WG; }
 
+int vx_tc_guard(int* status, int64_t wait_polls) {
+  VX_REQUIRE(wait_polls <= (int64_t)UINT32_MAX, "wait_polls above 2^32 - 1");
+  t_guard.status = status;
+  t_guard.limit = wait_polls < 0 ? kWaitLimit : (uint32_t)wait_polls;
+  return VX_OK;
+}
+
 int vx_tensor_core_timeouts(void) {
   int h = 0;
   const int zero = 0;
@@ -1179,7 +1234,7 @@ int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int 
     auto kern = bulk ? k_mlp_bwd_tc<true> : k_mlp_bwd_tc<false>;
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "radiance_mlp_backward: %s", cudaGetErrorString(e));
-    kern<<<nb, 256, smem, st>>>(x, ldx, xvec, n_points, w, d_colors, colors, d_hash, d_normal, partials);
+    kern<<<nb, 256, smem, st>>>(x, ldx, xvec, n_points, w, d_colors, colors, d_hash, d_normal, partials, t_guard);
   } else {
     cudaMemsetAsync(partials, 0, sizeof(float) * WG, st);
   }

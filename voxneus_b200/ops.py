@@ -1091,3 +1091,71 @@ def adam_torch_step_scalars(step: int, beta1: float, beta2: float, lr: float):
     out = (ctypes.c_float * 2)()
     L.query("vx_adam_torch_step_scalars", int(step), float(beta1), float(beta2), float(lr), out)
     return float(out[0]), float(out[1])
+
+
+# ------------------------------------------------------------------ tensor-core wait policy ------
+
+
+class tc_guard:
+    """Context manager: MLP launches of this thread inside it poll the tensor core's mbarriers at
+    most `wait_polls` times per wait (None: the library default) and increment the int32 device
+    tensor `status` (or nothing, when None) for every block that gave up. Restores the previous
+    policy on exit. Launches captured into a CUDA graph keep the policy they were captured with."""
+
+    _local = threading.local()
+
+    def __init__(self, status: Optional[torch.Tensor], wait_polls: Optional[int] = None):
+        if status is not None:
+            check_tensor(status, "status", dtype=torch.int32)
+        self.status = status
+        self.polls = -1 if wait_polls is None else int(wait_polls)
+
+    def __enter__(self):
+        stack = getattr(self._local, "stack", None)
+        if stack is None:
+            stack = self._local.stack = []
+        stack.append((self.status, self.polls))
+        call("vx_tc_guard", ptr(self.status), self.polls)
+        return self
+
+    def __exit__(self, *exc):
+        stack = self._local.stack
+        stack.pop()
+        status, polls = stack[-1] if stack else (None, -1)
+        call("vx_tc_guard", ptr(status), polls)
+        return False
+
+
+class StatusWatch:
+    """Reads a device int32 status word one step late without synchronising: `after_step()`
+    queues its copy to pinned host memory on the current stream; `check()` raises if a copy that
+    has landed holds a nonzero value (an earlier step's tensor-core wait gave up)."""
+
+    def __init__(self, status: torch.Tensor, what: str, slots: int = 4):
+        self.status = status
+        self.what = what
+        self.host = torch.zeros(slots, dtype=torch.int32).pin_memory()
+        self.events = [None] * slots
+        self.slot = 0
+
+    def after_step(self) -> None:
+        s = self.slot
+        if self.events[s] is not None:
+            self.events[s].synchronize()  # the copy queued `slots` steps ago
+            self._test(s)
+        self.host[s:s + 1].copy_(self.status, non_blocking=True)
+        ev = self.events[s] or torch.cuda.Event()
+        ev.record()
+        self.events[s] = ev
+        self.slot = (s + 1) % len(self.events)
+
+    def check(self) -> None:
+        for s, ev in enumerate(self.events):
+            if ev is not None and ev.query():
+                self._test(s)
+
+    def _test(self, s: int) -> None:
+        v = int(self.host[s])
+        if v:
+            raise RuntimeError(f"{self.what}: {v} block(s) gave up waiting on the tensor core; the gradients "
+                               f"and colours of that step are invalid")

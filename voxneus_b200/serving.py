@@ -165,7 +165,8 @@ class ServingEngine:
 
     def __init__(self, store: SceneStore, memory_fraction: float = 0.5, n_samples: int = 64,
                  n_importance: int = 64, budget_bytes: Optional[int] = None, fault_injector=None,
-                 render_buckets: Optional[Tuple[int, ...]] = None, query_buckets: Optional[Tuple[int, ...]] = None):
+                 render_buckets: Optional[Tuple[int, ...]] = None, query_buckets: Optional[Tuple[int, ...]] = None,
+                 tc_wait_polls: Optional[int] = None):
         if render_buckets:
             self.RENDER_BUCKETS = tuple(sorted(render_buckets))
         if query_buckets:
@@ -177,13 +178,18 @@ class ServingEngine:
         self.copy = torch.cuda.Stream(self.device)
         self.pool = torch.cuda.graph_pool_handle()
         self.graphs: Dict[Tuple[str, str, int], _GraphBucket] = {}
-        for name, m in store.scenes.items():
-            for size in self.RENDER_BUCKETS:
-                self.graphs[(name, "render", size)] = _GraphBucket(m, "render", size, self.sampler, self.pool,
-                                                                   self.compute)
-            for size in self.QUERY_BUCKETS:
-                self.graphs[(name, "query", size)] = _GraphBucket(m, "query", size, self.sampler, self.pool,
-                                                                  self.compute)
+        # blocks of the MLP kernels that gave up waiting on the tensor core (every graph is captured
+        # with this status word); a request whose completion sees it nonzero stops the engine
+        self.tc_status = torch.zeros(1, dtype=torch.int32, device=self.device)
+        self._status_host = torch.zeros(4096, dtype=torch.int32).pin_memory()
+        with ops.tc_guard(self.tc_status, tc_wait_polls):
+            for name, m in store.scenes.items():
+                for size in self.RENDER_BUCKETS:
+                    self.graphs[(name, "render", size)] = _GraphBucket(m, "render", size, self.sampler, self.pool,
+                                                                       self.compute)
+                for size in self.QUERY_BUCKETS:
+                    self.graphs[(name, "query", size)] = _GraphBucket(m, "query", size, self.sampler, self.pool,
+                                                                      self.compute)
         torch.cuda.synchronize(self.device)
         # device time of one replay of each bucket (the first scene's graphs stand for all scenes)
         self._cost_ms: Dict[Tuple[str, int], float] = {}
@@ -330,6 +336,9 @@ class ServingEngine:
 
     def _finish(self, req: Request):
         """All chunks of req are queued on the compute stream: queue its results for the host."""
+        with torch.cuda.stream(self.compute):  # the status word as of the request's last chunk
+            k = req.rid % self._status_host.numel()
+            self._status_host[k:k + 1].copy_(self.tc_status, non_blocking=True)
         evt = torch.cuda.Event()
         evt.record(self.compute)
         if req.inputs[0].device.type != "cpu":
@@ -362,6 +371,9 @@ class ServingEngine:
             self._pieces_inflight.append((evt, i, req, dst, n))
 
     def _complete(self, req: Request):
+        bad = int(self._status_host[req.rid % self._status_host.numel()])
+        if bad:  # raised into the loop's handler: every pending request fails and the engine stops
+            raise RuntimeError(f"{bad} block(s) of the MLP kernels gave up waiting on the tensor core")
         req.finished = time.perf_counter()
         self.reserved -= req._reserved
         req._dev_in, req._dev_out = (), {}

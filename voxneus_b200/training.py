@@ -144,7 +144,7 @@ class FusedTrainer:
                  lr_hash: float = 0.01, lr_mlp: float = 0.001, lr_variance: float = 0.0005, up_sample_steps: int = 4,
                  huber_delta: float = 0.1, optimize: bool = True, exchange=None,
                  occupancy_update_interval: int = 16, occupancy_seed: int = 0, cuda_graph: bool = False,
-                 grid_adam: str = "torch"):
+                 grid_adam: str = "torch", tc_wait_polls: Optional[int] = None):
         self.model = model
         self.exchange = exchange  # dataparallel.GradExchange for world_size > 1
         self.sampler = sampler or RaySampler(64, 64, perturb=True)
@@ -170,6 +170,11 @@ class FusedTrainer:
         self.reg_losses = torch.zeros(2, device=dev)
         self.n_active = torch.zeros((), dtype=torch.int64, device=dev)  # |V_R| after the filters
         self.amp_flag = torch.zeros(1, dtype=torch.int32, device=dev)
+        # blocks of the MLP kernels that gave up waiting on the tensor core, accumulated over the
+        # steps; read one step late by the host (no synchronisation), which raises on a nonzero value
+        self.tc_status = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.tc_wait_polls = tc_wait_polls
+        self._tc_watch = ops.StatusWatch(self.tc_status, "training step")
         # training/trainer.py:171-173: occupancy refresh every `occupancy_update_interval` steps
         # (0 disables). Data-parallel ranks draw the cells from one shared seed so that their
         # masks stay identical; a single process draws from the default generator.
@@ -199,8 +204,11 @@ class FusedTrainer:
             raise RuntimeError("grid resolution changed; build a new FusedTrainer after scale_volume_grid")
         graphable = (self.cuda_graph and self.exchange is None and self.optimize and randoms is None
                      and z_vals is None and torch.is_grad_enabled())
+        self._tc_watch.check()
         if graphable and self._eager_steps >= GRAPH_WARMUP_STEPS:
-            return self._graph_step(rays_o, rays_d, target, step)
+            out = self._graph_step(rays_o, rays_d, target, step)
+            self._tc_watch.after_step()
+            return out
         self._graphs.clear()  # an eager step owns fresh gradients; replays would no longer see them
         self._eager_steps += 1
         dev = self.bitmap.device
@@ -208,7 +216,9 @@ class FusedTrainer:
                                   for t in (rays_o, rays_d, target))
         if z_vals is not None and z_vals.device != dev:
             z_vals = z_vals.to(dev, non_blocking=True)
-        return self._eager_step(rays_o, rays_d, target, step, randoms, z_vals)
+        out = self._eager_step(rays_o, rays_d, target, step, randoms, z_vals)
+        self._tc_watch.after_step()
+        return out
 
     def _refresh_occupancy(self, step: int) -> None:
         if self.occupancy_update_interval > 0 and step % self.occupancy_update_interval == 0:
@@ -220,11 +230,12 @@ class FusedTrainer:
         self.bitmap.zero_()
         self.counts.zero_()
         ex = self.exchange
-        out = m.render(rays_o, rays_d, self.sampler, None, None, up_sample_steps=self.up_sample_steps,
-                       sphere_radius=1.0, randoms=randoms, vr_bitmap=self.bitmap, extras=False,
-                       amplify_k=0.0 if ex is not None else amp_k, amp_flag=self.amp_flag, z_vals=z_vals)
-        loss = compute_huber_color_loss(out["rgb"], target, self.huber_delta)
-        loss.backward()
+        with ops.tc_guard(self.tc_status, self.tc_wait_polls):
+            out = m.render(rays_o, rays_d, self.sampler, None, None, up_sample_steps=self.up_sample_steps,
+                           sphere_radius=1.0, randoms=randoms, vr_bitmap=self.bitmap, extras=False,
+                           amplify_k=0.0 if ex is not None else amp_k, amp_flag=self.amp_flag, z_vals=z_vals)
+            loss = compute_huber_color_loss(out["rgb"], target, self.huber_delta)
+            loss.backward()
         if ex is not None:
             from .dataparallel import amplify_after_reduce
 
@@ -239,7 +250,7 @@ class FusedTrainer:
         ops.reg_stencil(grid.detach(), self.filtered, self.res, lo, hi, self.relax_radius, self.band, self.counts,
                         self.w_eik, self.w_curv, grid.grad, self.reg_losses, self.n_active)
         return {"loss_rgb": loss.detach(), "loss_eik": self.reg_losses[0], "loss_curv": self.reg_losses[1],
-                "n_active": self.n_active, "rgb": out["rgb"].detach()}
+                "n_active": self.n_active, "rgb": out["rgb"].detach(), "tc_status": self.tc_status}
 
     def _eager_step(self, rays_o, rays_d, target, step: int, randoms, z_vals=None) -> Dict[str, torch.Tensor]:
         m = self.model
