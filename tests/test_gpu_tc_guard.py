@@ -28,11 +28,11 @@ def _lib_loaded():
 
 def _mlp_inputs(p, ld):
     torch.manual_seed(3)
-    rows = torch.zeros(p, ld, device=DEV)
-    rows[:, :51] = torch.randn(p, 51, device=DEV)
+    wide = torch.zeros(p, ld, device=DEV)
+    wide[:, :51] = torch.randn(p, 51, device=DEV)
     l0, l1 = torch.nn.Linear(51, 64).to(DEV), torch.nn.Linear(64, 3).to(DEV)
     ws = [t.detach() for t in (l0.weight, l0.bias, l1.weight, l1.bias)]
-    return rows, ws
+    return wide[:, :51], ws  # 51 input columns at a row stride of ld floats
 
 
 @pytest.mark.parametrize("ld", [52, 56], ids=["bulk-copy kernels", "register-prefetch kernels"])
