@@ -237,12 +237,9 @@ class FusedTrainer:
             loss = compute_huber_color_loss(out["rgb"], target, self.huber_delta)
             loss.backward()
         if ex is not None:
-            from .dataparallel import amplify_after_reduce
-
-            ex.reduce_grads(list(m.parameters()))
-            ex.union_bitmap(self.bitmap)
-            if amp_k > 0:
-                self.amp_flag.copy_(amplify_after_reduce(m.variance_net.variance, amp_k).reshape(1).int())
+            flag = ex.exchange(list(m.parameters()), self.bitmap, m.variance_net.variance, amp_k)
+            if flag is not None:
+                self.amp_flag.copy_(flag.reshape(1).int())
         grid = m.sdf_grid.grid
         lo, hi = m.sdf_grid.bounds()
         ops.vr_count(self.bitmap, grid.detach(), self.res, lo, hi, self.relax_radius, self.band, self.counts,
