@@ -866,3 +866,49 @@ def test_sorted_field_query_is_bitwise_identical():
     torch.cuda.synchronize()
     for x, y in zip(a[:3], b[:3]):
         assert torch.equal(x, y)
+
+
+@pytest.mark.parametrize("res", [97, 160, 256, 321, 511])
+def test_relax_sphere_membership_at_the_boundary(res):
+    """The relax filter |xyz_min + i * eps| < 1.2 of V_R (training/trainer.py:262-266) on every
+    lattice vertex within 1e-5 of the radius. Membership equals the oracle's (the reference's
+    float32 ops on the host, torch.linalg.norm) wherever the exact distance is more than two ulps
+    from the float32 radius; inside that band any float32 evaluation order may decide either way,
+    and the disagreements there (with the host norm and with torch's CUDA norm) are printed."""
+    from voxneus_b200 import ops
+
+    eps = torch.tensor(2.0 / (res - 1), dtype=torch.float32)
+    lo = torch.tensor([-1.0, -1.0, -1.0])
+    i = torch.arange(res)
+    ii, jj = torch.meshgrid(i, i, indexing="ij")
+    c = (-1.0 + i.double() * float(eps))
+    rem = 1.2 ** 2 - c[ii] ** 2 - c[jj] ** 2
+    ok = rem > 0
+    kc = ((torch.sqrt(rem.clamp(min=0)) + 1.0) / float(eps)).round().long()
+    cand = []
+    for dk in (-1, 0, 1):
+        for sgn in (1, -1):
+            k = kc + dk if sgn > 0 else (res - 1) - kc - dk
+            v = torch.stack([ii, jj, k], -1)[ok & (k >= 0) & (k < res) if sgn > 0 else ok & (k >= 0) & (k < res)]
+            cand.append(v)
+    verts = torch.unique(torch.cat(cand).reshape(-1, 3), dim=0)
+    wc = lo + verts.to(torch.float32) * eps  # the reference's float32 world corners
+    r64 = wc.double().norm(dim=-1)
+    near = (r64 - 1.2).abs() < 1e-5
+    verts, wc, r64 = verts[near], wc[near], r64[near]
+    assert verts.shape[0] > 0
+    host = torch.linalg.norm(wc, dim=-1) < 1.2
+    dev_norm = (torch.linalg.norm(wc.to(DEV), dim=-1) < 1.2).cpu()
+    rs = [res] * 3
+    bm = ops.new_bitmap(rs, DEV)
+    ops.vr_mark_corners(to(verts), rs, bm)
+    counts = ops.vr_count(bm, None, rs, (-1.0,) * 3, (1.0,) * 3, 1.2, 0.0)
+    n = int(counts[1])
+    _, lin = ops.vr_compact(bm, None, rs, (-1.0,) * 3, (1.0,) * 3, 1.2, 0.0, counts, n)
+    vlin = verts[:, 0] * res * res + verts[:, 1] * res + verts[:, 2]
+    kern = torch.isin(vlin, lin.cpu())
+    r32 = float(torch.tensor(1.2, dtype=torch.float32))
+    ambiguous = (r64 - r32).abs() <= 2 * 2.0 ** -23 * r32
+    assert torch.equal(kern[~ambiguous], host[~ambiguous])
+    print(f"res {res}: {verts.shape[0]} vertices within 1e-5 of r = 1.2, {int(ambiguous.sum())} within 2 ulps; "
+          f"kernel vs host norm differ on {int((kern != host).sum())}, vs CUDA norm on {int((kern != dev_norm).sum())}")
