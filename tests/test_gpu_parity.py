@@ -868,10 +868,10 @@ def test_sorted_field_query_is_bitwise_identical():
         assert torch.equal(x, y)
 
 
-@pytest.mark.parametrize("res", [97, 160, 256, 321, 511])
+@pytest.mark.parametrize("res", [128, 241, 256, 321, 451, 511, 512])
 def test_relax_sphere_membership_at_the_boundary(res):
     """The relax filter |xyz_min + i * eps| < 1.2 of V_R (training/trainer.py:262-266) on every
-    lattice vertex within 1e-5 of the radius. Membership equals the oracle's (the reference's
+    lattice vertex within 1e-4 of the radius. Membership equals the oracle's (the reference's
     float32 ops on the host, torch.linalg.norm) wherever the exact distance is more than two ulps
     from the float32 radius; inside that band any float32 evaluation order may decide either way,
     and the disagreements there (with the host norm and with torch's CUDA norm) are printed."""
@@ -887,14 +887,12 @@ def test_relax_sphere_membership_at_the_boundary(res):
     kc = ((torch.sqrt(rem.clamp(min=0)) + 1.0) / float(eps)).round().long()
     cand = []
     for dk in (-1, 0, 1):
-        for sgn in (1, -1):
-            k = kc + dk if sgn > 0 else (res - 1) - kc - dk
-            v = torch.stack([ii, jj, k], -1)[ok & (k >= 0) & (k < res) if sgn > 0 else ok & (k >= 0) & (k < res)]
-            cand.append(v)
+        for k in (kc + dk, (res - 1) - kc - dk):  # the +z and -z crossings of the sphere
+            cand.append(torch.stack([ii, jj, k], -1)[ok & (k >= 0) & (k < res)])
     verts = torch.unique(torch.cat(cand).reshape(-1, 3), dim=0)
     wc = lo + verts.to(torch.float32) * eps  # the reference's float32 world corners
     r64 = wc.double().norm(dim=-1)
-    near = (r64 - 1.2).abs() < 1e-5
+    near = (r64 - 1.2).abs() < 1e-4
     verts, wc, r64 = verts[near], wc[near], r64[near]
     assert verts.shape[0] > 0
     host = torch.linalg.norm(wc, dim=-1) < 1.2
@@ -910,5 +908,5 @@ def test_relax_sphere_membership_at_the_boundary(res):
     r32 = float(torch.tensor(1.2, dtype=torch.float32))
     ambiguous = (r64 - r32).abs() <= 2 * 2.0 ** -23 * r32
     assert torch.equal(kern[~ambiguous], host[~ambiguous])
-    print(f"res {res}: {verts.shape[0]} vertices within 1e-5 of r = 1.2, {int(ambiguous.sum())} within 2 ulps; "
+    print(f"res {res}: {verts.shape[0]} vertices within 1e-4 of r = 1.2, {int(ambiguous.sum())} within 2 ulps; "
           f"kernel vs host norm differ on {int((kern != host).sum())}, vs CUDA norm on {int((kern != dev_norm).sum())}")
