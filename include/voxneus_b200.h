@@ -402,8 +402,10 @@ int vx_vr_compact(const uint32_t* bitmap, const float* grid, const int32_t res[3
  * library until exit. Limit: grids of at most 2^27 voxels (4096 compaction blocks, e.g. 512^3);
  * larger grids are rejected with VX_ERR_INVALID before any launch. Allocates nothing (no
  * cudaMalloc, cudaFree or allocating library call). The first call on each device looks up the
- * array's device address with that device current; make that first call before any stream
- * capture. All calls share the one array: calls that overlap on the GPU (other streams, other
+ * array's device address with that device current and keeps it for the life of the process;
+ * make that first call before any stream capture. The kept address assumes the device's
+ * primary context is never reset (cudaDeviceReset reloads the library's device code and may move
+ * the array; do not call this entry point after one). All calls share the one array: calls that overlap on the GPU (other streams, other
  * host threads) race and must be serialised by the caller. */
 int vx_vr_compact_noalloc(const uint32_t* bitmap, const float* grid, const int32_t res[3], const float xyz_min[3],
                           const float xyz_max[3], float relax_radius, float band, const unsigned long long* counts,

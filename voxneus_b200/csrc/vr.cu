@@ -317,7 +317,9 @@ constexpr int64_t kNoAllocMaxBlocks = 4096;
 static __device__ __align__(256) int g_vr_block_offsets[kNoAllocMaxBlocks];
 
 // Device address of g_vr_block_offsets, looked up once per device with that device
-// current (a host-side reference to the symbol is not a device address).
+// current (a host-side reference to the symbol is not a device address) and kept for the life
+// of the process: valid while the device's primary context lives (a cudaDeviceReset would
+// reload the module and could move the array).
 static int noalloc_offsets(int** out) {
   static std::mutex mu;
   static int* addr[64] = {nullptr};
