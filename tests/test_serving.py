@@ -124,3 +124,31 @@ def test_worker_exception_fails_requests_and_stops_engine():
             eng.submit(_query_req("s0", 10, seed=4))
     finally:
         eng.close()
+
+
+def test_admission_waits_for_memory_then_proceeds():
+    """HBM admission: with a budget that holds one request's device buffers at a time, requests
+    submitted together are admitted one after another, each as the previous one's memory is
+    released, and every result equals the same request served alone."""
+    from voxneus_b200.serving import ServingEngine
+
+    store = _store(n_scenes=2)
+    n = 3000
+    need = ServingEngine._bytes_for("render", n)
+    eng = _engine(store, budget_bytes=need)
+    try:
+        alone = eng.submit(_render_req("s0", n, seed=3)).wait(60).outputs["rgb"].clone()
+        reqs = [eng.submit(_render_req(f"s{i % 2}", n, seed=3 + i)) for i in range(4)]
+        for r in reqs:
+            r.wait(120)
+        assert eng.reserved == 0
+        order = sorted(reqs, key=lambda r: r.admitted)
+        for prev, nxt in zip(order, order[1:]):
+            assert nxt.admitted >= prev.finished  # waited until the budget had room again
+        waits = [r.admitted - r.arrival for r in order]
+        assert waits[-1] > waits[0]
+        assert torch.equal(reqs[0].outputs["rgb"], alone)
+        with pytest.raises(Exception):  # larger than the whole budget: refused at submission
+            eng.submit(_render_req("s0", n + 1, seed=9))
+    finally:
+        eng.close()
