@@ -53,6 +53,9 @@ def parse():
     ap.add_argument("--workload", default="train", choices=["train", "field", "serving"],
                     help="train (the metric line), field (512^3 queries), serving (the request mix)")
     ap.add_argument("--duration", type=float, default=10.0, help="serving: seconds of arrivals")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="train: skip the field-query and short serving-mix summaries of the default line")
+    ap.add_argument("--extras-duration", type=float, default=3.0, help="train: seconds of the serving mix summary")
     return ap.parse_args()
 
 
@@ -599,6 +602,12 @@ def run_fused(args):
         same_gpu = same_gpu_torch_leg(m, batches, dev, step0=STEP0 + n_warm)
         same_gpu["fused_over_same_gpu_torch"] = value / same_gpu["value"]
         same_gpu["fused_e2e_over_same_gpu_torch"] = e2e["value"] / same_gpu["value"]
+    field = serving = None
+    if world == 1 and not args.no_extras:
+        del tr
+        torch.cuda.empty_cache()
+        field = field_summary(args)
+        serving = serving_summary(args, args.extras_duration)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, rays and targets)",
@@ -610,7 +619,7 @@ def run_fused(args):
             "mlp_tensor": mlp_tensor(per_kernel, args.rays * (N_SAMPLES + N_IMPORTANCE)),
             "roofline_render": render_roofline(per_kernel, args.rays, peak, peak_kind),
             "grid_upsample_128_to_256_ms": up_ms, "clocks": clk.summary(), "cpu_baseline": cb,
-            "same_gpu_torch": same_gpu, "parity": parity}
+            "same_gpu_torch": same_gpu, "parity": parity, "field_query_512": field, "serving_mix": serving}
     print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
@@ -679,6 +688,10 @@ def _events():
 
 
 def run_field(args):
+    print(json.dumps(field_summary(args)), flush=True)
+
+
+def field_summary(args):
     """Large-grid field query: 512^3 grid of 32 Gaussian-bump spheres; SDF + Eq.7 normal on a 320^3
     lattice and on 2^24 uniform points; the full-grid eikonal + curvature stencil (every voxel in
     V_R, deterministic gather form)."""
@@ -726,10 +739,16 @@ def run_field(args):
     out["stencil_full_grid"] = {"voxels_per_s": vox / (ms / 1e3), "ms": ms, "bytes_per_voxel": 12,
                                 "achieved_gbs": vox * 12 / (ms / 1e3) / 1e9, "deterministic": True}
     out["value"] = out["random_2^24"]["points_per_s"]
-    print(json.dumps(out), flush=True)
+    del grid, pts, bm, fb, gg
+    torch.cuda.empty_cache()
+    return out
 
 
 def run_serving(args):
+    print(json.dumps(serving_summary(args, args.duration)), flush=True)
+
+
+def serving_summary(args, duration):
     """Serving mix: 16 resident 256^3 scenes (own hash table and MLP each), Poisson arrivals at
     200 req/s, 50/50 renders (log-uniform 4,096-480,000 rays from random views of the 64 cameras,
     128 samples, deterministic sampler) and SDF/normal queries (log-uniform 2^16-2^22 points)."""
@@ -777,7 +796,7 @@ def run_serving(args):
     views = [(o.pin_memory(), d.pin_memory()) for o, d in views]
     qpool = [(torch.rand(1 << 22, 3, generator=torch.Generator().manual_seed(k)) * 2 - 1).pin_memory()
              for k in range(4)]
-    duration = float(args.duration)
+    duration = float(duration)
     rate = 200.0
     t = 0.0
     plan = []
@@ -831,7 +850,9 @@ def run_serving(args):
             "query_points_per_s": sum(r.n for r in qry) / wall, "wall_s": wall,
             "latency_all": latency_stats(reqs), "latency_render": latency_stats(rend),
             "latency_query": latency_stats(qry), "clocks": clk.summary()}
-    print(json.dumps(line), flush=True)
+    del eng, store, views, qpool
+    torch.cuda.empty_cache()
+    return line
 
 
 def main():
