@@ -36,8 +36,10 @@ UNIT = "rays/s"
 N_SAMPLES, N_IMPORTANCE, STEPS_UP = 64, 64, 4
 CPU_SAMPLE_RAYS = 1024
 # the timed steps are numbered from here: past the trainer's s_warmup_steps (5000), so the k = 5
-# s-gradient amplification and its variance learning-rate rule are live, as in 35k of the 40k steps
-STEP0 = 5000
+# s-gradient amplification and its variance learning-rate rule are live, as in 35k of the 40k steps;
+# a multiple of the 16-step occupancy refresh, so the first warm-up step refreshes the mask as a
+# run's first step does
+STEP0 = 5008
 
 
 def parse():

@@ -54,6 +54,10 @@ struct TcGuard {
 // The guard the host launchers of this thread pass (vx_tc_guard).
 thread_local TcGuard t_guard{nullptr, kWaitLimit};
 
+// Whether this thread's launches take the caller's poll limit (a kernel variant that reads it) or
+// the default (a compile-time bound, which keeps the waits' loops as tight as before).
+inline bool custom_wait() { return t_guard.limit != kWaitLimit; }
+
 __device__ __forceinline__ void report_timeout(int* status) {
   atomicAdd(&g_tc_timeouts, 1);
   if (status) atomicAdd(status, 1);
@@ -213,11 +217,12 @@ __device__ __forceinline__ void colour_partial(const float z[32], int hh, const 
 // levels each; SH of the view direction; the normal); else they are read from rows X. kRowsOut
 // also writes the rows for the adjoint. 256 threads: warp w reads TMEM lanes 32*(w%4).. and
 // hidden columns 32*(w/4)..; the two column halves meet in shared memory.
-template <bool kHashIn, bool kRowsOut>
+template <bool kHashIn, bool kRowsOut, bool kCustomWait>
 __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* __restrict__ X, int64_t ldx, int xvec,
                                                        int64_t P, MlpW w, float* __restrict__ colors,
                                                        TcGuard g) {
   extern __shared__ __align__(1024) uint8_t smem[];
+  const uint32_t wait_limit = kCustomWait ? g.limit : kWaitLimit;  // a constant bound unless a caller set one
   uint8_t* XH = smem;
   uint8_t* XL = XH + kXBytes;
   uint8_t* W2 = XL + kXBytes;
@@ -318,15 +323,15 @@ __global__ void __launch_bounds__(256, 2) k_mlp_fwd_tc(HashArgs a, const float* 
     }
     if (!kHashIn && t + gridDim.x < ntiles)  // next tile's rows fly during the MMA and the epilogue
       load_row_chunks(X, ldx, xvec != 0, P, (t + gridDim.x) * TM, tid & (TM - 1), tid >> 7, pre);
-    const bool ok = tc::mbar_wait(bar, phase, g.limit);
+    const bool ok = tc::mbar_wait(bar, phase, wait_limit);
+    phase ^= 1u;
     if (__syncthreads_or(!ok)) {
       if (tid == 0) {
-        if (!ok) tc::mbar_wait(bar, phase, kDrainLimit);  // this tile's Z MMA, before TMEM is freed
+        if (!ok) tc::mbar_wait(bar, phase ^ 1u, kDrainLimit);  // this tile's Z MMA, before TMEM is freed
         report_timeout(g.status);
       }
       break;
     }
-    phase ^= 1u;
     tc::fence_after_sync();
     float z[32];
     tmem_ld_sum32(tbase + ((uint32_t)(32 * q) << 16) + 32 * hh, z);
@@ -373,9 +378,11 @@ __device__ __forceinline__ void slot_sync(int slot) {
   asm volatile("bar.sync %0, 256;" ::"r"(1 + slot) : "memory");
 }
 
+template <bool kCustomWait>
 __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restrict__ X, int64_t P, MlpW w,
                                                          float* __restrict__ colors, TcGuard g) {
   extern __shared__ __align__(1024) uint8_t smem[];
+  const uint32_t wait_limit = kCustomWait ? g.limit : kWaitLimit;
   uint8_t* W2 = smem;
   float* B0 = reinterpret_cast<float*>(W2 + kWBytes);
   float* W1s = B0 + NH;
@@ -426,8 +433,10 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
     tc::mbar_arrive_expect_tx(bar_rows, bytes);
     tc::bulk_g2s(ROWS, X + m0 * KP, bytes, bar_rows);
   };
-  bool rows_pending = false;  // slot thread 0: a rows copy is in flight
-  bool mma_pending = false;   // slot thread 0: its wait on the slot's MMA gave up
+  // slot thread 0's bookkeeping for a give-up: a rows copy in flight and the mbarrier parity it
+  // completes, and whether its own wait on the slot's MMA gave up
+  bool rows_pending = false, mma_pending = false;
+  uint32_t rows_parity = 0;
   if (stid == 0 && t0 < ntiles) {
     fetch_rows(t0);
     rows_pending = true;
@@ -436,15 +445,12 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
   for (int64_t t = t0; t < ntiles; t += tstride) {
     const int64_t m0 = t * TM;
     const bool valid = m0 + m < P;
-    const bool got = tc::mbar_wait(bar_rows, rphase, g.limit);
-    if (got) {  // on a give-up, rphase still names the copy in flight
-      rphase ^= 1u;
-      if (stid == 0) rows_pending = false;
-    } else {
-      s_fail[slot] = 1;
-    }
+    const bool got = tc::mbar_wait(bar_rows, rphase, wait_limit);
+    rphase ^= 1u;
+    if (!got) s_fail[slot] = 1;
     slot_sync(slot);
     if (s_fail[slot]) break;
+    if (stid == 0) rows_pending = false;
     {  // rows -> X_hi (TMEM) and X_lo (sample rows); column 51 zero (the padding column may hold anything)
       const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * (KP * 4));
       const int c0 = hh ? 7 : 0;
@@ -488,14 +494,14 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
       if (t + tstride < ntiles) {  // ROWS has been read: bring this slot's next tile
         fetch_rows(t + tstride);
         rows_pending = true;
+        rows_parity = rphase;
       }
     }
-    const bool ok = tc::mbar_wait(bar, phase, g.limit);
-    if (ok) {
-      phase ^= 1u;
-    } else {
+    const bool ok = tc::mbar_wait(bar, phase, wait_limit);
+    phase ^= 1u;
+    if (!ok) {
       s_fail[slot] = 1;
-      if (stid == 0) mma_pending = true;
+      mma_pending = true;  // read by slot thread 0 only
     }
     slot_sync(slot);
     if (s_fail[slot]) break;
@@ -521,8 +527,8 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
   if (stid == 0 && s_fail[slot]) {
     // this slot's MMA and a rows copy into its buffer may still run: let them finish (bounded)
     // before TMEM and shared memory are released
-    if (mma_pending) tc::mbar_wait(bar, phase, kDrainLimit);
-    if (rows_pending) tc::mbar_wait(bar_rows, rphase, kDrainLimit);
+    if (mma_pending) tc::mbar_wait(bar, phase ^ 1u, kDrainLimit);
+    if (rows_pending) tc::mbar_wait(bar_rows, rows_parity, kDrainLimit);
     report_timeout(g.status);
   }
   tc::fence_before_sync();
@@ -565,13 +571,14 @@ __device__ __forceinline__ uint32_t wt_off(int f, int n) {
 // shared memory through one bulk copy issued as soon as the previous tile has been staged, so no
 // registers or load instructions are spent on the prefetch. Otherwise the rows are prefetched
 // into registers during the previous tile.
-template <bool kBulk>
+template <bool kBulk, bool kCustomWait>
 __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__ X, int64_t ldx, int xvec, int64_t P,
                                                       MlpW w, const float* __restrict__ d_out,
                                                       const float* __restrict__ y_in,
                                                       float* __restrict__ d_hash, float* __restrict__ d_normal,
                                                       float* __restrict__ partials, TcGuard g) {
   extern __shared__ __align__(1024) uint8_t smem[];
+  const uint32_t wait_limit = kCustomWait ? g.limit : kWaitLimit;
   uint8_t* W2 = smem;
   uint8_t* WT2 = W2 + kWBytes;
   uint8_t* XT2 = WT2 + kWBytes;
@@ -624,7 +631,9 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     tc::bulk_g2s(ROWS, X + m0 * KP, bytes, bar_rows);
   };
   uint32_t rphase = 0;
-  bool rows_pending = false;  // thread 0: a rows copy is in flight
+  // thread 0's bookkeeping for a give-up: a rows copy in flight and the mbarrier parity it completes
+  bool rows_pending = false;
+  uint32_t rows_parity = 0;
   if (kBulk && tid == 0 && (int64_t)blockIdx.x < ntiles) {
     fetch_rows(blockIdx.x);
     rows_pending = true;
@@ -642,7 +651,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   }
   float sb[NO] = {0.0f, 0.0f, 0.0f};
   bool first_w = true, failed = false;
-  bool mma_pending = false;  // thread 0: its wait on an MMA gave up
+  bool mma_pending = false;  // thread 0: its own wait on an MMA gave up
   uint32_t phase = 0;
   float4 pre[7];  // !kBulk: this tile's row chunks, loaded during the previous tile
   float dy[NO], yv[NO] = {0.0f, 0.0f, 0.0f};  // dL/dcolour and (y_in) the forward's colour of this sample
@@ -659,15 +668,13 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     const int64_t m0 = t * TM;
     const bool valid = m0 + m < P;
     if (kBulk) {
-      const bool got = tc::mbar_wait(bar_rows, rphase, g.limit);
-      if (got) {  // on a give-up, rphase still names the copy in flight
-        rphase ^= 1u;
-        if (tid == 0) rows_pending = false;
-      }
+      const bool got = tc::mbar_wait(bar_rows, rphase, wait_limit);
+      rphase ^= 1u;
       if (__syncthreads_or(!got)) {
         failed = true;
         break;
       }
+      if (tid == 0) rows_pending = false;
     }
     // rows -> X_hi (TMEM, sample lanes), X_lo (sample rows, R1) and X^T (feature rows); column 51
     // = 1 on real rows (db0)
@@ -723,15 +730,14 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
       if (kBulk && t + gridDim.x < ntiles) {  // ROWS has been read: bring the next tile's rows
         fetch_rows(t + gridDim.x);
         rows_pending = true;
+        rows_parity = rphase;
       }
     }
-    bool ok = tc::mbar_wait(bar, phase, g.limit);
-    if (ok)
-      phase ^= 1u;
-    else if (tid == 0)
-      mma_pending = true;
+    bool ok = tc::mbar_wait(bar, phase, wait_limit);
+    phase ^= 1u;
     if (__syncthreads_or(!ok)) {
       failed = true;
+      mma_pending = !ok;
       break;
     }
     tc::fence_after_sync();
@@ -817,13 +823,11 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
       issue_split_ts(tbase, tbase + kAhiCol, r1 + kXBytes, wt2, 8);
       tc::commit(bar);
     }
-    ok = tc::mbar_wait(bar, phase, g.limit);
-    if (ok)
-      phase ^= 1u;
-    else if (tid == 0)
-      mma_pending = true;
+    ok = tc::mbar_wait(bar, phase, wait_limit);
+    phase ^= 1u;
     if (__syncthreads_or(!ok)) {
       failed = true;
+      mma_pending = !ok;
       break;
     }
     tc::fence_after_sync();
@@ -883,14 +887,12 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
         d_normal[(m0 + m) * 3 + 2] = v[2];
       }
     }
-    ok = tc::mbar_wait(bar, phase, g.limit);  // R1 and X^T are rewritten by the next tile
-    if (ok)
-      phase ^= 1u;
-    else if (tid == 0)
-      mma_pending = true;
+    ok = tc::mbar_wait(bar, phase, wait_limit);  // R1 and X^T are rewritten by the next tile
+    phase ^= 1u;
     tc::fence_before_sync();
     if (__syncthreads_or(!ok)) {
       failed = true;
+      mma_pending = !ok;
       break;
     }
     tc::fence_after_sync();
@@ -898,8 +900,8 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   if (failed && tid == 0) {
     // the MMAs and a rows copy may still run: let them finish (bounded) before tensor memory is
     // read and freed and the block leaves
-    if (mma_pending) tc::mbar_wait(bar, phase, kDrainLimit);
-    if (kBulk && rows_pending) tc::mbar_wait(bar_rows, rphase, kDrainLimit);
+    if (mma_pending) tc::mbar_wait(bar, phase ^ 1u, kDrainLimit);
+    if (kBulk && rows_pending) tc::mbar_wait(bar_rows, rows_parity, kDrainLimit);
     report_timeout(g.status);
   }
   // weight-gradient partials of this block
@@ -1078,14 +1080,15 @@ int launch_fwd(const HashArgs& a, const float* X, int64_t ldx, int64_t P, const 
                cudaStream_t st) {
   const int64_t tiles = (P + TM - 1) / TM;
   if (!kHashIn && ldx == KP && (reinterpret_cast<uintptr_t>(X) & 15) == 0) {  // contiguous rows: two slots
-    cudaError_t e = cudaFuncSetAttribute(k_mlp_fwd_rows2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwd2Smem);
+    auto kern2 = custom_wait() ? k_mlp_fwd_rows2<true> : k_mlp_fwd_rows2<false>;
+    cudaError_t e = cudaFuncSetAttribute(kern2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwd2Smem);
     if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "mlp forward: %s", cudaGetErrorString(e));
     const int64_t pairs = (tiles + 1) / 2;
     const unsigned blocks = (unsigned)(pairs < (int64_t)kSMs ? pairs : (int64_t)kSMs);
-    k_mlp_fwd_rows2<<<blocks, 512, kFwd2Smem, st>>>(X, P, w, colors, t_guard);
+    kern2<<<blocks, 512, kFwd2Smem, st>>>(X, P, w, colors, t_guard);
     return VX_OK;
   }
-  auto kern = k_mlp_fwd_tc<kHashIn, kRowsOut>;
+  auto kern = custom_wait() ? k_mlp_fwd_tc<kHashIn, kRowsOut, true> : k_mlp_fwd_tc<kHashIn, kRowsOut, false>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwdSmem);
   if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "mlp forward: %s", cudaGetErrorString(e));
   const unsigned blocks = (unsigned)(tiles < (int64_t)kSMs * 2 ? tiles : (int64_t)kSMs * 2);
@@ -1231,7 +1234,8 @@ int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int 
     const int xvec = (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
     const bool bulk = xvec && ldx == KP;
     const size_t smem = bulk ? kBwdSmemBulk : kBwdSmemRegs;
-    auto kern = bulk ? k_mlp_bwd_tc<true> : k_mlp_bwd_tc<false>;
+    auto kern = bulk ? (custom_wait() ? k_mlp_bwd_tc<true, true> : k_mlp_bwd_tc<true, false>)
+                     : (custom_wait() ? k_mlp_bwd_tc<false, true> : k_mlp_bwd_tc<false, false>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "radiance_mlp_backward: %s", cudaGetErrorString(e));
     kern<<<nb, 256, smem, st>>>(x, ldx, xvec, n_points, w, d_colors, colors, d_hash, d_normal, partials, t_guard);
