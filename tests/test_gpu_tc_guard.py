@@ -97,7 +97,7 @@ def test_training_step_raises_a_step_later():
     o = (3.0 * o / o.norm(dim=-1, keepdim=True)).to(DEV)
     d = torch.nn.functional.normalize(-o + 0.2 * torch.randn(256, 3, device=DEV), dim=-1)
     t = torch.rand(256, 3, device=DEV)
-    tr = FusedTrainer(m, RaySampler(16, 16, perturb=False), optimize=False, tc_wait_polls=0)
+    tr = FusedTrainer(m, RaySampler(16, 16, perturb=False), optimize=False, tc_wait_polls=0, tc_check_every=1)
     out = tr.step(o, d, t, step=1)
     torch.cuda.synchronize()
     assert int(out["tc_status"].item()) > 0

@@ -1127,18 +1127,24 @@ class tc_guard:
 
 
 class StatusWatch:
-    """Reads a device int32 status word one step late without synchronising: `after_step()`
+    """Reads a device int32 status word without synchronising: every `every`-th `after_step()`
     queues its copy to pinned host memory on the current stream; `check()` raises if a copy that
-    has landed holds a nonzero value (an earlier step's tensor-core wait gave up)."""
+    has landed holds a nonzero value (an earlier step's tensor-core wait gave up). A copy costs the
+    stream a device-to-host round trip (~10 us in a step of graph replays), hence the interval."""
 
-    def __init__(self, status: torch.Tensor, what: str, slots: int = 4):
+    def __init__(self, status: torch.Tensor, what: str, slots: int = 4, every: int = 1):
         self.status = status
         self.what = what
+        self.every = max(int(every), 1)
+        self.calls = 0
         self.host = torch.zeros(slots, dtype=torch.int32).pin_memory()
         self.events = [None] * slots
         self.slot = 0
 
     def after_step(self) -> None:
+        self.calls += 1
+        if self.calls % self.every:
+            return
         s = self.slot
         if self.events[s] is not None:
             self.events[s].synchronize()  # the copy queued `slots` steps ago

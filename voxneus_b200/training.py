@@ -144,7 +144,7 @@ class FusedTrainer:
                  lr_hash: float = 0.01, lr_mlp: float = 0.001, lr_variance: float = 0.0005, up_sample_steps: int = 4,
                  huber_delta: float = 0.1, optimize: bool = True, exchange=None,
                  occupancy_update_interval: int = 16, occupancy_seed: int = 0, cuda_graph: bool = False,
-                 grid_adam: str = "torch", tc_wait_polls: Optional[int] = None):
+                 grid_adam: str = "torch", tc_wait_polls: Optional[int] = None, tc_check_every: int = 8):
         self.model = model
         self.exchange = exchange  # dataparallel.GradExchange for world_size > 1
         self.sampler = sampler or RaySampler(64, 64, perturb=True)
@@ -171,10 +171,12 @@ class FusedTrainer:
         self.n_active = torch.zeros((), dtype=torch.int64, device=dev)  # |V_R| after the filters
         self.amp_flag = torch.zeros(1, dtype=torch.int32, device=dev)
         # blocks of the MLP kernels that gave up waiting on the tensor core, accumulated over the
-        # steps; read one step late by the host (no synchronisation), which raises on a nonzero value
+        # steps (also returned by every step as "tc_status"); copied to the host every
+        # tc_check_every steps and read a step later without a synchronisation: a nonzero value
+        # makes the next step raise
         self.tc_status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.tc_wait_polls = tc_wait_polls
-        self._tc_watch = ops.StatusWatch(self.tc_status, "training step")
+        self._tc_watch = ops.StatusWatch(self.tc_status, "training step", every=tc_check_every)
         # training/trainer.py:171-173: occupancy refresh every `occupancy_update_interval` steps
         # (0 disables). Data-parallel ranks draw the cells from one shared seed so that their
         # masks stay identical; a single process draws from the default generator.
