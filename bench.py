@@ -587,9 +587,9 @@ def run_fused(args):
         dist.all_reduce(t_e, op=dist.ReduceOp.MAX)
         e2e_s = float(t_e.item())
     e2e = {"value": args.rays * world / e2e_s, "unit": UNIT, "h2d_bytes_per_step": args.rays * 9 * 4,
-           "d2h_bytes_per_step": 8, "ms_per_step": e2e_s * 1e3,
-           "readback": "every step's loss and the trainer's tensor-core status word to pinned host memory, read "
-                       "by the host one step later"}
+           "d2h_bytes_per_step": 4.5, "ms_per_step": e2e_s * 1e3,
+           "readback": "every step's loss (4 B) to pinned host memory, read by the host one step later; the "
+                       "trainer's tensor-core status word (4 B) every 8 steps"}
 
     if rank != 0:
         if world > 1:
