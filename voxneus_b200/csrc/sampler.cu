@@ -169,14 +169,10 @@ __device__ __forceinline__ void warp_rank_sort_new(const WarpArrays& A, int ns, 
 __device__ __forceinline__ void warp_merge(const WarpArrays& A, int n, int ns, int lane) {
   for (int i = lane; i < n; i += 32) {
     const float zi = A.z[i];
-    // new samples strictly below zi (ties: old first), by binary search of the sorted A.nz
-    int lo = 0, hi = ns;
-    while (lo < hi) {
-      const int mid = (lo + hi) >> 1;
-      if (A.nz[mid] < zi) lo = mid + 1; else hi = mid;
-    }
-    A.z2[i + lo] = zi;
-    A.f2[i + lo] = A.f[i];
+    int c = 0;
+    for (int k = 0; k < ns; ++k) c += (A.nz[k] < zi);
+    A.z2[i + c] = zi;
+    A.f2[i + c] = A.f[i];
   }
   if (lane < ns) {
     const float v = A.nz[lane];
