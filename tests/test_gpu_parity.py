@@ -636,23 +636,6 @@ def test_chunked_inference_appearance_matches_rows_path():
         _lib.call("vx_appearance_mlp_forward_chunked", *head, P(fused), P(small), ns - 1, st)
 
 
-def test_fused_appearance_render_matches_cublas_path(golden):
-    """Fused hash+MLP render gives the same values and gradients as the cuBLAS MLP path."""
-    from voxneus_b200.rendering import RaySampler, compute_huber_color_loss
-
-    g = golden("render_det.npz")
-    outs = []
-    for fused in (True, False):
-        m = _scene_from(g)
-        out = m.render(to(g["rays_o"]), to(g["rays_d"]), RaySampler(16, 16, perturb=False), to(g["near"]),
-                       to(g["far"]), fused_mlp=fused)
-        compute_huber_color_loss(out["rgb"], to(g["target"]), 0.1).backward()
-        outs.append((out["rgb"].detach(), [p.grad.clone() for p in m.parameters() if p.grad is not None]))
-    assert_close(outs[0][0], outs[1][0], VAL_TOL, "rgb")
-    for a, b in zip(outs[0][1], outs[1][1]):
-        assert_close(a, b, GRAD_TOL, "param grad")
-
-
 def test_deterministic_mode_is_bitwise_reproducible(golden):
     """Sorted segmented-reduction adjoints: identical bits on repeated runs, 1e-4 of the atomic mode."""
     from voxneus_b200 import ops
@@ -910,3 +893,34 @@ def test_relax_sphere_membership_at_the_boundary(res):
     assert torch.equal(kern[~ambiguous], host[~ambiguous])
     print(f"res {res}: {verts.shape[0]} vertices within 1e-4 of r = 1.2, {int(ambiguous.sum())} within 2 ulps; "
           f"kernel vs host norm differ on {int((kern != host).sum())}, vs CUDA norm on {int((kern != dev_norm).sum())}")
+
+
+def test_radiance_mlp_module_on_the_fused_kernels():
+    """RadianceMLP.forward (models/radiance_mlp.py:81-98) runs the tensor-core MLP, forward and
+    adjoint, against the oracle; the view embedding takes no gradient (an error when asked)."""
+    from voxneus_b200.models import RadianceMLP
+
+    torch.manual_seed(17)
+    mlp = RadianceMLP().to(DEV)
+    l0, l1 = mlp.net[0], mlp.net[2]
+    p = 3000
+    h, v, n = torch.randn(p, 32), torch.randn(p, 16), torch.randn(p, 3)
+    with torch.no_grad():
+        z64 = torch.cat([h, v, n], -1).double() @ l0.weight.detach().cpu().double().T + l0.bias.detach().cpu().double()
+        keep = (z64.abs() > 1e-6 * float(z64.abs().max())).all(dim=1)  # away from the ReLU kinks
+    h, v, n = h[keep], v[keep], n[keep]
+    ws = [t.detach().cpu().clone().requires_grad_(True) for t in (l0.weight, l0.bias, l1.weight, l1.bias)]
+    hr, nr = h.clone().requires_grad_(True), n.clone().requires_grad_(True)
+    ref = O.radiance_mlp(hr, v, nr, *ws)
+    cot = torch.randn(ref.shape)
+    (ref * cot).sum().backward()
+    hd, nd = to(h).requires_grad_(True), to(n).requires_grad_(True)
+    out = mlp(hd.reshape(-1, 1, 32), to(v).reshape(-1, 1, 16), nd.reshape(-1, 1, 3)).reshape(-1, 3)
+    assert_close(out, ref.detach(), VAL_TOL, "rgb")
+    (out * to(cot)).sum().backward()
+    assert_close(hd.grad, hr.grad, GRAD_TOL, "d hash")
+    assert_close(nd.grad, nr.grad, GRAD_TOL, "d normal")
+    for a, b, nm in zip((l0.weight, l0.bias, l1.weight, l1.bias), ws, ("W0", "b0", "W1", "b1")):
+        assert_close(a.grad, b.grad, GRAD_TOL, nm)
+    with pytest.raises(NotImplementedError):
+        mlp(hd, to(v).requires_grad_(True), nd)

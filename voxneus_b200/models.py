@@ -14,7 +14,6 @@ from typing import Dict, List, Optional, Tuple, Union
 
 import torch
 import torch.nn as nn
-import torch.nn.functional as F
 
 from . import ops
 
@@ -214,12 +213,16 @@ class RadianceMLP(nn.Module):
                 nn.init.zeros_(m.bias)
 
     def forward(self, hash_features, view_embeddings, normals, geom_features=None, sdf=None):
-        return self.net(torch.cat([hash_features, view_embeddings, normals], dim=-1))
-
-    def forward_rows(self, x: torch.Tensor) -> torch.Tensor:
-        """MLP on pre-assembled input rows (P, 51) (strided views allowed)."""
+        """models/radiance_mlp.py:81-98 on the fused tensor-core MLP (forward and adjoint). The
+        adjoint gives the gradients of the hash features, the normals and the weights; the view
+        embedding (SH of the ray directions) takes none, as in the reference's training."""
+        if view_embeddings.requires_grad:
+            raise NotImplementedError("the fused MLP adjoint gives no gradient for the view embedding")
+        x = torch.cat([hash_features, view_embeddings, normals], dim=-1)
+        lead = x.shape[:-1]
         l0, l1 = self.net[0], self.net[2]
-        return torch.sigmoid(F.linear(F.relu(F.linear(x, l0.weight, l0.bias)), l1.weight, l1.bias))
+        out = ops.RadianceMLPFn.apply(x.reshape(-1, x.shape[-1]), l0.weight, l0.bias, l1.weight, l1.bias)
+        return out.reshape(*lead, 3)
 
 
 class OccupancyGrid(nn.Module):
@@ -333,7 +336,7 @@ class VoxNeuS(nn.Module):
     def render(self, rays_o, rays_d, sampler, near=None, far=None, background_rgb=None, cos_anneal_ratio=0.0,
                use_iter_cos_annealing=False, active_levels=None, up_sample_steps=4, sphere_radius=1.0,
                *, randoms=None, vr_bitmap=None, extras=True, amplify_k=0.0, amp_flag=None,
-               fused_mlp=True, z_vals=None) -> Dict[str, torch.Tensor]:
+               z_vals=None) -> Dict[str, torch.Tensor]:
         """Fused render (models/voxneus.py:169-260).
 
         near/far None: computed from the unit sphere inside the sampler kernel. randoms:
@@ -367,18 +370,13 @@ class VoxNeuS(nn.Module):
                 _, dists, mid = ops.sample_multistep(self.sdf_grid.grid.detach(), lo, hi, o, d, near, far, ns, ni,
                                                      up_sample_steps, perturb, t_rand, u, occ.occupancy_mask,
                                                      *occ.bounds(), want_z=False)
-        handoff = ops.NormalGradHandoff(torch.is_grad_enabled()) if fused_mlp else None
+        handoff = ops.NormalGradHandoff(torch.is_grad_enabled())
         sdf, normal, gsamp = ops.RenderGeometryFn.apply(self.sdf_grid.grid, o, d, mid, lo, hi, vr_bitmap, extras,
                                                         handoff)
-        if fused_mlp:
-            l0, l1 = self.radiance_mlp.net[0], self.radiance_mlp.net[2]
-            colors = ops.AppearanceMLPFn.apply(self.radiance_hash.encoder.embeddings, normal, l0.weight, l0.bias,
-                                               l1.weight, l1.bias, o, d, mid, lo, hi, self.radiance_hash.encoder.cfg,
-                                               active_levels, torch.is_grad_enabled(), handoff)
-        else:
-            x = ops.AppearanceInputFn.apply(self.radiance_hash.encoder.embeddings, normal, o, d, mid, lo, hi,
-                                            self.radiance_hash.encoder.cfg, active_levels)
-            colors = self.radiance_mlp.forward_rows(x).reshape(nr, mid.shape[1], 3)
+        l0, l1 = self.radiance_mlp.net[0], self.radiance_mlp.net[2]
+        colors = ops.AppearanceMLPFn.apply(self.radiance_hash.encoder.embeddings, normal, l0.weight, l0.bias, l1.weight,
+                                           l1.bias, o, d, mid, lo, hi, self.radiance_hash.encoder.cfg, active_levels,
+                                           torch.is_grad_enabled(), handoff)
         out_t = ops.CompositeFn.apply(colors, sdf, normal, self.variance_net.variance, d, mid, dists, None, o, True,
                                       self.variance_net._s_max, sphere_radius if sphere_radius else 0.0,
                                       background_rgb, use_iter_cos_annealing, cos_anneal_ratio, amplify_k, amp_flag,

@@ -515,43 +515,6 @@ MLP_LD = 52  # row stride of the radiance-MLP input buffer: [hash 32 | SH 16 | n
 INFER_CHUNK_ROWS = 1 << 22
 
 
-class AppearanceInputFn(torch.autograd.Function):
-    """Radiance-MLP input rows for (rays, midpoints): hash features, SH(view dir), normal."""
-
-    @staticmethod
-    def forward(ctx, embeddings, normals, rays_o, rays_d, mid, xyz_min, xyz_max, cfg, active_levels):
-        nr, ns = mid.shape
-        p = nr * ns
-        width = 2 * cfg.n_levels + 16 + 3
-        ld = width + 1
-        buf = torch.empty(p, ld, device=mid.device)
-        lw = cfg.level_weights(active_levels)
-        nrm = normals.detach().contiguous()
-        call("vx_appearance_forward", ptr(embeddings.detach()), cfg.n_levels, cfg.log2_size, cfg.n_features,
-             cfg._res_c, lw, None, ptr(rays_o), ptr(rays_d), ptr(mid), ns, f3(xyz_min), f3(xyz_max), p, ptr(buf), ld,
-             2 * cfg.n_levels, None, 0, 2 * cfg.n_levels + 16, ptr(nrm), width, stream_ptr(mid.device))
-        ctx.save_for_backward(rays_o, rays_d, mid)
-        ctx.meta = (xyz_min, xyz_max, cfg, active_levels, embeddings.shape, width)
-        return buf[:, :width]
-
-    @staticmethod
-    def backward(ctx, g):
-        rays_o, rays_d, mid = ctx.saved_tensors
-        xyz_min, xyz_max, cfg, active_levels, eshape, width = ctx.meta
-        nr, ns = mid.shape
-        g = g.contiguous()
-        d_emb = None
-        if ctx.needs_input_grad[0]:
-            d_emb = torch.zeros(eshape, device=g.device)
-            hash_backward(d_emb, cfg, active_levels, None, rays_o, rays_d, mid, ns, xyz_min, xyz_max, nr * ns, g,
-                          g.shape[1])
-        d_n = None
-        if ctx.needs_input_grad[1]:
-            c0 = 2 * cfg.n_levels + 16
-            d_n = g[:, c0:c0 + 3].reshape(nr, ns, 3)
-        return d_emb, d_n, None, None, None, None, None, None, None
-
-
 def mlp_forward(rows: torch.Tensor, W0, b0, W1, b1) -> torch.Tensor:
     """Fused radiance MLP on input rows (P, >=51) with any row stride: colours (P, 3)."""
     p = rows.shape[0]
