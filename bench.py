@@ -250,7 +250,18 @@ def cpu_baseline(args, n_rays=CPU_SAMPLE_RAYS, steps=3):
     from oracle import reference_path as O
     from voxneus_b200 import synthetic
 
+    threads = torch.get_num_threads()
     torch.set_num_threads(os.cpu_count() or 1)
+    try:
+        return _cpu_baseline(args, n_rays, steps)
+    finally:  # every host thread busy in later legs (the serving engine) would contend with its thread
+        torch.set_num_threads(threads)
+
+
+def _cpu_baseline(args, n_rays, steps):
+    from oracle import reference_path as O
+    from voxneus_b200 import synthetic
+
     torch.manual_seed(0)
     g128 = synthetic.shapes_grid(args.res // 2, seed=0)
     grid = O.upsample_grid(g128, args.res).clone().requires_grad_(True)

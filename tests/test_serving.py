@@ -152,3 +152,21 @@ def test_admission_waits_for_memory_then_proceeds():
             eng.submit(_render_req("s0", n + 1, seed=9))
     finally:
         eng.close()
+
+
+def test_small_request_overlaps_a_large_one_on_the_express_lane():
+    """A small request submitted right after a large one finishes first (its chunks run on the
+    higher-priority express stream beside the large request's) and equals the same request alone."""
+    store = _store(n_scenes=2)
+    eng = _engine(store)
+    try:
+        small_alone = eng.submit(_render_req("s0", 700, seed=21)).wait(60).outputs["rgb"].clone()
+        big = eng.submit(_render_req("s1", 60000, seed=22))
+        small = eng.submit(_render_req("s0", 700, seed=21))
+        small.wait(60)
+        big.wait(120)
+        assert small._express and not big._express
+        assert small.finished < big.finished
+        assert torch.equal(small.outputs["rgb"], small_alone)
+    finally:
+        eng.close()

@@ -9,15 +9,20 @@ Design:
 * SceneStore keeps every scene's parameters resident on the device (grid, hash table, MLP,
   variance, occupancy mask).
 * Work is cut into chunks of a few fixed size buckets; each (scene, kind, bucket) has a CUDA
-  graph captured once (all graphs share one memory pool: they replay on one stream, one at a
-  time), so a chunk costs one graph launch whatever kernels it contains.
+  graph captured once (the bulk graphs share one memory pool: they replay on one stream, one at
+  a time), so a chunk costs one graph launch whatever kernels it contains.
+* Two lanes. Requests of at most EXPRESS_CHUNKS chunks of the smallest bucket take the express
+  lane: a higher-priority stream with its own graphs of the smallest buckets (their own memory
+  pool), served first come first served with about EXPRESS_AHEAD_MS of work queued, so their
+  kernels run beside the bulk chunks on the device (the block scheduler prefers the higher
+  priority) instead of behind them. The other requests take the bulk lane.
 * The engine thread admits pending requests while the reserved device memory stays under the
-  budget (a fraction of the free HBM measured at start). It keeps about AHEAD_MS of estimated
-  device work queued on the compute stream (each bucket's graph is timed once at start) and
-  fills it with chunks of the active request with the least remaining work, so a small request
-  that arrives behind large ones runs after at most that much queued work instead of behind
-  every chunk already admitted, while the queue still covers pauses of the engine thread; input
-  copies run on a separate copy stream ahead of the compute stream. Results for
+  budget (a fraction of the free HBM measured at start), between every two chunks it queues. It
+  keeps about AHEAD_MS of estimated bulk work queued on the compute stream (each bucket's graph
+  is timed once at start) and fills it with chunks of the active request with the least
+  remaining work, chosen again for every chunk, so a request that arrives behind large ones runs
+  after at most that much queued work, while the queue still covers pauses of the engine thread;
+  input copies run on a separate copy stream ahead of the compute streams. Results for
   host requests come back through a fixed ring of pinned staging blocks on the copy stream and
   are copied into ordinary host tensors by the engine thread as each block lands (allocating
   pinned memory per request would cost milliseconds and synchronise the device).
@@ -70,6 +75,7 @@ class Request:
     _copy_evt: Optional[torch.cuda.Event] = None
     _out_evt: Optional[torch.cuda.Event] = None
     _pieces_left: int = 0
+    _express: bool = False
 
     @property
     def latency(self) -> float:
@@ -162,11 +168,13 @@ class ServingEngine:
     STAGE_BYTES = 16 << 20  # pinned staging block
     STAGE_BLOCKS = 8
     AHEAD_MS = 20.0  # estimated device time kept queued on the compute stream
+    EXPRESS_CHUNKS = 2  # requests of at most this many smallest-bucket chunks take the express lane
+    EXPRESS_AHEAD_MS = 2.0  # estimated device time kept queued on the express stream
 
     def __init__(self, store: SceneStore, memory_fraction: float = 0.5, n_samples: int = 64,
                  n_importance: int = 64, budget_bytes: Optional[int] = None, fault_injector=None,
                  render_buckets: Optional[Tuple[int, ...]] = None, query_buckets: Optional[Tuple[int, ...]] = None,
-                 tc_wait_polls: Optional[int] = None):
+                 tc_wait_polls: Optional[int] = None, express: bool = True):
         if render_buckets:
             self.RENDER_BUCKETS = tuple(sorted(render_buckets))
         if query_buckets:
@@ -178,6 +186,12 @@ class ServingEngine:
         self.copy = torch.cuda.Stream(self.device)
         self.pool = torch.cuda.graph_pool_handle()
         self.graphs: Dict[Tuple[str, str, int], _GraphBucket] = {}
+        # the express lane: a higher-priority stream whose own graphs (smallest buckets, their own
+        # memory pool) let small requests run beside the bulk chunks instead of behind them
+        self.express = torch.cuda.Stream(self.device, priority=torch.cuda.Stream.priority_range()[1]) \
+            if express else None
+        self.xpool = torch.cuda.graph_pool_handle() if express else None
+        self.xgraphs: Dict[Tuple[str, str, int], _GraphBucket] = {}
         # blocks of the MLP kernels that gave up waiting on the tensor core (every graph is captured
         # with this status word); a request whose completion sees it nonzero stops the engine
         self.tc_status = torch.zeros(1, dtype=torch.int32, device=self.device)
@@ -190,6 +204,10 @@ class ServingEngine:
                 for size in self.QUERY_BUCKETS:
                     self.graphs[(name, "query", size)] = _GraphBucket(m, "query", size, self.sampler, self.pool,
                                                                       self.compute)
+                if self.express is not None:
+                    for kind, size in (("render", self.RENDER_BUCKETS[0]), ("query", self.QUERY_BUCKETS[0])):
+                        self.xgraphs[(name, kind, size)] = _GraphBucket(m, kind, size, self.sampler, self.xpool,
+                                                                        self.express)
         torch.cuda.synchronize(self.device)
         # device time of one replay of each bucket (the first scene's graphs stand for all scenes)
         self._cost_ms: Dict[Tuple[str, int], float] = {}
@@ -224,6 +242,8 @@ class ServingEngine:
         self._pieces_inflight: List[Tuple[torch.cuda.Event, int, Request, torch.Tensor, int]] = []
         self._ahead: "collections.deque" = collections.deque()  # (completion event, cost ms) of queued chunks
         self._ahead_ms = 0.0
+        self._xahead: "collections.deque" = collections.deque()  # the same for the express stream
+        self._xahead_ms = 0.0
         self._rid = 0
         self._stop = threading.Event()
         self._failed: Optional[str] = None
@@ -282,6 +302,8 @@ class ServingEngine:
             self.reserved += need
             req._reserved = need
             req.admitted = time.perf_counter()
+            smallest = self.RENDER_BUCKETS[0] if req.kind == "render" else self.QUERY_BUCKETS[0]
+            req._express = self.express is not None and req.n <= self.EXPRESS_CHUNKS * smallest
             with torch.cuda.stream(self.copy):
                 req._dev_in = tuple(t.to(self.device, non_blocking=True) for t in req.inputs)
                 if req.kind == "render":
@@ -304,10 +326,15 @@ class ServingEngine:
 
     def _run_chunk(self, req: Request):
         start = req._next
-        size = self._bucket(req.kind, req.n - start)
+        if req._express:
+            size = self.RENDER_BUCKETS[0] if req.kind == "render" else self.QUERY_BUCKETS[0]
+            gb = self.xgraphs[(req.scene, req.kind, size)]
+            s = self.express
+        else:
+            size = self._bucket(req.kind, req.n - start)
+            gb = self.graphs[(req.scene, req.kind, size)]
+            s = self.compute
         cnt = min(size, req.n - start)
-        gb = self.graphs[(req.scene, req.kind, size)]
-        s = self.compute
         s.wait_event(req._copy_evt)
         with torch.cuda.stream(s):
             for dst, src in zip(gb.inp, req._dev_in):
@@ -320,8 +347,12 @@ class ServingEngine:
             evt = torch.cuda.Event()
             evt.record(s)
         cost = self._cost_ms[(req.kind, size)]
-        self._ahead.append((evt, cost))
-        self._ahead_ms += cost
+        if req._express:
+            self._xahead.append((evt, cost))
+            self._xahead_ms += cost
+        else:
+            self._ahead.append((evt, cost))
+            self._ahead_ms += cost
         req._next = start + cnt
 
     def _room(self) -> bool:
@@ -330,17 +361,24 @@ class ServingEngine:
             self._ahead_ms -= self._ahead.popleft()[1]
         return self._ahead_ms < self.AHEAD_MS
 
+    def _xroom(self) -> bool:
+        """Less than EXPRESS_AHEAD_MS of estimated work still queued on the express stream."""
+        while self._xahead and self._xahead[0][0].query():
+            self._xahead_ms -= self._xahead.popleft()[1]
+        return self._xahead_ms < self.EXPRESS_AHEAD_MS
+
     def _remaining(self, req: Request) -> float:
         size = self._bucket(req.kind, req.n - req._next)
         return (req.n - req._next) / size * self._cost_ms[(req.kind, size)]
 
     def _finish(self, req: Request):
-        """All chunks of req are queued on the compute stream: queue its results for the host."""
-        with torch.cuda.stream(self.compute):  # the status word as of the request's last chunk
+        """All chunks of req are queued on its stream: queue its results for the host."""
+        s = self.express if req._express else self.compute
+        with torch.cuda.stream(s):  # the status word as of the request's last chunk
             k = req.rid % self._status_host.numel()
             self._status_host[k:k + 1].copy_(self.tc_status, non_blocking=True)
         evt = torch.cuda.Event()
-        evt.record(self.compute)
+        evt.record(s)
         if req.inputs[0].device.type != "cpu":
             req.outputs = dict(req._dev_out)
             self._inflight.append((evt, req))
@@ -400,6 +438,15 @@ class ServingEngine:
         self._pieces_inflight = keep_p
         self._issue_pieces()
 
+    def _step(self, req: Request) -> None:
+        """Queue the next chunk of req; hand it to the output path when it was the last."""
+        if self._fault is not None:
+            self._fault(req)
+        self._run_chunk(req)
+        if req._next >= req.n:
+            self.active.remove(req)
+            self._finish(req)
+
     def _busy(self) -> bool:
         return bool(self.active or self._inflight or self._pieces or self._pieces_inflight)
 
@@ -409,18 +456,28 @@ class ServingEngine:
             while not self._stop.is_set():
                 self._admit()
                 self._poll()
-                if not self.active or not self._room():
-                    if not self._busy() or self.active:
-                        time.sleep(0.0002)
-                    continue
-                while self.active and self._room():
-                    req = min(self.active, key=self._remaining)  # least remaining work first
-                    if self._fault is not None:
-                        self._fault(req)
-                    self._run_chunk(req)
-                    if req._next >= req.n:
-                        self.active.remove(req)
-                        self._finish(req)
+                progressed = False
+                # small requests first, on the express stream (FIFO), while it has room
+                while self._xroom():
+                    req = next((r for r in self.active if r._express), None)
+                    if req is None:
+                        break
+                    progressed = True
+                    self._step(req)
+                    self._admit()
+                # then the bulk lane: least remaining work first, re-chosen after every chunk so a
+                # request admitted meanwhile competes for the next one
+                while self._room():
+                    bulk = [r for r in self.active if not r._express]
+                    if not bulk:
+                        break
+                    progressed = True
+                    self._step(min(bulk, key=self._remaining))
+                    self._admit()
+                    if any(r._express for r in self.active) and self._xroom():
+                        break
+                if not progressed:
+                    time.sleep(0.0002)
         except Exception as e:  # host-side failure: fail every request and stop
             self._failed = f"{type(e).__name__}: {e}"
             in_copy = [p[0] for p in self._pieces] + [p[2] for p in self._pieces_inflight]
