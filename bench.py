@@ -247,9 +247,6 @@ def load_traffic():
 
 def cpu_baseline(args, n_rays=CPU_SAMPLE_RAYS, steps=3):
     """The oracle's training step on the host cores (bounded sample of the same workload)."""
-    from oracle import reference_path as O
-    from voxneus_b200 import synthetic
-
     threads = torch.get_num_threads()
     torch.set_num_threads(os.cpu_count() or 1)
     try:
