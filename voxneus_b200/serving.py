@@ -208,6 +208,13 @@ class ServingEngine:
                     for kind, size in (("render", self.RENDER_BUCKETS[0]), ("query", self.QUERY_BUCKETS[0])):
                         self.xgraphs[(name, kind, size)] = _GraphBucket(m, kind, size, self.sampler, self.xpool,
                                                                         self.express)
+        # one replay of every graph before serving: the first launch of a graph uploads it to the
+        # device, which would otherwise stall the engine thread on the first request of each scene
+        for graphs, stream in ((self.graphs, self.compute), (self.xgraphs, self.express)):
+            if graphs:
+                with torch.cuda.stream(stream):
+                    for gb in graphs.values():
+                        gb.graph.replay()
         torch.cuda.synchronize(self.device)
         # device time of one replay of each bucket (the first scene's graphs stand for all scenes)
         self._cost_ms: Dict[Tuple[str, int], float] = {}
@@ -465,6 +472,7 @@ class ServingEngine:
                     progressed = True
                     self._step(req)
                     self._admit()
+                    self._poll()
                 # then the bulk lane: least remaining work first, re-chosen after every chunk so a
                 # request admitted meanwhile competes for the next one
                 while self._room():
@@ -474,6 +482,7 @@ class ServingEngine:
                     progressed = True
                     self._step(min(bulk, key=self._remaining))
                     self._admit()
+                    self._poll()
                     if any(r._express for r in self.active) and self._xroom():
                         break
                 if not progressed:
