@@ -617,7 +617,7 @@ def run_fused(args):
         del tr
         torch.cuda.empty_cache()
         field = field_summary(args)
-        serving = serving_summary(args, args.extras_duration)
+        serving = serving_subprocess(args.extras_duration)
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, rays and targets)",
@@ -752,6 +752,23 @@ def field_summary(args):
     del grid, pts, bm, fb, gg
     torch.cuda.empty_cache()
     return out
+
+
+def serving_subprocess(duration):
+    """The serving mix measured in a process of its own, as a serving deployment runs (its engine
+    thread shares the interpreter with nothing else): `bench.py --workload serving`."""
+    cmd = [sys.executable, os.path.abspath(__file__), "--workload", "serving", "--duration", str(duration)]
+    try:
+        out = subprocess.run(cmd, cwd=ROOT, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True,
+                             timeout=600)
+    except subprocess.TimeoutExpired:
+        return {"error": "serving subprocess timed out"}
+    lines = [ln for ln in out.stdout.splitlines() if ln.startswith("{")]
+    if out.returncode != 0 or not lines:
+        return {"error": f"serving subprocess rc={out.returncode}: {out.stderr.strip().splitlines()[-1:]}"}
+    res = json.loads(lines[-1])
+    res["process"] = "separate (bench.py --workload serving)"
+    return res
 
 
 def run_serving(args):
