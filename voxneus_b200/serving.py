@@ -26,8 +26,12 @@ Design:
   host requests come back through a fixed ring of pinned staging blocks on the copy stream and
   are copied into ordinary host tensors by the engine thread as each block lands (allocating
   pinned memory per request would cost milliseconds and synchronise the device).
+* Requests share launches: a bulk chunk that its request cannot fill (its last one) takes the
+  next rays of the other active requests of the same scene and kind, through a segment table
+  (request, first ray, count, offset in the bucket) applied by the copies into and out of the
+  graph's buffers.
 * A result is the same alone and in any mix: every ray and point is computed independently,
-  with the same kernels and launch shapes, whatever chunk it falls in.
+  with the same kernels and launch shapes, whatever chunk (and whichever neighbours) it falls in.
 * Failures stay on the host: malformed requests are rejected at submission, a request larger
   than the budget is rejected, and an exception inside the engine fails the affected requests
   and stops the engine cleanly.
@@ -251,6 +255,7 @@ class ServingEngine:
         self._ahead_ms = 0.0
         self._xahead: "collections.deque" = collections.deque()  # the same for the express stream
         self._xahead_ms = 0.0
+        self.packed_launches = 0  # bulk launches that carried rays of more than one request
         self._rid = 0
         self._stop = threading.Event()
         self._failed: Optional[str] = None
@@ -331,26 +336,46 @@ class ServingEngine:
                 return b
         return buckets[-1]
 
-    def _run_chunk(self, req: Request):
-        start = req._next
+    def _run_chunk(self, req: Request) -> List[Request]:
+        """Queue one bucket launch for req's next rays (or points). A bulk chunk that req cannot fill
+        takes the next rays of other active requests of the same scene and kind, in admission order
+        (a segment table: request, first ray, count, offset in the bucket). Returns the requests of
+        the launch."""
         if req._express:
             size = self.RENDER_BUCKETS[0] if req.kind == "render" else self.QUERY_BUCKETS[0]
             gb = self.xgraphs[(req.scene, req.kind, size)]
             s = self.express
         else:
-            size = self._bucket(req.kind, req.n - start)
+            size = self._bucket(req.kind, req.n - req._next)
             gb = self.graphs[(req.scene, req.kind, size)]
             s = self.compute
-        cnt = min(size, req.n - start)
-        s.wait_event(req._copy_evt)
+        segs = [(req, req._next, min(size, req.n - req._next), 0)]
+        room = size - segs[0][2]
+        if room > 0 and not req._express:
+            for other in self.active:
+                if room == 0:
+                    break
+                if other is req or other._express or other.scene != req.scene or other.kind != req.kind:
+                    continue
+                take = min(room, other.n - other._next)
+                if take > 0:
+                    segs.append((other, other._next, take, size - room))
+                    room -= take
+        if len(segs) > 1:
+            self.packed_launches += 1
+        for r, _, _, _ in segs:
+            s.wait_event(r._copy_evt)
         with torch.cuda.stream(s):
-            for dst, src in zip(gb.inp, req._dev_in):
-                dst[:cnt].copy_(src[start:start + cnt])
-                if cnt < size:
-                    dst[cnt:].copy_(src[start + cnt - 1:start + cnt].expand(size - cnt, 3))
+            for a, dst in enumerate(gb.inp):
+                for r, start, cnt, off in segs:
+                    dst[off:off + cnt].copy_(r._dev_in[a][start:start + cnt])
+                if room > 0:  # pad with the last ray of the launch
+                    r, start, cnt, off = segs[-1]
+                    dst[size - room:].copy_(r._dev_in[a][start + cnt - 1:start + cnt].expand(room, 3))
             gb.graph.replay()
             for k, v in gb.out.items():
-                req._dev_out[k][start:start + cnt].copy_(v[:cnt])
+                for r, start, cnt, off in segs:
+                    r._dev_out[k][start:start + cnt].copy_(v[off:off + cnt])
             evt = torch.cuda.Event()
             evt.record(s)
         cost = self._cost_ms[(req.kind, size)]
@@ -360,7 +385,9 @@ class ServingEngine:
         else:
             self._ahead.append((evt, cost))
             self._ahead_ms += cost
-        req._next = start + cnt
+        for r, start, cnt, _ in segs:
+            r._next = start + cnt
+        return [r for r, _, _, _ in segs]
 
     def _room(self) -> bool:
         """Less than AHEAD_MS of estimated work still queued on the compute stream."""
@@ -446,13 +473,14 @@ class ServingEngine:
         self._issue_pieces()
 
     def _step(self, req: Request) -> None:
-        """Queue the next chunk of req; hand it to the output path when it was the last."""
+        """Queue the next chunk of req; hand every request of the launch that it completed to the
+        output path."""
         if self._fault is not None:
             self._fault(req)
-        self._run_chunk(req)
-        if req._next >= req.n:
-            self.active.remove(req)
-            self._finish(req)
+        for r in self._run_chunk(req):
+            if r._next >= r.n:
+                self.active.remove(r)
+                self._finish(r)
 
     def _busy(self) -> bool:
         return bool(self.active or self._inflight or self._pieces or self._pieces_inflight)
