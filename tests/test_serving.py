@@ -175,14 +175,19 @@ def test_small_request_overlaps_a_large_one_on_the_express_lane():
 def test_requests_share_a_launch_and_match_alone():
     """Two bulk requests of one scene submitted together: the first one's last chunk is filled with
     the second one's first rays (one launch, a segment table), and both equal the requests alone."""
-    store = _store(n_scenes=1)
+    store = _store(n_scenes=2)
     eng = _engine(store)
     try:
         a_alone = eng.submit(_render_req("s0", 1500, seed=31)).wait(60).outputs["rgb"].clone()
         b_alone = eng.submit(_render_req("s0", 2600, seed=32)).wait(60).outputs["rgb"].clone()
         before = eng.packed_launches
+        # a large request of the other scene keeps the engine queuing chunks, so the two arrive
+        # in the same admission round
+        busy = eng.submit(_render_req("s1", 120000, seed=33))
+        time.sleep(0.002)
         a = eng.submit(_render_req("s0", 1500, seed=31))
         b = eng.submit(_render_req("s0", 2600, seed=32))
+        busy.wait(120)
         a.wait(60)
         b.wait(60)
         assert eng.packed_launches > before
