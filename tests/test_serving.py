@@ -138,7 +138,9 @@ def test_admission_waits_for_memory_then_proceeds():
     eng = _engine(store, budget_bytes=need)
     try:
         alone = eng.submit(_render_req("s0", n, seed=3)).wait(60).outputs["rgb"].clone()
-        reqs = [eng.submit(_render_req(f"s{i % 2}", n, seed=3 + i)) for i in range(4)]
+        reqs = [_render_req(f"s{i % 2}", n, seed=3 + i) for i in range(4)]  # built first: submitted together
+        for r in reqs:
+            eng.submit(r)
         for r in reqs:
             r.wait(120)
         assert eng.reserved == 0
@@ -183,10 +185,12 @@ def test_requests_share_a_launch_and_match_alone():
         before = eng.packed_launches
         # a large request of the other scene keeps the engine queuing chunks, so the two arrive
         # in the same admission round
-        busy = eng.submit(_render_req("s1", 120000, seed=33))
+        busy, a, b = (_render_req("s1", 120000, seed=33), _render_req("s0", 1500, seed=31),
+                      _render_req("s0", 2600, seed=32))
+        eng.submit(busy)
         time.sleep(0.002)
-        a = eng.submit(_render_req("s0", 1500, seed=31))
-        b = eng.submit(_render_req("s0", 2600, seed=32))
+        eng.submit(a)
+        eng.submit(b)
         busy.wait(120)
         a.wait(60)
         b.wait(60)
