@@ -163,8 +163,9 @@ def test_small_request_overlaps_a_large_one_on_the_express_lane():
     eng = _engine(store)
     try:
         small_alone = eng.submit(_render_req("s0", 700, seed=21)).wait(60).outputs["rgb"].clone()
-        big = eng.submit(_render_req("s1", 60000, seed=22))
-        small = eng.submit(_render_req("s0", 700, seed=21))
+        big, small = _render_req("s1", 60000, seed=22), _render_req("s0", 700, seed=21)
+        eng.submit(big)
+        eng.submit(small)
         small.wait(60)
         big.wait(120)
         assert small._express and not big._express
