@@ -176,8 +176,8 @@ def test_small_request_overlaps_a_large_one_on_the_express_lane():
 
 
 def test_requests_share_a_launch_and_match_alone():
-    """Two bulk requests of one scene submitted together: the first one's last chunk is filled with
-    the second one's first rays (one launch, a segment table), and both equal the requests alone."""
+    """Two bulk requests of one scene submitted together: a chunk that one of them cannot fill is
+    filled with the other's rays (one launch, a segment table), and both equal the requests alone."""
     store = _store(n_scenes=2)
     eng = _engine(store)
     try:
@@ -190,8 +190,8 @@ def test_requests_share_a_launch_and_match_alone():
                       _render_req("s0", 2600, seed=32))
         eng.submit(busy)
         time.sleep(0.002)
+        eng.submit(b)  # b's first chunk is full; its second one has room for a's rays
         eng.submit(a)
-        eng.submit(b)
         busy.wait(120)
         a.wait(60)
         b.wait(60)
