@@ -388,6 +388,105 @@ def same_gpu_torch_leg(m, batches, dev, steps=3, step0=0):
                     "golden-pinned) on this GPU at the full workload, FP32, TF32 off"}
 
 
+def reference_kernels_leg(m, batch, dev, reps=20):
+    """The reference's own CUDA kernels (voxneus/cuda/*.cu built from its sources into oracle/_ref by
+    oracle/build_ref.py: the checker's second comparison point, never the product) against this
+    library's drop-in entry points, on the inputs of one timed step: Eq.7 interpolation forward and
+    backward at the step's 1M sample positions, eikonal and curvature on the narrow-band vertex list,
+    masked Adam on the 256^3 grid. CUDA-event means over `reps` calls each."""
+    from oracle import build_ref
+    from voxneus_b200 import cuda as vcuda
+    from voxneus_b200 import ops
+
+    ref = build_ref.load()
+    if ref is None:
+        return {"unavailable": "the reference extension was not built (oracle/build_ref.py)"}
+
+    def timed(fn):
+        for _ in range(3):
+            fn()
+        s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        s_.record()
+        for _ in range(reps):
+            fn()
+        e_.record()
+        torch.cuda.synchronize()
+        return s_.elapsed_time(e_) / reps
+
+    def rel(a, b):
+        a, b = a.detach().double(), b.detach().double()
+        return float((a - b).abs().max() / b.abs().max().clamp_min(1e-30))
+
+    o, d, _ = batch
+    n = o.shape[0]
+    gen = torch.Generator(device=dev).manual_seed(77)
+    t_rand, u = m.draw_sampler_randoms(n, N_SAMPLES, N_IMPORTANCE, STEPS_UP, dev, generator=gen)
+    lo, hi = m.sdf_grid.bounds()
+    occ = m.occupancy_grid
+    grid5 = m.sdf_grid.grid.detach()
+    grid3 = grid5[0, 0].contiguous()
+    res = list(grid3.shape)
+    _, _, mid = ops.sample_multistep(grid5, lo, hi, o, d, None, None, N_SAMPLES, N_IMPORTANCE, STEPS_UP, True, t_rand,
+                                     u, occ.occupancy_mask, *occ.bounds(), want_z=False)
+    pts = (o[:, None, :] + d[:, None, :] * mid[..., None]).reshape(-1, 3)
+    lo_t, hi_t = torch.tensor(lo, device=dev), torch.tensor(hi, device=dev)
+    rt = torch.tensor(res, dtype=torch.float32, device=dev)
+    coords = ((pts - lo_t) / (hi_t - lo_t + 1e-8) * (rt - 1.0)).contiguous()  # geometry/coordinates.py:10-29
+    vs = ((hi_t - lo_t) / (rt - 1.0)).contiguous()
+    out = {"points": int(coords.shape[0])}
+    g_ref = ref.gradient_interp_forward(grid3, coords, vs)
+    g_our = vcuda.cuda_gradient_interp(grid3, coords, vs)
+    out["gradient_interp_forward"] = {"reference_ms": timed(lambda: ref.gradient_interp_forward(grid3, coords, vs)),
+                                      "ours_ms": timed(lambda: ops.gradient_interp_raw(grid3, coords, vs.tolist())),
+                                      "max_rel_diff": rel(g_our, g_ref)}
+    gout = torch.randn(coords.shape, device=dev, generator=torch.Generator(device=dev).manual_seed(78))
+    ga, gb = torch.zeros_like(grid3), torch.zeros_like(grid3)
+    ref.gradient_interp_backward(gout, coords, ga, vs)
+    eps = vs.tolist()
+    ops.call("vx_gradient_interp_backward", ops.ptr(gout), ops.ptr(coords), coords.shape[0], ops.ptr(gb), ops.i3(res),
+             ops.f3(eps), ops.stream_ptr(dev))
+    out["gradient_interp_backward"] = {
+        "reference_ms": timed(lambda: ref.gradient_interp_backward(gout, coords, ga, vs)),
+        "ours_ms": timed(lambda: ops.call("vx_gradient_interp_backward", ops.ptr(gout), ops.ptr(coords),
+                                          coords.shape[0], ops.ptr(gb), ops.i3(res), ops.f3(eps),
+                                          ops.stream_ptr(dev))),
+        "max_rel_diff": rel(gb, ga)}
+    # the narrow band |f| < 3 voxels inside the relax sphere, as a vertex list (V_R of a dense render)
+    band = float(torch.tensor(3.0 * eps[0], dtype=torch.float32))
+    bm = torch.full((ops.bitmap_words(res),), -1, dtype=torch.int32, device=dev)
+    counts = ops.vr_count(bm, grid5, res, lo, hi, 1.2, band)
+    nv = int(ops.final_count(counts, 1.2, band))
+    verts, _ = ops.vr_compact(bm, grid5, res, lo, hi, 1.2, band, counts, nv)
+    out["vertices"] = nv
+    for kind, rf in (("eikonal", ref.eikonal_grad), ("curvature", ref.curvature_grad)):
+        ga.zero_()
+        gb.zero_()
+        rf(grid3, verts, ga, vs, 0.1)
+        ops.reg_list(kind, grid3, verts, eps, 0.1, gb)
+        out[f"{kind}_grad"] = {"reference_ms": timed(lambda: rf(grid3, verts, ga, vs, 0.1)),
+                               "ours_ms": timed(lambda: ops.reg_list(kind, grid3, verts, eps, 0.1, gb)),
+                               "max_rel_diff": rel(gb, ga)}
+    p0 = grid3.clone()
+    g = torch.randn(p0.shape, device=dev, generator=torch.Generator(device=dev).manual_seed(79))
+    g = torch.where(torch.rand(p0.shape, device=dev, generator=torch.Generator(device=dev).manual_seed(80)) < 0.5, g,
+                    torch.zeros_like(g))
+    pa, pb = p0.clone(), p0.clone()
+    ma, va, mb, vb = (torch.zeros_like(p0) for _ in range(4))
+    ref.masked_adam_upd(pa, g, ma, va, 1, 0.9, 0.99, 0.1, 1e-8)
+    ops.adam_update(pb, g, mb, vb, 1, 0.9, 0.99, 0.1, 1e-8, masked=True)
+    out["masked_adam_upd"] = {"reference_ms": timed(lambda: ref.masked_adam_upd(pa, g, ma, va, 2, 0.9, 0.99, 0.1, 1e-8)),
+                              "ours_ms": timed(lambda: ops.adam_update(pb, g, mb, vb, 2, 0.9, 0.99, 0.1, 1e-8,
+                                                                       masked=True)),
+                              "max_rel_diff_after_one_step": rel(pb - p0, pa - p0)}
+    for v in out.values():
+        if isinstance(v, dict) and v.get("reference_ms"):
+            v["speedup"] = v["reference_ms"] / v["ours_ms"]
+    out["what"] = ("the reference's own CUDA extension (voxneus/cuda, built from its sources for sm_100a; legacy "
+                   "stream, voxel size read with .item()) against this library's drop-ins, same inputs")
+    return out
+
+
 # Render forward per ray, the unit of the "render kernel" target: sampler 4,444 B (112 SDF queries x
 # 32 B + occupancy + z) + Eq.7 stencil 128 x 128 B + appearance hand-off 128 x 36 B + ray I/O 64 B
 RENDER_BYTES_PER_RAY = 4444 + 16384 + 4608 + 64
@@ -605,13 +704,14 @@ def run_fused(args):
 
             dist.destroy_process_group()
         return
-    cb = parity = same_gpu = None
+    cb = parity = same_gpu = ref_kernels = None
     if world == 1 and not args.no_cpu_baseline:
         cb, _ = cpu_baseline(args)
         parity = parity_leg(m, batches[0], dev)
         same_gpu = same_gpu_torch_leg(m, batches, dev, step0=STEP0 + n_warm)
         same_gpu["fused_over_same_gpu_torch"] = value / same_gpu["value"]
         same_gpu["fused_e2e_over_same_gpu_torch"] = e2e["value"] / same_gpu["value"]
+        ref_kernels = reference_kernels_leg(m, batches[0], dev)
     field = serving = None
     if world == 1 and not args.no_extras:
         del tr
@@ -629,7 +729,8 @@ def run_fused(args):
             "mlp_tensor": mlp_tensor(per_kernel, args.rays * (N_SAMPLES + N_IMPORTANCE)),
             "roofline_render": render_roofline(per_kernel, args.rays, peak, peak_kind),
             "grid_upsample_128_to_256_ms": up_ms, "clocks": clk.summary(), "cpu_baseline": cb,
-            "same_gpu_torch": same_gpu, "parity": parity, "field_query_512": field, "serving_mix": serving}
+            "same_gpu_torch": same_gpu, "parity": parity, "reference_cuda_kernels": ref_kernels,
+            "field_query_512": field, "serving_mix": serving}
     print(json.dumps(line), flush=True)
     if world > 1:
         import torch.distributed as dist
