@@ -465,47 +465,6 @@ def hash_backward(d_emb, cfg, active_levels, pts, rays_o, rays_d, mid, n_samples
              ptr(d_out), ld, stream_ptr(dev))
 
 
-class overlap_hash_adjoint:
-    """Context manager for a caller that orders its own streams (the fused trainer): inside it,
-    AppearanceMLPFn.backward launches the hash-table adjoint on a side stream forked from the
-    current one, so it runs beside the geometry adjoint and whatever the caller queues next on
-    the current stream (they write other buffers). The caller must call `join()` on the current
-    stream before it reads the hash table's gradient; the gradient tensor is then safe to use."""
-
-    _local = threading.local()
-    _streams: Dict[int, torch.cuda.Stream] = {}
-
-    def __enter__(self):
-        self._local.active = True
-        self._local.pending = getattr(self._local, "pending", [])
-        return self
-
-    def __exit__(self, *exc):
-        self._local.active = False
-        return False
-
-    @classmethod
-    def side_stream(cls, device) -> Optional[torch.cuda.Stream]:
-        if not getattr(cls._local, "active", False):
-            return None
-        idx = torch.device(device).index
-        idx = torch.cuda.current_device() if idx is None else idx
-        if idx not in cls._streams:
-            cls._streams[idx] = torch.cuda.Stream(idx)
-        return cls._streams[idx]
-
-    @classmethod
-    def record(cls, event: torch.cuda.Event) -> None:
-        cls._local.pending = getattr(cls._local, "pending", []) + [event]
-
-    @classmethod
-    def join(cls) -> None:
-        """The current stream waits for every side-stream adjoint launched since the last join."""
-        for ev in getattr(cls._local, "pending", []):
-            torch.cuda.current_stream().wait_event(ev)
-        cls._local.pending = []
-
-
 class HashConfig:
     """Static hash-grid description (models/radiance_hash.py:25-60)."""
 
@@ -663,23 +622,9 @@ class AppearanceMLPFn(torch.autograd.Function):
         d_hash, d_normal, dW0, db0, dW1, db1 = mlp_backward(rows, W0, b0, W1, b1, g.reshape(-1, 3), colors)
         d_emb = None
         if ctx.needs_input_grad[0]:
-            side = overlap_hash_adjoint.side_stream(g.device)
-            if side is None:
-                d_emb = torch.zeros(eshape, device=g.device)
-                hash_backward(d_emb, cfg, active_levels, None, rays_o, rays_d, mid, ns, xyz_min, xyz_max, nr * ns,
-                              d_hash, 32)
-            else:  # beside the geometry adjoint; the caller joins before it reads the table's gradient
-                main = torch.cuda.current_stream(g.device)
-                side.wait_stream(main)
-                with torch.cuda.stream(side):
-                    d_emb = torch.zeros(eshape, device=g.device)
-                    hash_backward(d_emb, cfg, active_levels, None, rays_o, rays_d, mid, ns, xyz_min, xyz_max,
-                                  nr * ns, d_hash, 32)
-                    done = torch.cuda.Event()
-                    done.record(side)
-                d_hash.record_stream(side)  # read on the side stream: not reused before it is done
-                d_emb.record_stream(main)
-                overlap_hash_adjoint.record(done)
+            d_emb = torch.zeros(eshape, device=g.device)
+            hash_backward(d_emb, cfg, active_levels, None, rays_o, rays_d, mid, ns, xyz_min, xyz_max, nr * ns, d_hash,
+                          32)
         d_nrm = d_normal.reshape(nshape)
         if ctx.handoff is not None and ctx.needs_input_grad[1]:
             ctx.handoff.d_normal, d_nrm = d_normal, None  # summed inside the geometry adjoint

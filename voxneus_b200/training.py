@@ -144,8 +144,7 @@ class FusedTrainer:
                  lr_hash: float = 0.01, lr_mlp: float = 0.001, lr_variance: float = 0.0005, up_sample_steps: int = 4,
                  huber_delta: float = 0.1, optimize: bool = True, exchange=None,
                  occupancy_update_interval: int = 16, occupancy_seed: int = 0, cuda_graph: bool = False,
-                 grid_adam: str = "torch", tc_wait_polls: Optional[int] = None, tc_check_every: int = 8,
-                 overlap: bool = True):
+                 grid_adam: str = "torch", tc_wait_polls: Optional[int] = None, tc_check_every: int = 8):
         self.model = model
         self.exchange = exchange  # dataparallel.GradExchange for world_size > 1
         self.sampler = sampler or RaySampler(64, 64, perturb=True)
@@ -176,9 +175,6 @@ class FusedTrainer:
         # tc_check_every steps and read a step later without a synchronisation: a nonzero value
         # makes the next step raise
         self.tc_status = torch.zeros(1, dtype=torch.int32, device=dev)
-        # the hash-table adjoint on a side stream beside the geometry adjoint, V_R and the
-        # regularizer (they write the grid's gradient, it the table's), joined before the optimizers
-        self.overlap = bool(overlap)
         self.tc_wait_polls = tc_wait_polls
         self._tc_watch = ops.StatusWatch(self.tc_status, "training step", every=tc_check_every)
         # training/trainer.py:171-173: occupancy refresh every `occupancy_update_interval` steps
@@ -236,17 +232,12 @@ class FusedTrainer:
         self.bitmap.zero_()
         self.counts.zero_()
         ex = self.exchange
-        overlap = self.overlap and ex is None  # the exchange reads every gradient right after backward
         with ops.tc_guard(self.tc_status, self.tc_wait_polls):
             out = m.render(rays_o, rays_d, self.sampler, None, None, up_sample_steps=self.up_sample_steps,
                            sphere_radius=1.0, randoms=randoms, vr_bitmap=self.bitmap, extras=False,
                            amplify_k=0.0 if ex is not None else amp_k, amp_flag=self.amp_flag, z_vals=z_vals)
             loss = compute_huber_color_loss(out["rgb"], target, self.huber_delta)
-            if overlap:
-                with ops.overlap_hash_adjoint():
-                    loss.backward()
-            else:
-                loss.backward()
+            loss.backward()
         if ex is not None:
             flag = ex.exchange(list(m.parameters()), self.bitmap, m.variance_net.variance, amp_k)
             if flag is not None:
@@ -257,8 +248,6 @@ class FusedTrainer:
                      self.filtered)
         ops.reg_stencil(grid.detach(), self.filtered, self.res, lo, hi, self.relax_radius, self.band, self.counts,
                         self.w_eik, self.w_curv, grid.grad, self.reg_losses, self.n_active)
-        if overlap:
-            ops.overlap_hash_adjoint.join()
         return {"loss_rgb": loss.detach(), "loss_eik": self.reg_losses[0], "loss_curv": self.reg_losses[1],
                 "n_active": self.n_active, "rgb": out["rgb"].detach(), "tc_status": self.tc_status}
 
