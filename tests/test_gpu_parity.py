@@ -924,3 +924,41 @@ def test_radiance_mlp_module_on_the_fused_kernels():
         assert_close(a.grad, b.grad, GRAD_TOL, nm)
     with pytest.raises(NotImplementedError):
         mlp(hd, to(v).requires_grad_(True), nd)
+
+
+def test_field_query_at_512():
+    """The large-grid field query workload (512^3 grid of 32 Gaussian-bump spheres): 2^20 scattered
+    points through the Morton-sorted path equal the unsorted kernel bit for bit; a subset of them
+    and of a 320^3 lattice match the oracle's grid_sample SDF and Eq.7 normals (models/sdf_grid.py:
+    90-160, geometry/gradients.py:59-139, the batched query of geometry/mesh.py:80-114)."""
+    from voxneus_b200 import ops, synthetic
+
+    res = 512
+    grid = synthetic.bumpy_spheres_grid(res, 32, seed=3, device=DEV).contiguous()
+    lo, hi = (-1.0, -1.0, -1.0), (1.0, 1.0, 1.0)
+    g = torch.Generator(device=DEV).manual_seed(5)
+    pts = (torch.rand(1 << 20, 3, device=DEV, generator=g) * 2 - 1).contiguous()
+    assert pts.shape[0] >= ops.SORTED_QUERY_MIN_POINTS and grid.numel() * 4 >= ops.SORTED_QUERY_MIN_GRID_BYTES
+    s_sorted, _, n_sorted, _, _ = ops.field_query(grid, lo, hi, pts, sdf=True, normal=True)
+    o_sdf = torch.empty(pts.shape[0], device=DEV)
+    o_nrm = torch.empty(pts.shape[0], 3, device=DEV)
+    ops.call("vx_field_query", ops.ptr(grid), ops.i3([res] * 3), ops.f3(lo), ops.f3(hi), ops.ptr(pts), pts.shape[0],
+             ops.ptr(o_sdf), None, ops.ptr(o_nrm), None, None, ops.stream_ptr(DEV))
+    assert torch.equal(s_sorted, o_sdf) and torch.equal(n_sorted, o_nrm)
+    g5 = grid.cpu()
+    pick = torch.randperm(pts.shape[0], generator=torch.Generator().manual_seed(6))[:4096]
+    p = pts.cpu()[pick]
+    lo_t, hi_t = torch.tensor(lo), torch.tensor(hi)
+    assert_close(s_sorted.cpu()[pick], O.query_sdf(g5, p, lo_t, hi_t).squeeze(-1), VAL_TOL, "sdf 512")
+    _, nrm, _, _ = O.query_normals(g5, p, lo_t, hi_t)
+    assert_close(n_sorted.cpu()[pick], nrm, VAL_TOL, "normal")
+    # lattice: 320^3 points spanning [-1, 1] with torch.linspace spacing, z fastest
+    lat = 320
+    ls, ln = ops.field_query_lattice(grid, lo, hi, [lat] * 3, lo, hi)
+    ax = torch.linspace(-1.0, 1.0, lat)
+    idx = torch.randint(0, lat, (4096, 3), generator=torch.Generator().manual_seed(7))
+    q = torch.stack([ax[idx[:, 0]], ax[idx[:, 1]], ax[idx[:, 2]]], -1)
+    flat = (idx[:, 0] * lat + idx[:, 1]) * lat + idx[:, 2]
+    assert_close(ls.cpu()[flat], O.query_sdf(g5, q, lo_t, hi_t).squeeze(-1), VAL_TOL, "lattice sdf")
+    _, qn, _, _ = O.query_normals(g5, q, lo_t, hi_t)
+    assert_close(ln.cpu()[flat], qn, VAL_TOL, "lattice normal")
