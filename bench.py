@@ -194,8 +194,9 @@ def algorithmic_bytes(name, n_rays, n_samples, res, n_levels=16, ld=52, nnz=None
         "vx_sample_multistep": n_rays * (24 + 4 * N_SAMPLES + 4 * N_IMPORTANCE + 32 * q + occ + 8 * n_samples),
         "vx_render_geometry_forward": n_rays * 24 + P * (4 + 128 + 4 + 12 + 4),
         "vx_appearance_forward": n_rays * 24 + P * (4 + n_levels * 8 * 8 + 12 + 4 * ld),
-        # fused appearance + MLP: midpoint, hash gathers, normal in; colours and the adjoint's rows out
-        "vx_appearance_mlp_forward": n_rays * 24 + P * (4 + n_levels * 8 * 8 + 12 + 12 + 4 * ld),
+        # fused appearance + MLP: midpoint, hash gathers, normal in; colours and the adjoint's compact
+        # rows out ([hash 32 | normal 3 | pad], written once and read back once by the MLP kernel)
+        "vx_appearance_mlp_forward": n_rays * 24 + P * (4 + n_levels * 8 * 8 + 12 + 12 + 2 * 4 * 36),
         "vx_composite_forward": n_rays * (24 + 32) + P * 48,
         "vx_composite_backward": n_rays * (24 + 32) + P * 64,
         "vx_hash_encode_backward": n_rays * 24 + P * (4 + 4 * 2 * n_levels + n_levels * 8 * 16),
@@ -215,6 +216,8 @@ MLP_FLOPS = {
     # hidden recompute (the colours come from the forward), dL/dh 2*3*64, dW1 2*3*64, dW0 (+db0)
     # 2*52*64, dX (35 columns) 2*64*35
     "vx_radiance_mlp_backward": 2 * 52 * 64 + 2 * 3 * 64 * 2 + 2 * 52 * 64 + 2 * 64 * 35,
+    # the same adjoint on the compact rows (SH(d) recomputed from the ray direction: ~40 FLOPs, not counted)
+    "vx_appearance_mlp_backward": 2 * 52 * 64 + 2 * 3 * 64 * 2 + 2 * 52 * 64 + 2 * 64 * 35,
 }
 
 

@@ -259,7 +259,9 @@ int vx_radiance_mlp_forward(const float* x, int64_t ldx, int64_t n_points, int i
 /* Appearance branch + MLP in one pass (models/voxneus.py:147-157): hash features of o + d*mid
  * (16 levels x 2), SH of the ray direction and the normal are built in shared memory and fed to
  * the 51-64-3 MLP; writes colors (n,3) and, when rows is given, the MLP input rows (row stride
- * ld_rows >= 52, multiple of 4, 16-byte aligned; the adjoint's input). */
+ * ld_rows >= 52, multiple of 4, 16-byte aligned; the adjoint's input). ld_rows == 36 stores the
+ * compact rows of vx_appearance_mlp_backward instead: [hash 32 | normal 3 | pad], without the 16
+ * SH(d) columns, which the adjoint recomputes from rays_d. */
 int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, int n_features,
                               const int32_t* level_res, const float* level_weights, const float* rays_o,
                               const float* rays_d, const float* mid, int n_samples, const float xyz_min[3],
@@ -269,9 +271,10 @@ int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, i
 
 /* Inference form of vx_appearance_mlp_forward (models/voxneus.py:147-157 under no_grad, the path
  * of scripts/render.py:35-54; no rows kept for an adjoint): the same colours,
- * computed chunk by chunk of whole rays through the caller's scratch rows (scratch_count x 52
- * floats, 16-byte aligned; at least n_samples rows): each chunk's rows are gathered into the
- * scratch and the MLP reads them back (the gather and the MLP each at their own best occupancy).
+ * computed chunk by chunk of whole rays through the caller's scratch rows (scratch_count x 36
+ * floats, 16-byte aligned; at least n_samples rows): each chunk's compact rows [hash 32 | normal 3 |
+ * pad] are gathered into the scratch and the MLP reads them back with SH(d) recomputed from rays_d
+ * (the gather and the MLP each at their own best occupancy).
  * Fewer, larger chunks cost less: each chunk adds two launches and their tails. n_points must be a
  * multiple of n_samples (whole rays). */
 int vx_appearance_mlp_forward_chunked(const float* table, int n_levels, int log2_size, int n_features,
@@ -309,6 +312,17 @@ int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int 
                              const float* W0, const float* b0, const float* W1, const float* b1, const float* d_colors,
                              const float* colors, float* d_hash, float* d_normal, float* dW0, float* db0, float* dW1,
                              float* db1, float* partials, int64_t n_partial_floats, void* stream);
+
+/* The adjoint of the fused appearance path on its compact rows: n_points rows of 36 floats
+ * [hash 32 | normal 3 | pad] (16-byte aligned, contiguous) whose SH(d) features are recomputed from
+ * rays_d of the sample's ray (sample i belongs to ray i / n_samples): the 16 columns of a full row
+ * that depend on the ray only (models/embedder.py:55-87). Outputs and partials as
+ * vx_radiance_mlp_backward (the same bits as it gives on the full rows). */
+int vx_appearance_mlp_backward(const float* rows, const float* rays_d, int n_samples, int64_t n_points,
+                               const float* W0, const float* b0, const float* W1, const float* b1,
+                               const float* d_colors, const float* colors, float* d_hash, float* d_normal, float* dW0,
+                               float* db0, float* dW1, float* db1, float* partials, int64_t n_partial_floats,
+                               void* stream);
 
 /* ---------------------------------------------------------- render (per ray) --------------- */
 

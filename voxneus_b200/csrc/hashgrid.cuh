@@ -127,23 +127,48 @@ __device__ __forceinline__ void scatter_level(float2* __restrict__ tab, const Le
   }
 }
 
+// Degree-4 real spherical harmonics of a unit direction (models/embedder.py:55-87), four at a time:
+// values 4k .. 4k+3. k is a constant at every call (an unrolled loop), so only that group is built.
+// Every product and difference is rounded on its own, left to right as the reference's elementwise
+// float32 tensor ops evaluate them (Python constants rounded to float32), so the values are the
+// reference's bits in every kernel: no multiply-add is fused, whatever the surrounding code.
+__device__ __forceinline__ float4 sh_chunk(float x, float y, float z, int k) {
+  const float xx = __fmul_rn(x, x), yy = __fmul_rn(y, y);
+  if (k == 0)
+    return make_float4((float)0.28209479177387814, __fmul_rn((float)-0.4886025119029199, y),
+                       __fmul_rn((float)0.4886025119029199, z), __fmul_rn((float)-0.4886025119029199, x));
+  if (k == 1) {
+    const float zz2 = __fmul_rn(__fmul_rn(2.0f, z), z);
+    return make_float4(__fmul_rn(__fmul_rn((float)1.0925484305920792, x), y),
+                       __fmul_rn(__fmul_rn((float)-1.0925484305920792, y), z),
+                       __fmul_rn((float)0.31539156525252005, __fsub_rn(__fsub_rn(zz2, xx), yy)),
+                       __fmul_rn(__fmul_rn((float)-1.0925484305920792, x), z));
+  }
+  if (k == 2) {
+    const float zz4 = __fmul_rn(__fmul_rn(4.0f, z), z);
+    return make_float4(__fmul_rn((float)0.5462742152960396, __fsub_rn(xx, yy)),
+                       __fmul_rn(__fmul_rn((float)-0.5900435899266435, y),
+                                 __fsub_rn(__fmul_rn(__fmul_rn(3.0f, x), x), yy)),
+                       __fmul_rn(__fmul_rn(__fmul_rn((float)2.890611442640554, x), y), z),
+                       __fmul_rn(__fmul_rn((float)-0.4570457994644658, y), __fsub_rn(__fsub_rn(zz4, xx), yy)));
+  }
+  const float zz2 = __fmul_rn(__fmul_rn(2.0f, z), z), zz4 = __fmul_rn(__fmul_rn(4.0f, z), z);
+  const float xx3 = __fmul_rn(__fmul_rn(3.0f, x), x), yy3 = __fmul_rn(__fmul_rn(3.0f, y), y);
+  return make_float4(__fmul_rn(__fmul_rn((float)0.3731763325901154, z), __fsub_rn(__fsub_rn(zz2, xx3), yy3)),
+                     __fmul_rn(__fmul_rn((float)-0.4570457994644658, x), __fsub_rn(__fsub_rn(zz4, xx), yy)),
+                     __fmul_rn(__fmul_rn((float)1.445305721320277, z), __fsub_rn(xx, yy)),
+                     __fmul_rn(__fmul_rn((float)-0.5900435899266435, x), __fsub_rn(xx, yy3)));
+}
+
 __device__ __forceinline__ void sh16(float x, float y, float z, float o[16]) {
-  o[0] = 0.28209479177387814f;
-  o[1] = -0.4886025119029199f * y;
-  o[2] = 0.4886025119029199f * z;
-  o[3] = -0.4886025119029199f * x;
-  o[4] = 1.0925484305920792f * x * y;
-  o[5] = -1.0925484305920792f * y * z;
-  o[6] = 0.31539156525252005f * (2.0f * z * z - x * x - y * y);
-  o[7] = -1.0925484305920792f * x * z;
-  o[8] = 0.5462742152960396f * (x * x - y * y);
-  o[9] = -0.5900435899266435f * y * (3.0f * x * x - y * y);
-  o[10] = 2.890611442640554f * x * y * z;
-  o[11] = -0.4570457994644658f * y * (4.0f * z * z - x * x - y * y);
-  o[12] = 0.3731763325901154f * z * (2.0f * z * z - 3.0f * x * x - 3.0f * y * y);
-  o[13] = -0.4570457994644658f * x * (4.0f * z * z - x * x - y * y);
-  o[14] = 1.445305721320277f * z * (x * x - y * y);
-  o[15] = -0.5900435899266435f * x * (x * x - 3.0f * y * y);
+#pragma unroll
+  for (int k = 0; k < 4; ++k) {
+    const float4 v = sh_chunk(x, y, z, k);
+    o[4 * k] = v.x;
+    o[4 * k + 1] = v.y;
+    o[4 * k + 2] = v.z;
+    o[4 * k + 3] = v.w;
+  }
 }
 
 

@@ -29,6 +29,11 @@ namespace vx {
 
 constexpr int KIN = 51;  // input features
 constexpr int KP = 52;   // row width of the input rows (column 51 is padding)
+// Compact rows of the fused appearance path: [hash 32 | normal 3 | pad], 144 bytes. The 16 SH(d)
+// features (columns 32..47 of a full row) depend on the ray only; the MLP kernels recompute them
+// from the ray's direction while they stage a tile, the same function on the same operands as the
+// row writer, so both layouts give the same bits.
+constexpr int KC = 36;
 constexpr int NH = 64;   // hidden units
 constexpr int NO = 3;    // colours
 constexpr int TM = 128;  // samples per tile (TMEM lanes)
@@ -61,6 +66,39 @@ inline bool custom_wait() { return t_guard.limit != kWaitLimit; }
 __device__ __forceinline__ void report_timeout(int* status) {
   atomicAdd(&g_tc_timeouts, 1);
   if (status) atomicAdd(status, 1);
+}
+
+// Where a kernel's full rows come from: rays_d == nullptr, rows of KP floats; otherwise compact
+// rows of KC floats whose SH features are recomputed from rays_d of the sample's ray (i / S; the
+// entry points keep the sample count below 2^32).
+struct RowSrc {
+  const float* rays_d;
+  int64_t S;
+};
+
+// Feature chunk c = (hh ? 7 : 0) + j (0..12, four features each) of a staged sample: chunks 0..7
+// the hash features, 8..11 SH(d), 12 the normal and the pad column. j is a constant of the
+// unrolled staging loop, so each SH group is built only where it is stored.
+template <bool kCompact>
+__device__ __forceinline__ float4 x_chunk(const float4* rrow, bool hh, int j, float3 dir) {
+  if (kCompact && hh) {
+    if (j == 0) return rrow[7];
+    if (j <= 4) return sh_chunk(dir.x, dir.y, dir.z, j - 1);
+    return rrow[8];
+  }
+  return rrow[(hh ? 7 : 0) + j];
+}
+
+// The ray direction of sample i, for the thread that stages the sample's chunks 7..12.
+template <bool kCompact>
+__device__ __forceinline__ float3 stage_dir(const RowSrc& src, int64_t i, bool need) {
+  float3 d = make_float3(0.0f, 0.0f, 0.0f);
+  if (kCompact && need) {
+    const uint32_t r = (uint32_t)i / (uint32_t)src.S;
+    d = make_float3(__ldg(src.rays_d + 3 * (size_t)r), __ldg(src.rays_d + 3 * (size_t)r + 1),
+                    __ldg(src.rays_d + 3 * (size_t)r + 2));
+  }
+  return d;
 }
 
 struct MlpW {
@@ -378,9 +416,10 @@ __device__ __forceinline__ void slot_sync(int slot) {
   asm volatile("bar.sync %0, 256;" ::"r"(1 + slot) : "memory");
 }
 
-template <bool kCustomWait>
+template <bool kCustomWait, bool kCompact>
 __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restrict__ X, int64_t P, MlpW w,
-                                                         float* __restrict__ colors, TcGuard g) {
+                                                         float* __restrict__ colors, TcGuard g, RowSrc src) {
+  constexpr int kLd = kCompact ? KC : KP;  // floats per row in global memory
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t wait_limit = kCustomWait ? g.limit : kWaitLimit;
   uint8_t* W2 = smem;
@@ -429,9 +468,9 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
   const int64_t t0 = 2 * (int64_t)blockIdx.x + slot, tstride = 2 * (int64_t)gridDim.x;
   auto fetch_rows = [&](int64_t t) {
     const int64_t m0 = t * TM;
-    const uint32_t bytes = (uint32_t)(P - m0 < TM ? P - m0 : TM) * (uint32_t)(KP * 4);
+    const uint32_t bytes = (uint32_t)(P - m0 < TM ? P - m0 : TM) * (uint32_t)(kLd * 4);
     tc::mbar_arrive_expect_tx(bar_rows, bytes);
-    tc::bulk_g2s(ROWS, X + m0 * KP, bytes, bar_rows);
+    tc::bulk_g2s(ROWS, X + m0 * kLd, bytes, bar_rows);
   };
   // slot thread 0's bookkeeping for a give-up: a rows copy in flight and the mbarrier parity it
   // completes, and whether its own wait on the slot's MMA gave up
@@ -452,14 +491,15 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
     if (s_fail[slot]) break;
     if (stid == 0) rows_pending = false;
     {  // rows -> X_hi (TMEM) and X_lo (sample rows); column 51 zero (the padding column may hold anything)
-      const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * (KP * 4));
+      const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * (kLd * 4));
       const int c0 = hh ? 7 : 0;
+      const float3 dir = stage_dir<kCompact>(src, m0 + m, valid && hh);
       float xh[28];  // features 4*c0 .. 4*c0 + 27 (hh = 1: 28..55, with 52..55 the zero chunk 13)
 #pragma unroll
       for (int j = 0; j < 7; ++j) {
         const int c = c0 + j;
         if (c < 13) {
-          float4 u = valid ? rrow[c] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+          float4 u = valid ? x_chunk<kCompact>(rrow, hh, j, dir) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
           if (c == 12) u.w = 0.0f;
           const float v[4] = {u.x, u.y, u.z, u.w};
           float lo[4];
@@ -571,12 +611,13 @@ __device__ __forceinline__ uint32_t wt_off(int f, int n) {
 // shared memory through one bulk copy issued as soon as the previous tile has been staged, so no
 // registers or load instructions are spent on the prefetch. Otherwise the rows are prefetched
 // into registers during the previous tile.
-template <bool kBulk, bool kCustomWait>
+template <bool kBulk, bool kCustomWait, bool kCompact>
 __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__ X, int64_t ldx, int xvec, int64_t P,
                                                       MlpW w, const float* __restrict__ d_out,
                                                       const float* __restrict__ y_in,
                                                       float* __restrict__ d_hash, float* __restrict__ d_normal,
-                                                      float* __restrict__ partials, TcGuard g) {
+                                                      float* __restrict__ partials, TcGuard g, RowSrc src) {
+  constexpr uint32_t kRowB = (kCompact ? KC : KP) * 4;  // bytes per row in global and shared memory
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t wait_limit = kCustomWait ? g.limit : kWaitLimit;
   uint8_t* W2 = smem;
@@ -626,9 +667,9 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   // rows of tile t into ROWS (kBulk): one copy of the tile's valid rows, issued by thread 0
   auto fetch_rows = [&](int64_t t) {
     const int64_t m0 = t * TM;
-    const uint32_t bytes = (uint32_t)(P - m0 < TM ? P - m0 : TM) * kRowBytes;
+    const uint32_t bytes = (uint32_t)(P - m0 < TM ? P - m0 : TM) * kRowB;
     tc::mbar_arrive_expect_tx(bar_rows, bytes);
-    tc::bulk_g2s(ROWS, X + m0 * KP, bytes, bar_rows);
+    tc::bulk_g2s(ROWS, X + m0 * (kRowB / 4), bytes, bar_rows);
   };
   uint32_t rphase = 0;
   // thread 0's bookkeeping for a give-up: a rows copy in flight and the mbarrier parity it completes
@@ -680,7 +721,8 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     // = 1 on real rows (db0)
     {
       const int c0 = hh ? 7 : 0;
-      const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * kRowBytes);
+      const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * kRowB);
+      const float3 dir = stage_dir<kCompact>(src, m0 + m, valid && hh);
       float xh[28];  // features 4*c0 .. 4*c0 + 27 (hh = 1: 28..55, with 52..55 the zero chunk 13)
 #pragma unroll
       for (int jc = 0; jc < 7; ++jc) {
@@ -688,7 +730,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
         if (c < 13) {
           float4 u;
           if (kBulk)
-            u = valid ? rrow[c] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            u = valid ? x_chunk<kCompact>(rrow, hh, jc, dir) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
           else
             u = pre[jc];
           float v[4] = {u.x, u.y, u.z, u.w};
@@ -1009,8 +1051,10 @@ __global__ void __launch_bounds__(256) k_mlp_wgrad_reduce(const float* __restric
 // meet in shared memory and leave as one contiguous block (or row by row for a wider stride).
 constexpr int kRowsPerBlock = 64;
 
+template <bool kCompact>
 __global__ void __launch_bounds__(256) k_hash_rows(HashArgs a) {
-  __shared__ float4 srow[kRowsPerBlock * 13];
+  constexpr int kChunks = kCompact ? KC / 4 : 13;  // float4 chunks per row
+  __shared__ float4 srow[kRowsPerBlock * kChunks];
   const uint32_t mask = (1u << a.log2T) - 1u;
   const size_t T = (size_t)1 << a.log2T;
   const int tid = threadIdx.x, lane = tid & 31, w = tid >> 5, g = w >> 1;
@@ -1039,53 +1083,59 @@ __global__ void __launch_bounds__(256) k_hash_rows(HashArgs a) {
         f[2 * qq] = f0;
         f[2 * qq + 1] = f1;
       }
-      srow[ls * 13 + 2 * g] = make_float4(f[0], f[1], f[2], f[3]);
-      srow[ls * 13 + 2 * g + 1] = make_float4(f[4], f[5], f[6], f[7]);
-      if (g == 0) {
+      srow[ls * kChunks + 2 * g] = make_float4(f[0], f[1], f[2], f[3]);
+      srow[ls * kChunks + 2 * g + 1] = make_float4(f[4], f[5], f[6], f[7]);
+      if (g == 0 && !kCompact) {
         const int64_t r = i / a.S;
         float o[16];
         sh16(__ldg(a.rays_d + 3 * r), __ldg(a.rays_d + 3 * r + 1), __ldg(a.rays_d + 3 * r + 2), o);
 #pragma unroll
-        for (int c = 0; c < 4; ++c) srow[ls * 13 + 8 + c] = make_float4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
+        for (int c = 0; c < 4; ++c)
+          srow[ls * kChunks + 8 + c] = make_float4(o[4 * c], o[4 * c + 1], o[4 * c + 2], o[4 * c + 3]);
       } else if (g == 1) {
-        srow[ls * 13 + 12] = make_float4(a.normals[3 * i], a.normals[3 * i + 1], a.normals[3 * i + 2], 0.0f);
+        srow[ls * kChunks + kChunks - 1] = make_float4(a.normals[3 * i], a.normals[3 * i + 1], a.normals[3 * i + 2],
+                                                       0.0f);
       }
     }
     __syncthreads();
     const int nrows = (int)(a.P - base < kRowsPerBlock ? a.P - base : kRowsPerBlock);
-    if (a.ld == KP) {
-      float4* out = reinterpret_cast<float4*>(a.out + base * KP);
-      for (int k = tid; k < nrows * 13; k += 256) out[k] = srow[k];
+    if (a.ld == 4 * kChunks) {
+      float4* out = reinterpret_cast<float4*>(a.out + base * (4 * kChunks));
+      for (int k = tid; k < nrows * kChunks; k += 256) out[k] = srow[k];
     } else {
-      for (int k = tid; k < nrows * 13; k += 256)
-        reinterpret_cast<float4*>(a.out + (base + k / 13) * a.ld)[k % 13] = srow[k];
+      for (int k = tid; k < nrows * kChunks; k += 256)
+        reinterpret_cast<float4*>(a.out + (base + k / kChunks) * a.ld)[k % kChunks] = srow[k];
     }
     __syncthreads();
   }
 }
 
-// k_hash_rows over a.P samples, one wave of resident blocks.
+// k_hash_rows over a.P samples, one wave of resident blocks; compact rows when a.ld == KC.
 void launch_hash_rows(const HashArgs& a, cudaStream_t st) {
-  static int rows_per_sm = 0;
-  if (rows_per_sm == 0) {
+  static int rows_per_sm[2] = {0, 0};
+  const bool compact = a.ld == KC;
+  auto kern = compact ? k_hash_rows<true> : k_hash_rows<false>;
+  if (rows_per_sm[compact] == 0) {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_hash_rows, 256, 0) != cudaSuccess || nb < 1) nb = 4;
-    rows_per_sm = nb;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, 256, 0) != cudaSuccess || nb < 1) nb = 4;
+    rows_per_sm[compact] = nb;
   }
-  k_hash_rows<<<grid_for((a.P + kRowsPerBlock - 1) / kRowsPerBlock * 256, 256, rows_per_sm), 256, 0, st>>>(a);
+  kern<<<grid_for((a.P + kRowsPerBlock - 1) / kRowsPerBlock * 256, 256, rows_per_sm[compact]), 256, 0, st>>>(a);
 }
 
 template <bool kHashIn, bool kRowsOut>
 int launch_fwd(const HashArgs& a, const float* X, int64_t ldx, int64_t P, const MlpW& w, float* colors,
-               cudaStream_t st) {
+               cudaStream_t st, RowSrc src = RowSrc{nullptr, 0}) {
   const int64_t tiles = (P + TM - 1) / TM;
-  if (!kHashIn && ldx == KP && (reinterpret_cast<uintptr_t>(X) & 15) == 0) {  // contiguous rows: two slots
-    auto kern2 = custom_wait() ? k_mlp_fwd_rows2<true> : k_mlp_fwd_rows2<false>;
+  const bool compact = src.rays_d != nullptr;
+  if (!kHashIn && (compact || ldx == KP) && (reinterpret_cast<uintptr_t>(X) & 15) == 0) {  // contiguous rows: two slots
+    auto kern2 = compact ? (custom_wait() ? k_mlp_fwd_rows2<true, true> : k_mlp_fwd_rows2<false, true>)
+                         : (custom_wait() ? k_mlp_fwd_rows2<true, false> : k_mlp_fwd_rows2<false, false>);
     cudaError_t e = cudaFuncSetAttribute(kern2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwd2Smem);
     if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "mlp forward: %s", cudaGetErrorString(e));
     const int64_t pairs = (tiles + 1) / 2;
     const unsigned blocks = (unsigned)(pairs < (int64_t)kSMs ? pairs : (int64_t)kSMs);
-    kern2<<<blocks, 512, kFwd2Smem, st>>>(X, P, w, colors, t_guard);
+    kern2<<<blocks, 512, kFwd2Smem, st>>>(X, P, w, colors, t_guard, src);
     return VX_OK;
   }
   auto kern = custom_wait() ? k_mlp_fwd_tc<kHashIn, kRowsOut, true> : k_mlp_fwd_tc<kHashIn, kRowsOut, false>;
@@ -1095,6 +1145,40 @@ int launch_fwd(const HashArgs& a, const float* X, int64_t ldx, int64_t P, const 
   const int xvec = X && (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(X) & 15) == 0);
   kern<<<blocks, 256, kFwdSmem, st>>>(a, X, ldx, xvec, P, w, colors, t_guard);
   return VX_OK;
+}
+
+// The adjoint and its weight-gradient reduction. Full rows (src.rays_d == nullptr, any stride
+// >= 51: 52-float contiguous rows take the bulk-copy kernel) or compact rows (bulk copy only).
+int mlp_backward_launch(const float* x, int64_t ldx, int64_t n_points, const float* W0, const float* b0,
+                        const float* W1, const float* b1, const float* d_colors, const float* colors, float* d_hash,
+                        float* d_normal, float* dW0, float* db0, float* dW1, float* db1, float* partials,
+                        int64_t n_partial_floats, cudaStream_t st, RowSrc src, const char* what) {
+  VX_REQUIRE(x && W0 && b0 && W1 && b1 && d_colors && d_hash && d_normal && dW0 && db0 && dW1 && db1 && partials,
+             "null pointer");
+  VX_REQUIRE((reinterpret_cast<uintptr_t>(d_hash) & 15) == 0, "d_hash must be 16-byte aligned");
+  const int nb = vx_mlp_blocks(n_points);
+  VX_REQUIRE(n_partial_floats >= (int64_t)nb * WG, "partials buffer holds %lld floats, need %lld",
+             (long long)n_partial_floats, (long long)nb * WG);
+  MlpW w{W0, b0, W1, b1};
+  const bool compact = src.rays_d != nullptr;
+  if (n_points > 0) {
+    const int xvec = (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
+    const bool bulk = xvec && (compact || ldx == KP);
+    const size_t smem = bulk ? kBwdSmemBulk : kBwdSmemRegs;
+    const bool cw = custom_wait();
+    auto kern = compact ? (cw ? k_mlp_bwd_tc<true, true, true> : k_mlp_bwd_tc<true, false, true>)
+                        : bulk ? (cw ? k_mlp_bwd_tc<true, true, false> : k_mlp_bwd_tc<true, false, false>)
+                               : (cw ? k_mlp_bwd_tc<false, true, false> : k_mlp_bwd_tc<false, false, false>);
+    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+    kern<<<nb, 256, smem, st>>>(x, ldx, xvec, n_points, w, d_colors, colors, d_hash, d_normal, partials, t_guard, src);
+  } else {
+    cudaMemsetAsync(partials, 0, sizeof(float) * WG, st);
+  }
+  k_mlp_wgrad_reduce<<<(WG + 31) / 32, dim3(32, kReduceSlices), 0, st>>>(partials, n_points > 0 ? nb : 1, dW0, db0,
+                                                                        dW1, db1);
+  count_launches(2);
+  return check_launch(what);
 }
 
 }  // namespace vx
@@ -1116,8 +1200,9 @@ int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, i
   if (n_points == 0) return VX_OK;
   VX_REQUIRE(table && rays_o && rays_d && mid && xyz_min && xyz_max && normals && W0 && b0 && W1 && b1 && colors,
              "null pointer");
-  VX_REQUIRE(!rows || (ld_rows >= KP && ld_rows % 4 == 0 && ((uintptr_t)rows & 15) == 0),
-             "rows need a row stride >= 52 floats, a multiple of 4, and 16-byte alignment");
+  VX_REQUIRE(!rows || ((ld_rows == KC || ld_rows >= KP) && ld_rows % 4 == 0 && ((uintptr_t)rows & 15) == 0),
+             "rows need a row stride of 36 floats (compact) or >= 52, a multiple of 4, and 16-byte alignment");
+  VX_REQUIRE(!rows || ld_rows != KC || n_points < (int64_t(1) << 32), "compact rows take fewer than 2^32 samples");
   fill_positions(a, nullptr, rays_o, rays_d, mid, n_samples, xyz_min, xyz_max);
   a.P = n_points;
   a.out = rows;
@@ -1127,7 +1212,8 @@ int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, i
   cudaStream_t st = (cudaStream_t)stream;
   if (rows) {  // training: rows gathered at high occupancy, then the MLP on the rows
     launch_hash_rows(a, st);
-    if (int s = launch_fwd<false, false>(a, rows, ld_rows, n_points, w, colors, st)) return s;
+    const RowSrc src{ld_rows == KC ? rays_d : nullptr, n_samples};
+    if (int s = launch_fwd<false, false>(a, rows, ld_rows, n_points, w, colors, st, src)) return s;
     count_launches(2);
   } else {  // inference: features built in shared memory, nothing else written
     if (int s = launch_fwd<true, false>(a, nullptr, 0, n_points, w, colors, st)) return s;
@@ -1154,8 +1240,9 @@ int vx_appearance_mlp_forward_chunked(const float* table, int n_levels, int log2
   VX_REQUIRE(((uintptr_t)scratch_rows & 15) == 0, "scratch rows must be 16-byte aligned");
   VX_REQUIRE(scratch_count >= n_samples, "scratch holds %lld rows, fewer than one ray's %d samples",
              (long long)scratch_count, n_samples);
+  VX_REQUIRE(scratch_count < (int64_t(1) << 32), "the scratch takes fewer than 2^32 rows");
   fill_positions(a, nullptr, rays_o, rays_d, mid, n_samples, xyz_min, xyz_max);
-  a.ld = KP;
+  a.ld = KC;  // compact rows: SH(d) is recomputed from rays_d by the MLP kernel
   a.out = scratch_rows;
   MlpW w{W0, b0, W1, b1};
   cudaStream_t st = (cudaStream_t)stream;
@@ -1171,7 +1258,9 @@ int vx_appearance_mlp_forward_chunked(const float* table, int n_levels, int log2
     ac.normals = normals + 3 * c0;
     ac.P = len;
     launch_hash_rows(ac, st);
-    if (int s = launch_fwd<false, false>(ac, scratch_rows, KP, len, w, colors + 3 * c0, st)) return s;
+    if (int s = launch_fwd<false, false>(ac, scratch_rows, KC, len, w, colors + 3 * c0, st,
+                                         RowSrc{ac.rays_d, n_samples}))
+      return s;
     launches += 2;
   }
   count_launches(launches);
@@ -1222,30 +1311,23 @@ int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int 
                              float* db1, float* partials, int64_t n_partial_floats, void* stream) {
   VX_REQUIRE(in_dim == KIN && hidden == NH && out_dim == NO, "the fused MLP is %d -> %d -> %d", KIN, NH, NO);
   VX_REQUIRE(n_points >= 0 && ldx >= KIN, "bad sizes");
-  VX_REQUIRE(x && W0 && b0 && W1 && b1 && d_colors && d_hash && d_normal && dW0 && db0 && dW1 && db1 && partials,
-             "null pointer");
-  VX_REQUIRE((reinterpret_cast<uintptr_t>(d_hash) & 15) == 0, "d_hash must be 16-byte aligned");
-  const int nb = vx_mlp_blocks(n_points);
-  VX_REQUIRE(n_partial_floats >= (int64_t)nb * WG, "partials buffer holds %lld floats, need %lld",
-             (long long)n_partial_floats, (long long)nb * WG);
-  MlpW w{W0, b0, W1, b1};
-  cudaStream_t st = (cudaStream_t)stream;
-  if (n_points > 0) {
-    const int xvec = (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
-    const bool bulk = xvec && ldx == KP;
-    const size_t smem = bulk ? kBwdSmemBulk : kBwdSmemRegs;
-    auto kern = bulk ? (custom_wait() ? k_mlp_bwd_tc<true, true> : k_mlp_bwd_tc<true, false>)
-                     : (custom_wait() ? k_mlp_bwd_tc<false, true> : k_mlp_bwd_tc<false, false>);
-    cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "radiance_mlp_backward: %s", cudaGetErrorString(e));
-    kern<<<nb, 256, smem, st>>>(x, ldx, xvec, n_points, w, d_colors, colors, d_hash, d_normal, partials, t_guard);
-  } else {
-    cudaMemsetAsync(partials, 0, sizeof(float) * WG, st);
-  }
-  k_mlp_wgrad_reduce<<<(WG + 31) / 32, dim3(32, kReduceSlices), 0, st>>>(partials, n_points > 0 ? nb : 1, dW0, db0,
-                                                                        dW1, db1);
-  count_launches(2);
-  return check_launch("radiance_mlp_backward");
+  return mlp_backward_launch(x, ldx, n_points, W0, b0, W1, b1, d_colors, colors, d_hash, d_normal, dW0, db0, dW1, db1,
+                             partials, n_partial_floats, (cudaStream_t)stream, RowSrc{nullptr, 0},
+                             "radiance_mlp_backward");
+}
+
+int vx_appearance_mlp_backward(const float* rows, const float* rays_d, int n_samples, int64_t n_points,
+                               const float* W0, const float* b0, const float* W1, const float* b1,
+                               const float* d_colors, const float* colors, float* d_hash, float* d_normal, float* dW0,
+                               float* db0, float* dW1, float* db1, float* partials, int64_t n_partial_floats,
+                               void* stream) {
+  VX_REQUIRE(n_points >= 0 && n_samples >= 1, "bad sizes");
+  VX_REQUIRE(rays_d && rows, "null pointer");
+  VX_REQUIRE(((uintptr_t)rows & 15) == 0, "compact rows must be 16-byte aligned");
+  VX_REQUIRE(n_points < (int64_t(1) << 32), "compact rows take fewer than 2^32 samples");
+  return mlp_backward_launch(rows, KC, n_points, W0, b0, W1, b1, d_colors, colors, d_hash, d_normal, dW0, db0, dW1,
+                             db1, partials, n_partial_floats, (cudaStream_t)stream, RowSrc{rays_d, n_samples},
+                             "appearance_mlp_backward");
 }
 
 }  // extern "C"

@@ -508,7 +508,10 @@ class HashConfig:
 
 
 MLP_LD = 52  # row stride of the radiance-MLP input buffer: [hash 32 | SH 16 | normal 3 | pad]
-# Inference rows scratch: up to 4M rows (832 MiB) per call, whole rays at a time. The split
+# Row stride of the fused appearance path's compact rows, [hash 32 | normal 3 | pad]: the 16 SH(d)
+# columns depend on the ray only and the MLP kernels recompute them from the ray direction.
+MLP_LD_COMPACT = 36
+# Inference rows scratch: up to 4M compact rows (576 MiB) per call, whole rays at a time. The split
 # gather + MLP kernels beat the fused in-shared-memory kernel by ~25% per sample, and chunks this
 # large keep the per-chunk launch and tail cost small (a 65,536-ray render: 256K-row chunks
 # 3.2 ms, 1M 2.66 ms, 4M 2.49 ms of appearance time).
@@ -526,9 +529,10 @@ def mlp_forward(rows: torch.Tensor, W0, b0, W1, b1) -> torch.Tensor:
     return out
 
 
-def mlp_backward(rows, W0, b0, W1, b1, d_colors, colors=None):
+def mlp_backward(rows, W0, b0, W1, b1, d_colors, colors=None, rays_d=None, n_samples=0):
     """colors: the forward's (P, 3) outputs (the adjoint then skips recomputing the output layer),
-    or None."""
+    or None. rays_d given: rows are the compact rows of AppearanceMLPFn (P, 36) whose SH(d) the
+    kernel recomputes from rays_d of row i's ray (i // n_samples)."""
     dev = rows.device
     p = rows.shape[0]
     if colors is not None:
@@ -543,10 +547,17 @@ def mlp_backward(rows, W0, b0, W1, b1, d_colors, colors=None):
     d_hash = torch.empty(p, 32, device=dev)
     d_normal = torch.empty(p, 3, device=dev)
     dW0, db0, dW1, db1 = (torch.empty_like(t) for t in (W0, b0, W1, b1))
-    call("vx_radiance_mlp_backward", ptr(rows), rows.stride(0), p, rows.shape[1], W0.shape[0], W1.shape[0],
-         ptr(W0.detach()), ptr(b0.detach()), ptr(W1.detach()), ptr(b1.detach()),
-         ptr(check_tensor(d_colors.contiguous(), "d_colors")), ptr(colors), ptr(d_hash), ptr(d_normal), ptr(dW0),
-         ptr(db0), ptr(dW1), ptr(db1), ptr(sc.mlp_partials), sc.mlp_partials.numel(), stream_ptr(dev))
+    weights = (ptr(W0.detach()), ptr(b0.detach()), ptr(W1.detach()), ptr(b1.detach()))
+    outs = (ptr(check_tensor(d_colors.contiguous(), "d_colors")), ptr(colors), ptr(d_hash), ptr(d_normal), ptr(dW0),
+            ptr(db0), ptr(dW1), ptr(db1), ptr(sc.mlp_partials), sc.mlp_partials.numel(), stream_ptr(dev))
+    if rays_d is None:
+        call("vx_radiance_mlp_backward", ptr(rows), rows.stride(0), p, rows.shape[1], W0.shape[0], W1.shape[0],
+             *weights, *outs)
+    else:
+        if rows.shape[1] != MLP_LD_COMPACT or not rows.is_contiguous():
+            raise RuntimeError(f"compact MLP rows must be contiguous ({MLP_LD_COMPACT} floats a row)")
+        call("vx_appearance_mlp_backward", ptr(rows), ptr(check_tensor(rays_d, "rays_d")), n_samples, p, *weights,
+             *outs)
     return d_hash, d_normal, dW0, db0, dW1, db1
 
 
@@ -573,8 +584,9 @@ class RadianceMLPFn(torch.autograd.Function):
 class AppearanceMLPFn(torch.autograd.Function):
     """Hash encoding + SH + normal rows -> fused MLP -> colours for (rays, midpoints).
 
-    models/voxneus.py:147-157 without materialising the hidden layer: the rows buffer is kept
-    for the adjoint, which recomputes the hidden layer and scatters into the hash table.
+    models/voxneus.py:147-157 without materialising the hidden layer: the compact rows
+    [hash 32 | normal 3 | pad] are kept for the adjoint, which recomputes SH(d) from the ray
+    direction and the hidden layer, and scatters into the hash table.
     """
 
     @staticmethod
@@ -585,7 +597,7 @@ class AppearanceMLPFn(torch.autograd.Function):
         width = 2 * cfg.n_levels + 16 + 3
         if width != 51:
             raise RuntimeError("the fused appearance path needs 16 hash levels x 2 features")
-        ld = MLP_LD
+        ld = MLP_LD_COMPACT
         # keep_rows: the caller's grad mode (forward itself always runs with grad disabled, and
         # needs_input_grad stays True under no_grad), so inference does not write the rows
         need_rows = bool(keep_rows) and any(ctx.needs_input_grad[:6])
@@ -599,10 +611,8 @@ class AppearanceMLPFn(torch.autograd.Function):
             call("vx_appearance_mlp_forward", *args, ptr(rows), ld, stream_ptr(mid.device))
         else:  # inference: rows pass through an L2-sized scratch, whole rays at a time
             n_rows = max(ns, min(p, (INFER_CHUNK_ROWS // ns) * ns))
-            scratch = torch.empty(n_rows, MLP_LD, device=mid.device)
+            scratch = torch.empty(n_rows, MLP_LD_COMPACT, device=mid.device)
             call("vx_appearance_mlp_forward_chunked", *args, ptr(scratch), n_rows, stream_ptr(mid.device))
-        if rows is not None:
-            rows = rows[:, :width]
         ctx.save_for_backward(rays_o, rays_d, mid, W0, b0, W1, b1)
         ctx.rows = rows
         ctx.colors = colors if rows is not None else None  # the adjoint's sigmoid derivative reads them
@@ -619,7 +629,8 @@ class AppearanceMLPFn(torch.autograd.Function):
         ctx.rows = ctx.colors = None
         if rows is None:
             raise RuntimeError("AppearanceMLPFn: forward ran with keep_rows=False; no adjoint input kept")
-        d_hash, d_normal, dW0, db0, dW1, db1 = mlp_backward(rows, W0, b0, W1, b1, g.reshape(-1, 3), colors)
+        d_hash, d_normal, dW0, db0, dW1, db1 = mlp_backward(rows, W0, b0, W1, b1, g.reshape(-1, 3), colors, rays_d,
+                                                            ns)
         d_emb = None
         if ctx.needs_input_grad[0]:
             d_emb = torch.zeros(eshape, device=g.device)
