@@ -187,6 +187,14 @@ int vx_up_sample(const float* rays_o, const float* rays_d, const float* z, const
 int vx_sample_pdf(const float* bins, const float* weights, const float* cdf, int64_t n_rays, int n_bins,
                   int n_samples, const float* u, const float* u_det, float* out, int64_t* idx_out, void* stream);
 
+/* The sort-and-carry of cat_z_vals (rendering/sampler.py:295-320): per ray, the depths z_old
+ * (n_rays, n_old) and z_new (n_rays, n_new; need not be sorted) concatenated and sorted ascending
+ * as torch.sort orders floats (NaN last) into z_out (n_rays, n_old + n_new); with sdf_out given,
+ * the SDF values sdf_old / sdf_new move with their depths (the reference's gather by the sort's
+ * indices). Equal depths keep concatenation order. n_old + n_new <= 8192. */
+int vx_cat_z_vals(const float* z_old, const float* z_new, const float* sdf_old, const float* sdf_new, int64_t n_rays,
+                  int n_old, int n_new, float* z_out, float* sdf_out, void* stream);
+
 /* ---------------------------------------------------------- render (per sample) ------------ */
 
 /* Pass-2 geometry of VoxNeuS.render (models/voxneus.py:226-236 -> forward_points :115-167):

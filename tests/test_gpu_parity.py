@@ -232,6 +232,40 @@ def test_up_sample_single_step():
     assert_close(out, ref, VAL_TOL, "up_sample")
 
 
+@pytest.mark.parametrize("nr,n,ni", [(50, 64, 16), (7, 112, 16), (3, 1, 1), (5, 0, 9), (4, 300, 200)])
+def test_cat_z_vals_matches_oracle(nr, n, ni):
+    """rendering.cat_z_vals against the oracle's torch.sort + gather (rendering/sampler.py:295-320):
+    the depths and the carried SDF values bit for bit, the new depths unsorted (sample_pdf with
+    random draws), depths present in both lists, NaN depths (sorted last), an empty old list, and
+    `last` (no query, SDF passed through)."""
+    from voxneus_b200.models import DenseSDFGrid
+    from voxneus_b200.rendering import cat_z_vals
+
+    torch.manual_seed(31 + n)
+    o = torch.randn(nr, 3)
+    o = 2.5 * o / o.norm(dim=-1, keepdim=True)
+    d = -o / o.norm(dim=-1, keepdim=True)
+    z = torch.sort(torch.rand(nr, n) * 3 + 0.5, dim=-1)[0]
+    nz = torch.rand(nr, ni) * 3 + 0.5
+    if n > 2 and ni > 2:
+        nz[:, 0] = z[:, 1]  # a depth in both lists
+        nz[0, 1] = float("nan")
+    grid = DenseSDFGrid(24).to(DEV)
+    with torch.no_grad():
+        grid.grid.normal_(0.0, 0.3)
+    fn = grid.sdf_fn()
+    with torch.no_grad():
+        sdf = fn((to(o)[:, None, :] + to(d)[:, None, :] * to(z)[..., None]).reshape(-1, 3)).reshape(nr, n)
+        ref_fn = lambda p: fn(to(p)).cpu()
+        zr, sr = O.cat_z_vals(o, d, z, nz, sdf.cpu(), ref_fn, last=False)
+        zg, sg = cat_z_vals(to(o), to(d), to(z), to(nz), sdf, fn, last=False)
+        zl, sl = cat_z_vals(to(o), to(d), to(z), to(nz), sdf, fn, last=True)
+    assert torch.equal(torch.nan_to_num(zg.cpu(), nan=7.0), torch.nan_to_num(zr, nan=7.0))
+    assert torch.equal(torch.nan_to_num(sg.cpu(), nan=7.0), torch.nan_to_num(sr, nan=7.0))
+    assert torch.equal(torch.nan_to_num(zl.cpu(), nan=7.0), torch.nan_to_num(zr, nan=7.0)) and sl is sdf
+    assert bool(torch.isnan(zg[0]).any()) == (n > 2 and ni > 2) and (n < 3 or not bool(torch.isnan(zg[0, :-1]).any()))
+
+
 # ------------------------------------------------------------------ render forward / backward
 
 

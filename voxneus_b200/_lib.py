@@ -63,6 +63,7 @@ _PROTOS = {
     "vx_tensor_core_timeouts": [],
     "vx_huber_loss_blocks": [I64],
     "vx_huber_loss": [P, P, I64, F32, P, P, P, I64, P],
+    "vx_cat_z_vals": [P, P, P, P, I64, I32, I32, P, P, P],
     "vx_radiance_mlp_backward": [P, I64, I64, I32, I32, I32, P, P, P, P, P, P, P, P, P, P, P, P, P, I64, P],
     "vx_appearance_mlp_backward": [P, P, I32, I64, P, P, P, P, P, P, P, P, P, P, P, P, P, I64, P],
     "vx_composite_workspace_blocks": [I64],

@@ -376,6 +376,43 @@ __global__ void k_near_far(const float* __restrict__ o, const float* __restrict_
   }
 }
 
+// Total order of torch.sort on floats: ascending, -0 equal to +0, NaN after everything.
+__device__ __forceinline__ uint32_t sort_key(float v) {
+  if (v != v) return 0xffffffffu;
+  const uint32_t u = __float_as_uint(v == 0.0f ? 0.0f : v);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+
+// cat_z_vals (rendering/sampler.py:295-320): the ray's old and new depths concatenated and put in
+// ascending order, the SDF values carried along. One block per ray (grid-stride over rays): the
+// keys are staged in shared memory and every element finds its place by counting the smaller
+// keys, equal keys ranked by position in the concatenation (so a depth present in both lists keeps
+// the old value first; equal depths carry equal SDF values). Unsorted new depths are fine.
+__global__ void __launch_bounds__(128) k_cat_z_vals(const float* __restrict__ z_old, const float* __restrict__ z_new,
+                                                    const float* __restrict__ sdf_old,
+                                                    const float* __restrict__ sdf_new, int64_t n_rays, int n_old,
+                                                    int n_new, float* __restrict__ z_out, float* __restrict__ sdf_out) {
+  extern __shared__ uint32_t keys[];
+  const int n = n_old + n_new;
+  for (int64_t r = blockIdx.x; r < n_rays; r += gridDim.x) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x)
+      keys[i] = sort_key(i < n_old ? z_old[r * n_old + i] : z_new[r * n_new + (i - n_old)]);
+    __syncthreads();
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+      const uint32_t k = keys[i];
+      int rank = 0;
+      for (int j = 0; j < n; ++j) {
+        const uint32_t kj = keys[j];
+        rank += (kj < k) || (kj == k && j < i);
+      }
+      const bool old = i < n_old;
+      z_out[r * n + rank] = old ? z_old[r * n_old + i] : z_new[r * n_new + (i - n_old)];
+      if (sdf_out) sdf_out[r * n + rank] = old ? sdf_old[r * n_old + i] : sdf_new[r * n_new + (i - n_old)];
+    }
+    __syncthreads();
+  }
+}
+
 }  // namespace vx
 
 using namespace vx;
@@ -460,6 +497,22 @@ int vx_sample_pdf(const float* bins, const float* weights, const float* cdf, int
       bins, weights, cdf, n_rays, n_bins, n_samples, u, u_det, out, idx_out);
   count_launches(1);
   return check_launch("sample_pdf");
+}
+
+int vx_cat_z_vals(const float* z_old, const float* z_new, const float* sdf_old, const float* sdf_new, int64_t n_rays,
+                  int n_old, int n_new, float* z_out, float* sdf_out, void* stream) {
+  VX_REQUIRE(n_rays >= 0 && n_old >= 0 && n_new >= 0, "bad sizes");
+  VX_REQUIRE((int64_t)n_old + n_new <= 8192, "at most 8192 depths per ray");
+  if (n_rays == 0 || n_old + n_new == 0) return VX_OK;
+  VX_REQUIRE((z_old || n_old == 0) && (z_new || n_new == 0) && z_out, "null pointer");
+  VX_REQUIRE(!sdf_out || ((sdf_old || n_old == 0) && (sdf_new || n_new == 0)),
+             "carrying SDF values needs both lists' values");
+  const size_t smem = (size_t)(n_old + n_new) * sizeof(uint32_t);
+  k_cat_z_vals<<<grid_for(n_rays * 128, 128, 8), 128, smem, (cudaStream_t)stream>>>(z_old, z_new, sdf_old, sdf_new,
+                                                                                   n_rays, n_old, n_new, z_out,
+                                                                                   sdf_out);
+  count_launches(1);
+  return check_launch("cat_z_vals");
 }
 
 }  // extern "C"

@@ -338,6 +338,24 @@ def sample_pdf(bins, weights, n_samples, det=False, u=None, cdf=None, return_ind
     return (out, idx) if return_indices else out
 
 
+def cat_z_vals(z_old, z_new, sdf_old=None, sdf_new=None):
+    """Per ray: z_old (R, n) and z_new (R, m) concatenated and sorted as torch.sort orders them; the
+    SDF values (when given) carried with their depths. Returns (z, sdf or None)."""
+    zo = check_tensor(z_old.contiguous(), "z_vals")
+    zn = check_tensor(z_new.contiguous(), "new_z_vals", device=zo.device)
+    nr, n = zo.shape
+    m = zn.shape[1]
+    if zn.shape[0] != nr:
+        raise RuntimeError(f"new_z_vals has {zn.shape[0]} rays, z_vals {nr}")
+    carry = sdf_old is not None
+    so = check_tensor(sdf_old.reshape(nr, n).contiguous(), "sdf", device=zo.device) if carry else None
+    sn = check_tensor(sdf_new.reshape(nr, m).contiguous(), "new_sdf", device=zo.device) if carry else None
+    z = torch.empty(nr, n + m, device=zo.device)
+    sdf = torch.empty(nr, n + m, device=zo.device) if carry else None
+    call("vx_cat_z_vals", ptr(zo), ptr(zn), ptr(so), ptr(sn), nr, n, m, ptr(z), ptr(sdf), stream_ptr(zo.device))
+    return z, sdf
+
+
 # ------------------------------------------------------------------ render geometry -------
 
 

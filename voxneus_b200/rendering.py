@@ -34,15 +34,15 @@ def up_sample(rays_o, rays_d, z_vals, sdf, n_importance: int, inv_s: float, det:
 
 
 def cat_z_vals(rays_o, rays_d, z_vals, new_z_vals, sdf, sdf_fn, last: bool = False):
-    """Concatenate, sort and query (rendering/sampler.py:295-320)."""
-    nr, ns = z_vals.shape
-    ni = new_z_vals.shape[1]
-    z, order = torch.sort(torch.cat([z_vals, new_z_vals], dim=-1), dim=-1)
-    if not last:
-        pts = rays_o[:, None, :] + rays_d[:, None, :] * new_z_vals[..., :, None]
-        fnew = sdf_fn(pts.reshape(-1, 3)).reshape(nr, ni)
-        sdf = torch.gather(torch.cat([sdf, fnew], dim=-1), -1, order)
-    return z, sdf
+    """Concatenate, sort and query (rendering/sampler.py:295-320): the caller's sdf_fn evaluates the
+    new points (unless last), one kernel sorts the depths and carries the SDF values along."""
+    nr, ni = new_z_vals.shape
+    if last:
+        z, _ = ops.cat_z_vals(z_vals, new_z_vals)
+        return z, sdf
+    pts = rays_o[:, None, :] + rays_d[:, None, :] * new_z_vals[..., :, None]
+    fnew = sdf_fn(pts.reshape(-1, 3)).reshape(nr, ni)
+    return ops.cat_z_vals(z_vals, new_z_vals, sdf, fnew)
 
 
 class RaySampler(nn.Module):
