@@ -711,23 +711,29 @@ def _dir_strides(dirs: torch.Tensor, n_rays: int, n_samples: int):
     raise RuntimeError("ray_dirs must be (N,3) or (N,S,3)")
 
 
+def huber_loss(pred, target, delta, with_grad=True):
+    """(loss, dloss/dpred or None): the NeuS2 Huber colour loss and its gradient from one kernel."""
+    p = check_tensor(pred.detach().contiguous(), "pred")
+    t = check_tensor(target.detach().contiguous(), "target")
+    if p.shape != t.shape:
+        raise RuntimeError(f"pred {tuple(p.shape)} and target {tuple(t.shape)} differ")
+    n = p.numel()
+    nb = int(L.query("vx_huber_loss_blocks", n))
+    part = Scratch.get(p.device).partials_for(nb)
+    loss = torch.empty((), device=p.device)
+    grad = torch.empty_like(p) if with_grad else None
+    call("vx_huber_loss", ptr(p), ptr(t), n, float(delta), ptr(loss), ptr(grad), ptr(part), part.numel(),
+         stream_ptr(p.device))
+    return loss, grad
+
+
 class HuberLossFn(torch.autograd.Function):
     """NeuS2 Huber colour loss (rendering/volume_render.py:43-54): mean elementwise Huber of
     pred - target; the gradient is written by the same kernel and scaled in the backward."""
 
     @staticmethod
     def forward(ctx, pred, target, delta):
-        p = check_tensor(pred.detach().contiguous(), "pred")
-        t = check_tensor(target.detach().contiguous(), "target")
-        if p.shape != t.shape:
-            raise RuntimeError(f"pred {tuple(p.shape)} and target {tuple(t.shape)} differ")
-        n = p.numel()
-        nb = int(L.query("vx_huber_loss_blocks", n))
-        part = Scratch.get(p.device).partials_for(nb)
-        loss = torch.empty((), device=p.device)
-        grad = torch.empty_like(p) if ctx.needs_input_grad[0] else None
-        call("vx_huber_loss", ptr(p), ptr(t), n, float(delta), ptr(loss), ptr(grad), ptr(part), part.numel(),
-             stream_ptr(p.device))
+        loss, grad = huber_loss(pred, target, delta, ctx.needs_input_grad[0])
         ctx.grad = grad
         ctx.shape = pred.shape
         return loss

@@ -25,7 +25,7 @@ from torch.optim import Optimizer
 
 from . import ops
 from .models import VoxNeuS
-from .rendering import RaySampler, compute_huber_color_loss
+from .rendering import RaySampler
 
 
 def amplify_s_gradient(variance_param: torch.nn.Parameter, k: float = 5.0) -> bool:
@@ -236,8 +236,10 @@ class FusedTrainer:
             out = m.render(rays_o, rays_d, self.sampler, None, None, up_sample_steps=self.up_sample_steps,
                            sphere_radius=1.0, randoms=randoms, vr_bitmap=self.bitmap, extras=False,
                            amplify_k=0.0 if ex is not None else amp_k, amp_flag=self.amp_flag, z_vals=z_vals)
-            loss = compute_huber_color_loss(out["rgb"], target, self.huber_delta)
-            loss.backward()
+            # the loss kernel writes dL/drgb beside the loss: the backward starts from it directly
+            # (the same values as loss.backward(), without the seed fill and the scale by 1)
+            loss, d_rgb = ops.huber_loss(out["rgb"], target, self.huber_delta)
+            out["rgb"].backward(d_rgb)
         if ex is not None:
             flag = ex.exchange(list(m.parameters()), self.bitmap, m.variance_net.variance, amp_k)
             if flag is not None:
