@@ -169,7 +169,9 @@ int vx_hash_encode_backward(float* table_grad, int n_levels, int log2_size, int 
   a.P = n_points;
   a.d_out = d_out;
   a.ld_d = ld_d;
-  k_hash_bwd<<<grid_for(n_points * 4, 256), 256, 0, (cudaStream_t)stream>>>(a);
+  // 32 blocks a SM (4 resident): more, shorter blocks keep the atomics' tail short (0.118 ->
+  // 0.111 ms at 1M samples against 16)
+  k_hash_bwd<<<grid_for(n_points * 4, 256, 32), 256, 0, (cudaStream_t)stream>>>(a);
   count_launches(1);
   return check_launch("hash_encode_backward");
 }

@@ -457,7 +457,9 @@ int vx_sample_multistep(const float* grid, const int32_t res[3], const float xyz
   Occ oc = make_occ(occupancy, occ_res, occ_min, occ_max);
   const int threads = 128;
   const size_t smem = (size_t)(threads / 32) * (6 * total + 64) * sizeof(float);
-  k_sample_multistep<<<grid_for(n_rays * 32, threads, 9), threads, smem, (cudaStream_t)stream>>>(a, grid, g, oc);
+  // a warp per ray up to 64 blocks a SM (9 are resident): one wave of persistent warps left some
+  // warps two rays and others one; the block scheduler balances single-ray warps better
+  k_sample_multistep<<<grid_for(n_rays * 32, threads, 64), threads, smem, (cudaStream_t)stream>>>(a, grid, g, oc);
   count_launches(1);
   return check_launch("sample_multistep");
 }
