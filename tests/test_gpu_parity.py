@@ -1004,6 +1004,43 @@ def test_radiance_mlp_module_on_the_fused_kernels():
         mlp(hd, to(v).requires_grad_(True), nd)
 
 
+@pytest.mark.parametrize("res,offset", [((64, 48, 80), 0), ((37, 41, 29), 0), ((64, 48, 80), 1)])
+def test_geometry_forward_matches_field_query_bitwise(res, offset):
+    """The render geometry forward (positions o + d*t from rays and midpoints) and the field query
+    (the same positions given as points) give the same bits: SDF, Eq.7 gradient and normal, for rays
+    crossing the whole box (border cells with their one-sided differences included), odd row
+    lengths, and a grid view 4 bytes off 16-byte alignment."""
+    from voxneus_b200 import ops
+
+    torch.manual_seed(41 + offset)
+    n_vox = res[0] * res[1] * res[2]
+    store = torch.randn(n_vox + 4, device=DEV) * 0.3
+    grid = store[offset:offset + n_vox].view(1, 1, *res)
+    lo, hi = (-1.0, -0.8, -1.2), (1.0, 0.9, 1.1)
+    nr, ns = 300, 128
+    o = torch.randn(nr, 3)
+    o = 2.5 * o / o.norm(dim=-1, keepdim=True)
+    d = -o / o.norm(dim=-1, keepdim=True) + 0.2 * torch.randn(nr, 3)
+    d = d / d.norm(dim=-1, keepdim=True)
+    mid = torch.sort(torch.rand(nr, ns) * 4.0 + 0.5, dim=-1).values
+    od, dd, md = to(o), to(d), to(mid)
+    sdf = torch.empty(nr, ns, device=DEV)
+    nrm = torch.empty(nr, ns, 3, device=DEV)
+    gr = torch.empty(nr, ns, 3, device=DEV)
+    ops.call("vx_render_geometry_forward", ops.ptr(grid), ops.i3(res), ops.f3(lo), ops.f3(hi), ops.ptr(od),
+             ops.ptr(dd), ops.ptr(md), nr, ns, ops.ptr(sdf), ops.ptr(nrm), ops.ptr(gr), None, ops.stream_ptr(DEV))
+    pts = (od[:, None, :] + dd[:, None, :] * md[..., None]).reshape(-1, 3).contiguous()
+    f_sdf = torch.empty(nr * ns, device=DEV)
+    f_nrm = torch.empty(nr * ns, 3, device=DEV)
+    f_gr = torch.empty(nr * ns, 3, device=DEV)
+    ops.call("vx_field_query", ops.ptr(grid), ops.i3(res), ops.f3(lo), ops.f3(hi), ops.ptr(pts), nr * ns,
+             ops.ptr(f_sdf), ops.ptr(f_gr), ops.ptr(f_nrm), None, None, ops.stream_ptr(DEV))
+    torch.cuda.synchronize()
+    assert torch.equal(sdf.reshape(-1), f_sdf)
+    assert torch.equal(gr.reshape(-1, 3), f_gr)
+    assert torch.equal(nrm.reshape(-1, 3), f_nrm)
+
+
 def test_field_query_at_512():
     """The large-grid field query workload (512^3 grid of 32 Gaussian-bump spheres): 2^20 scattered
     points through the Morton-sorted path equal the unsorted kernel bit for bit; a subset of them
