@@ -269,7 +269,8 @@ int vx_radiance_mlp_forward(const float* x, int64_t ldx, int64_t n_points, int i
  * the 51-64-3 MLP; writes colors (n,3) and, when rows is given, the MLP input rows (row stride
  * ld_rows >= 52, multiple of 4, 16-byte aligned; the adjoint's input). ld_rows == 36 stores the
  * compact rows of vx_appearance_mlp_backward instead: [hash 32 | normal 3 | pad], without the 16
- * SH(d) columns, which the adjoint recomputes from rays_d. */
+ * SH(d) columns, which the MLP takes from rays_d (folded into a per-ray hidden bias when n_samples
+ * is a multiple of 128, as vx_appearance_mlp_backward describes). */
 int vx_appearance_mlp_forward(const float* table, int n_levels, int log2_size, int n_features,
                               const int32_t* level_res, const float* level_weights, const float* rays_o,
                               const float* rays_d, const float* mid, int n_samples, const float xyz_min[3],
@@ -322,10 +323,15 @@ int vx_radiance_mlp_backward(const float* x, int64_t ldx, int64_t n_points, int 
                              float* db1, float* partials, int64_t n_partial_floats, void* stream);
 
 /* The adjoint of the fused appearance path on its compact rows: n_points rows of 36 floats
- * [hash 32 | normal 3 | pad] (16-byte aligned, contiguous) whose SH(d) features are recomputed from
- * rays_d of the sample's ray (sample i belongs to ray i / n_samples): the 16 columns of a full row
- * that depend on the ray only (models/embedder.py:55-87). Outputs and partials as
- * vx_radiance_mlp_backward (the same bits as it gives on the full rows). */
+ * [hash 32 | normal 3 | pad] (16-byte aligned, contiguous) whose SH(d) features come from rays_d
+ * of the sample's ray (sample i belongs to ray i / n_samples): the 16 columns of a full row that
+ * depend on the ray only (models/embedder.py:55-87). Outputs and partials as
+ * vx_radiance_mlp_backward. When n_samples is a multiple of 128 (every 128-sample tile inside one
+ * ray: the training and serving shapes) the MLP is folded: SH(d) enters as a per-ray bias of the
+ * hidden layer (b0 + W0[:, 32:48] SH(d)) and the SH columns of dW0 come from per-tile column sums
+ * of dL/dz, so the results agree with the full rows within FP32 rounding; otherwise SH(d) is
+ * rebuilt per sample and they are the same bits. vx_appearance_mlp_forward folds on the same
+ * condition. */
 int vx_appearance_mlp_backward(const float* rows, const float* rays_d, int n_samples, int64_t n_points,
                                const float* W0, const float* b0, const float* W1, const float* b1,
                                const float* d_colors, const float* colors, float* d_hash, float* d_normal, float* dW0,

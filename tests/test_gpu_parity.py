@@ -672,12 +672,16 @@ def test_chunked_inference_appearance_matches_rows_path():
         _lib.call("vx_appearance_mlp_forward_chunked", *head, P(fused), P(small), ns - 1, st)
 
 
-@pytest.mark.parametrize("nr,ns", [(397, 127), (64, 128), (3, 1)])
+@pytest.mark.parametrize("nr,ns", [(397, 127), (3, 1), (64, 128), (5, 256)])
 def test_compact_rows_match_full_rows(nr, ns):
-    """The compact rows [hash 32 | normal 3 | pad] of the training path, whose SH(d) the MLP kernels
-    recompute from the ray direction, give the same bits as the full 52-float rows: the stored
-    hash and normal columns, the colours, and every output of the adjoint (hash and normal
-    cotangents, weight and bias gradients). Ragged sizes: a partial last tile, one sample a ray."""
+    """The compact rows [hash 32 | normal 3 | pad] of the training path against the full 52-float
+    rows [hash | SH | normal | pad]: the stored hash and normal columns are the same bits. Where the
+    samples of a ray do not fill whole 128-row tiles (127, 1), the MLP kernels rebuild SH(d) in the
+    staging and the colours and every adjoint output are the same bits; where they do (128, 256),
+    the folded MLP adds SH(d) as a per-ray bias of the hidden layer and takes the SH columns of dW0
+    from per-tile column sums, so the results agree within FP32 rounding: colours to 1e-6, weight
+    gradients to 1e-5 of their scale, the per-sample cotangents to 1e-5 of scale on samples whose
+    hidden pre-activations are all clear of zero (a ReLU at |z| < 1e-5 may switch)."""
     from voxneus_b200 import _lib, ops
 
     torch.manual_seed(23 + nr)
@@ -703,13 +707,27 @@ def test_compact_rows_match_full_rows(nr, ns):
     _lib.call("vx_appearance_mlp_forward", *head, P(c_compact), P(compact), 36, st)
     torch.cuda.synchronize()
     assert torch.equal(compact[:, :32], full[:, :32]) and torch.equal(compact[:, 32:35], full[:, 48:51])
-    assert torch.equal(c_compact, c_full)
+    folded = ns % 128 == 0
+    if folded:
+        assert float((c_compact - c_full).abs().max()) <= 1e-6
+    else:
+        assert torch.equal(c_compact, c_full)
     g = to(torch.randn(p, 3) * 0.1)
+    z = full[:, :51].double() @ wd[0].double().t() + wd[1].double()
+    clear = (z.abs().min(dim=1).values > 1e-5).cpu()
+    assert float(clear.double().mean()) > 0.99
     for colors in (None, c_full):
         a = ops.mlp_backward(full[:, :51], *wd, g, colors)
         b = ops.mlp_backward(compact, *wd, g, colors, dd, ns)
         for name, x, y in zip(("d_hash", "d_normal", "dW0", "db0", "dW1", "db1"), a, b):
-            assert torch.equal(x, y), name
+            if not folded:
+                assert torch.equal(x, y), name
+                continue
+            x, y = x.cpu(), y.cpu()
+            if name in ("d_hash", "d_normal"):
+                x, y = x[clear], y[clear]
+            scale = max(float(x.abs().max()), 1e-30)
+            assert float((x - y).abs().max()) <= 1e-5 * scale, (name, float((x - y).abs().max()), scale)
     with pytest.raises(RuntimeError, match="compact MLP rows"):
         ops.mlp_backward(full[:, :36], *wd, g, None, dd, ns)
 

@@ -108,6 +108,27 @@ struct MlpW {
   const float* b1;  // (3)
 };
 
+// The folded MLP (compact rows whose 128-row tiles each lie inside one ray, so SH(d) is constant
+// over a tile): the 16 SH columns leave the contraction and become a per-ray bias of the hidden
+// layer, b0 + W0[:, 32:48] SH(d). Its input features are [hash 32 | normal 3 | one | 0 x 4], K = 40.
+// Folded feature k comes from column fold_col(k) of W0 (-1: none).
+__device__ __forceinline__ int fold_col(int k) { return k < 32 ? k : (k < 35 ? 48 + (k - 32) : -1); }
+
+// The per-ray bias of hidden unit n: b0[n] + sum_k W0[n, 32 + k] sh[k], k = 0..15 in order (the
+// forward and the adjoint evaluate it identically, so the adjoint's recomputed hidden layer has
+// the forward's bits).
+__device__ __forceinline__ float fold_bias(const MlpW& w, int n, const float sh[16]) {
+  float b = __ldg(w.b0 + n);
+#pragma unroll
+  for (int k = 0; k < 16; ++k) b = fmaf(__ldg(w.W0 + n * KIN + 32 + k), sh[k], b);
+  return b;
+}
+
+// SH(d) of ray r.
+__device__ __forceinline__ void ray_sh(const float* __restrict__ rays_d, int64_t r, float sh[16]) {
+  sh16(__ldg(rays_d + 3 * r), __ldg(rays_d + 3 * r + 1), __ldg(rays_d + 3 * r + 2), sh);
+}
+
 __device__ __forceinline__ uint32_t x_off(int f, int m) { return (uint32_t)((f * 16 + (m >> 3)) * 128 + (m & 7) * 16); }
 // row r of [W_hi; W_lo] (r < 64: hi of hidden unit r, else lo of hidden unit r - 64), feature k
 __device__ __forceinline__ uint32_t w_off(int r, int k) {
@@ -407,7 +428,11 @@ constexpr size_t kFwdSmem = 2 * kXBytes + kWBytes + sizeof(float) * (NH + NO * N
 // rows at a time.
 constexpr uint32_t kFwdSlotBytes = kXBytes + TM * KP * 4 + 2 * TM * 4 * 4;  // XL, rows, RED
 // shared head: W0 [hi; lo], b0, W1, b1, barriers, TMEM address, fail flags; slots from a 1 KB boundary
-constexpr size_t kFwd2Head = 1024 * ((kWBytes + sizeof(float) * (NH + NO * NH + 4) + 64 + 1023) / 1024);
+constexpr size_t kFwd2Head =
+    1024 * ((kWBytes + sizeof(float) * (NH + NO * NH + 4) + 64 + 2 * NH * sizeof(float) + 1023) / 1024);
+// the folded MLP's per-ray hidden bias of each slot's tile: the last 2 x 64 floats of the head
+constexpr size_t kFwd2Beta = kFwd2Head - 2 * NH * sizeof(float);
+static_assert(kFwd2Beta >= kWBytes + sizeof(float) * (NH + NO * NH + 4) + 64, "forward head overlaps its bias");
 constexpr size_t kFwd2Smem = kFwd2Head + 2 * (size_t)kFwdSlotBytes;
 // one CTA per SM (it allocates all 512 TMEM columns): two would need <= 116 KB each
 static_assert(kFwd2Smem > 116 * 1024, "two forward CTAs would fit on an SM and contend for TMEM");
@@ -416,9 +441,10 @@ __device__ __forceinline__ void slot_sync(int slot) {
   asm volatile("bar.sync %0, 256;" ::"r"(1 + slot) : "memory");
 }
 
-template <bool kCustomWait, bool kCompact>
+template <bool kCustomWait, bool kCompact, bool kFold>
 __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restrict__ X, int64_t P, MlpW w,
                                                          float* __restrict__ colors, TcGuard g, RowSrc src) {
+  static_assert(!kFold || kCompact, "the folded MLP reads compact rows");
   constexpr int kLd = kCompact ? KC : KP;  // floats per row in global memory
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t wait_limit = kCustomWait ? g.limit : kWaitLimit;
@@ -433,6 +459,7 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
   const int wid = stid >> 5, lane = tid & 31, q = wid & 3, hh = wid >> 2;
   const int m = 32 * q + lane;  // this thread's sample in its slot's tile
   uint8_t* SL = smem + kFwd2Head + (size_t)slot * kFwdSlotBytes;
+  float* BETA = reinterpret_cast<float*>(smem + kFwd2Beta) + NH * slot;  // kFold: this slot's tile's bias
   uint8_t* XL = SL;
   uint8_t* ROWS = XL + kXBytes;
   float* RED = reinterpret_cast<float*>(ROWS + TM * KP * 4);  // [2][TM][4]
@@ -441,8 +468,9 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
   // weights and each slot's X_lo feature chunks 13..15 (zero), by all 512 threads
   for (int e = tid; e < NH * 64; e += blockDim.x) {
     const int n = e >> 6, k = e & 63;
+    const int col = kFold ? fold_col(k) : (k < KIN ? k : -1);
     float h, l;
-    tc::split_tf32(k < KIN ? w.W0[n * KIN + k] : 0.0f, h, l);
+    tc::split_tf32(col >= 0 ? w.W0[n * KIN + col] : 0.0f, h, l);
     *reinterpret_cast<float*>(W2 + w_off(n, k)) = h;
     *reinterpret_cast<float*>(W2 + w_off(NH + n, k)) = l;
   }
@@ -481,6 +509,13 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
     rows_pending = true;
   }
   uint32_t phase = 0, rphase = 0;
+  float dnx = 0.0f, dny = 0.0f, dnz = 0.0f;  // kFold, threads 0..63: this tile's ray direction
+  if (kFold && stid < NH && t0 < ntiles) {
+    const int64_t r = t0 * TM / src.S;
+    dnx = __ldg(src.rays_d + 3 * r);
+    dny = __ldg(src.rays_d + 3 * r + 1);
+    dnz = __ldg(src.rays_d + 3 * r + 2);
+  }
   for (int64_t t = t0; t < ntiles; t += tstride) {
     const int64_t m0 = t * TM;
     const bool valid = m0 + m < P;
@@ -490,7 +525,32 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
     slot_sync(slot);
     if (s_fail[slot]) break;
     if (stid == 0) rows_pending = false;
-    {  // rows -> X_hi (TMEM) and X_lo (sample rows); column 51 zero (the padding column may hold anything)
+    if constexpr (kFold) {  // rows -> X_hi / X_lo: [hash 32 | normal 3 | 0 | 0 x 4]
+      const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * (kLd * 4));
+      const int c0 = hh ? 5 : 0;
+      float xh[20];  // features 4*c0 .. 4*c0 + 19
+#pragma unroll
+      for (int j = 0; j < 5; ++j) {
+        const int c = c0 + j;
+        float4 u = (valid && c < 9) ? rrow[c] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (c == 8) u.w = 0.0f;
+        const float v[4] = {u.x, u.y, u.z, u.w};
+        float lo[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) tc::split_tf32(v[i], xh[4 * j + i], lo[i]);
+        *reinterpret_cast<float4*>(XL + x_off(c, m)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+      }
+      const uint32_t ta = acol + lane_base + 4 * c0;  // stores aligned to their widths
+      if (hh == 0) {
+        tc::tmem_st16(ta, xh);
+        tc::tmem_st4(ta + 16, xh + 16);
+      } else {
+        tc::tmem_st4(ta, xh);
+        tc::tmem_st8(ta + 4, xh + 4);
+        tc::tmem_st8(ta + 12, xh + 12);
+      }
+      tc::tmem_wait_st();
+    } else {  // rows -> X_hi (TMEM) and X_lo (sample rows); column 51 zero (the padding column may hold anything)
       const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * (kLd * 4));
       const int c0 = hh ? 7 : 0;
       const float3 dir = stage_dir<kCompact>(src, m0 + m, valid && hh);
@@ -529,13 +589,24 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
     slot_sync(slot);
     if (stid == 0) {
       tc::fence_after_sync();
-      issue_split_ts(tcol, acol, xl, w2, 7);
+      issue_split_ts(tcol, acol, xl, w2, kFold ? 5 : 7);
       tc::commit(bar);
       if (t + tstride < ntiles) {  // ROWS has been read: bring this slot's next tile
         fetch_rows(t + tstride);
         rows_pending = true;
         rows_parity = rphase;
       }
+    }
+    if (kFold && stid < NH) {  // the tile's hidden bias, while its MMA runs (read after the wait)
+      float sh[16];
+      sh16(dnx, dny, dnz, sh);
+      if (t + tstride < ntiles) {  // the direction of the slot's next tile's ray, a tile ahead
+        const int64_t r = (t + tstride) * TM / src.S;
+        dnx = __ldg(src.rays_d + 3 * r);
+        dny = __ldg(src.rays_d + 3 * r + 1);
+        dnz = __ldg(src.rays_d + 3 * r + 2);
+      }
+      BETA[stid] = fold_bias(w, stid, sh);
     }
     const bool ok = tc::mbar_wait(bar, phase, wait_limit);
     phase ^= 1u;
@@ -549,7 +620,7 @@ __global__ void __launch_bounds__(512, 1) k_mlp_fwd_rows2(const float* __restric
     float z[32];
     tmem_ld_sum32(tcol + lane_base + 32 * hh, z);
     float p0, p1, p2;
-    colour_partial(z, hh, B0, W1s, p0, p1, p2);
+    colour_partial(z, hh, kFold ? BETA : B0, W1s, p0, p1, p2);
     float* r = RED + (hh * TM + m) * 4;
     r[0] = p0;
     r[1] = p1;
@@ -611,12 +682,13 @@ __device__ __forceinline__ uint32_t wt_off(int f, int n) {
 // shared memory through one bulk copy issued as soon as the previous tile has been staged, so no
 // registers or load instructions are spent on the prefetch. Otherwise the rows are prefetched
 // into registers during the previous tile.
-template <bool kBulk, bool kCustomWait, bool kCompact>
+template <bool kBulk, bool kCustomWait, bool kCompact, bool kFold>
 __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__ X, int64_t ldx, int xvec, int64_t P,
                                                       MlpW w, const float* __restrict__ d_out,
                                                       const float* __restrict__ y_in,
                                                       float* __restrict__ d_hash, float* __restrict__ d_normal,
                                                       float* __restrict__ partials, TcGuard g, RowSrc src) {
+  static_assert(!kFold || (kCompact && kBulk), "the folded MLP reads compact rows by bulk copy");
   constexpr uint32_t kRowB = (kCompact ? KC : KP) * 4;  // bytes per row in global and shared memory
   extern __shared__ __align__(1024) uint8_t smem[];
   const uint32_t wait_limit = kCustomWait ? g.limit : kWaitLimit;
@@ -625,30 +697,45 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   uint8_t* XT2 = WT2 + kWBytes;
   uint8_t* R1 = XT2 + kXtBytes;
   uint8_t* ROWS = R1 + kR1Bytes;  // kBulk only
-  float* RED = reinterpret_cast<float*>(ROWS + (kBulk ? kRowsBytes : 0));  // [2][TM][4]
+  float* RED = reinterpret_cast<float*>(ROWS + (kBulk ? TM * kRowB : 0));  // [2][TM][4]
   float* W1s = RED + 2 * TM * 4;
   float* B0 = W1s + NO * NH;
   float* B1 = B0 + NH;
   uint64_t* bar = reinterpret_cast<uint64_t*>(B1 + 4);
   uint64_t* bar_rows = bar + 1;
   uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bar + 2);
+  // kFold: the SH columns of dW0, [16][128]: one column per TMEM lane of DZ^T (hidden unit hi
+  // parts in lanes 0..63, lo parts in 64..127; lanes consecutive, so a warp's accesses are
+  // conflict-free); the tile's hidden bias (read as float4: 16-byte aligned)
+  // and the SH(d) of the last two tiles. The dynamic shared memory starts 1024-byte aligned, so aligning the address aligns
+  // the offset.
+  float* SHACC = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(bar) + 24 + 15) & ~uintptr_t(15));
+  float* BETA = SHACC + TM * 16;  // [2][64]: tiles by parity
+  float* SHT = BETA + 2 * NH;     // [2][16]
   const int tid = threadIdx.x, wid = tid >> 5, lane = tid & 31, q = wid & 3, hh = wid >> 2;
   const int m = 32 * q + lane;  // this thread's sample in the tile (its TMEM lane)
   // W0 [hi; lo] (hidden rows) for Z, W0^T [hi; lo] (feature rows) for dX, b0, W1, b1; X^T feature
   // rows 52..63 (hi and lo) zero
   for (int e = tid; e < NH * 64; e += blockDim.x) {
     const int n = e >> 6, k = e & 63;
+    const int col = kFold ? fold_col(k) : (k < KIN ? k : -1);
     float h, l;
-    tc::split_tf32(k < KIN ? w.W0[n * KIN + k] : 0.0f, h, l);
+    tc::split_tf32(col >= 0 ? w.W0[n * KIN + col] : 0.0f, h, l);
     *reinterpret_cast<float*>(W2 + w_off(n, k)) = h;
     *reinterpret_cast<float*>(W2 + w_off(NH + n, k)) = l;
     *reinterpret_cast<float*>(WT2 + wt_off(k, n)) = h;
     *reinterpret_cast<float*>(WT2 + wt_off(64 + k, n)) = l;
   }
-  for (int e = tid; e < 12 * TM; e += blockDim.x) {
-    *reinterpret_cast<float*>(XT2 + xt_off(52 + e / TM, e % TM)) = 0.0f;
-    *reinterpret_cast<float*>(XT2 + xt_off(64 + 52 + e / TM, e % TM)) = 0.0f;
+  constexpr int kXtZero = kFold ? 36 : 52;  // X^T feature rows never written by the tiles
+  for (int e = tid; e < (64 - kXtZero) * TM; e += blockDim.x) {
+    *reinterpret_cast<float*>(XT2 + xt_off(kXtZero + e / TM, e % TM)) = 0.0f;
+    *reinterpret_cast<float*>(XT2 + xt_off(64 + kXtZero + e / TM, e % TM)) = 0.0f;
   }
+  if (kFold && hh == 1) {
+#pragma unroll
+    for (int k = 0; k < 16; ++k) SHACC[k * TM + m] = 0.0f;
+  }
+
   for (int i = tid; i < NH; i += blockDim.x) B0[i] = w.b0[i];
   for (int i = tid; i < NO * NH; i += blockDim.x) W1s[i] = w.W1[i];
   if (tid < NO) B1[tid] = w.b1[tid];
@@ -663,6 +750,33 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   const uint32_t tbase = *s_taddr;
   const uint32_t lane_base = (uint32_t)(32 * q) << 16;
   const uint32_t w2 = tc::smem_u32(W2), wt2 = tc::smem_u32(WT2), xt2 = tc::smem_u32(XT2), r1 = tc::smem_u32(R1);
+  float ones_prev = 0.0f;  // kFold: this lane's ones column of dW0 after the previous tile
+  int it = 0;              // tiles this block has completed
+  // kFold, warps 4..7 (lanes 0..127 = the rows of DZ^T): the SH columns of dW0 from a completed
+  // tile: its column sum of dL/dz (its growth of the ones column, feature 35 of the X_hi product;
+  // lane m is hidden unit m % 64, hi or lo part) times its SH(d)
+  auto fold_sh_columns = [&](const float* sht) {
+    float v[4];
+    tc::tmem_ld4(tbase + lane_base + 128 + 32, v);
+    tc::tmem_wait_ld();
+    const float sum = v[3] - ones_prev;
+    ones_prev = v[3];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) SHACC[k * TM + m] = fmaf(sum, sht[k], SHACC[k * TM + m]);
+  };
+  // kFold, threads 0..63: the hidden bias and (thread 0) the SH(d) of tile `tile` into buffer
+  // `buf`, a tile ahead (the global loads overlap the previous tile's dW0 MMAs)
+  auto fold_prepare = [&](int64_t tile, int buf) {
+    if (tid < NH) {
+      float sh[16];
+      ray_sh(src.rays_d, tile * TM / src.S, sh);
+      BETA[NH * buf + tid] = fold_bias(w, tid, sh);
+      if (tid == 0) {
+#pragma unroll
+        for (int k = 0; k < 16; ++k) SHT[16 * buf + k] = sh[k];
+      }
+    }
+  };
   const int64_t ntiles = (P + TM - 1) / TM;
   // rows of tile t into ROWS (kBulk): one copy of the tile's valid rows, issued by thread 0
   auto fetch_rows = [&](int64_t t) {
@@ -698,6 +812,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   float dy[NO], yv[NO] = {0.0f, 0.0f, 0.0f};  // dL/dcolour and (y_in) the forward's colour of this sample
   if ((int64_t)blockIdx.x < ntiles) {
     const int64_t m0 = (int64_t)blockIdx.x * TM;
+    if (kFold) fold_prepare(blockIdx.x, 0);
     if (!kBulk) load_row_chunks(X, ldx, xvec != 0, P, m0, m, hh, pre);
 #pragma unroll
     for (int c = 0; c < NO; ++c) {
@@ -718,8 +833,39 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
       if (tid == 0) rows_pending = false;
     }
     // rows -> X_hi (TMEM, sample lanes), X_lo (sample rows, R1) and X^T (feature rows); column 51
-    // = 1 on real rows (db0)
-    {
+    // (folded: 35) = 1 on real rows (db0)
+    if constexpr (kFold) {
+      const int c0 = hh ? 5 : 0;
+      const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * kRowB);
+      float xh[20];  // features 4*c0 .. 4*c0 + 19: [hash 32 | normal 3 | one | 0 x 4]
+#pragma unroll
+      for (int jc = 0; jc < 5; ++jc) {
+        const int c = c0 + jc;
+        float4 u = (valid && c < 9) ? rrow[c] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (c == 8) u.w = valid ? 1.0f : 0.0f;
+        const float v[4] = {u.x, u.y, u.z, u.w};
+        float lo[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+          tc::split_tf32(v[i], xh[4 * jc + i], lo[i]);
+          if (c < 9) {
+            *reinterpret_cast<float*>(XT2 + xt_off(4 * c + i, m)) = xh[4 * jc + i];
+            *reinterpret_cast<float*>(XT2 + xt_off(64 + 4 * c + i, m)) = lo[i];
+          }
+        }
+        *reinterpret_cast<float4*>(R1 + kXBytes + x_off(c, m)) = make_float4(lo[0], lo[1], lo[2], lo[3]);
+      }
+      const uint32_t ta = tbase + lane_base + kAhiCol + 4 * c0;  // stores aligned to their widths
+      if (hh == 0) {
+        tc::tmem_st16(ta, xh);
+        tc::tmem_st4(ta + 16, xh + 16);
+      } else {
+        tc::tmem_st4(ta, xh);
+        tc::tmem_st8(ta + 4, xh + 4);
+        tc::tmem_st8(ta + 12, xh + 12);
+      }
+      tc::tmem_wait_st();
+    } else {
       const int c0 = hh ? 7 : 0;
       const float4* rrow = reinterpret_cast<const float4*>(ROWS + m * kRowB);
       const float3 dir = stage_dir<kCompact>(src, m0 + m, valid && hh);
@@ -767,7 +913,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     __syncthreads();
     if (tid == 0) {
       tc::fence_after_sync();
-      issue_split_ts(tbase, tbase + kAhiCol, r1 + kXBytes, w2, 7);
+      issue_split_ts(tbase, tbase + kAhiCol, r1 + kXBytes, w2, kFold ? 5 : 7);
       tc::commit(bar);
       if (kBulk && t + gridDim.x < ntiles) {  // ROWS has been read: bring the next tile's rows
         fetch_rows(t + gridDim.x);
@@ -775,6 +921,8 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
         rows_parity = rphase;
       }
     }
+    // while the Z MMA runs: the previous tile's SH columns of dW0
+    if (kFold && hh == 1 && it > 0) fold_sh_columns(SHT + 16 * ((it - 1) & 1));
     bool ok = tc::mbar_wait(bar, phase, wait_limit);
     phase ^= 1u;
     if (__syncthreads_or(!ok)) {
@@ -792,7 +940,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     } else {     // block-uniform branch: every thread takes the same side of the barrier
       {
         float p0, p1, p2;
-        colour_partial(z, hh, B0, W1s, p0, p1, p2);
+        colour_partial(z, hh, kFold ? BETA + NH * (it & 1) : B0, W1s, p0, p1, p2);
         float* r = RED + (hh * TM + m) * 4;
         r[0] = p0;
         r[1] = p1;
@@ -813,7 +961,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     // dW1 (TMEM accumulators), dL/dz (kept in z), then DZ: the Z MMA has read X
 #pragma unroll
     for (int j4 = 0; j4 < 8; ++j4) {
-      const float4 b = *reinterpret_cast<const float4*>(B0 + 32 * hh + 4 * j4);
+      const float4 b = *reinterpret_cast<const float4*>((kFold ? BETA + NH * (it & 1) : B0) + 32 * hh + 4 * j4);
       z[4 * j4] += b.x;
       z[4 * j4 + 1] += b.y;
       z[4 * j4 + 2] += b.z;
@@ -899,6 +1047,7 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     // next tile's rows fly during the dW0 MMAs and the dX readout
     if (t + gridDim.x < ntiles) {
       const int64_t mn = (t + gridDim.x) * TM;
+      if (kFold) fold_prepare(t + gridDim.x, (it + 1) & 1);
       if (!kBulk) load_row_chunks(X, ldx, xvec != 0, P, mn, m, hh, pre);
 #pragma unroll
       for (int c = 0; c < NO; ++c) {
@@ -917,8 +1066,9 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
       }
     } else {
       float v[4], u[4];
-      tc::tmem_ld4(tbase + lane_base + 48, v);
-      tc::tmem_ld4(tbase + lane_base + 64 + 48, u);
+      constexpr int kNrmCol = kFold ? 32 : 48;  // the normal's feature columns
+      tc::tmem_ld4(tbase + lane_base + kNrmCol, v);
+      tc::tmem_ld4(tbase + lane_base + 64 + kNrmCol, u);
       tc::tmem_wait_ld();
       if (valid) {
         v[0] += u[0];
@@ -938,7 +1088,9 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
       break;
     }
     tc::fence_after_sync();
+    ++it;
   }
+  if (kFold && hh == 1 && it > 0 && !failed) fold_sh_columns(SHT + 16 * ((it - 1) & 1));  // the last tile's
   if (failed && tid == 0) {
     // the MMAs and a rows copy may still run: let them finish (bounded) before tensor memory is
     // read and freed and the block leaves
@@ -984,8 +1136,19 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
     for (int j = 0; j < 32; ++j) {
       const int col = 32 * hh + j;
       const float val = have ? (v1[j] + v2[j]) + R2[m * 64 + col] : 0.0f;
-      if (col < KP) pb[m * KP + col] = val;
-      if (col == KIN) pb[NH * KP + NO * NH + m] = val;  // ones column: db0
+      if (kFold) {  // folded feature col -> the column of W0 it came from; 35 is the ones column
+        const int oc = fold_col(col);
+        if (oc >= 0) pb[m * KP + oc] = val;
+        if (col == 35) pb[NH * KP + NO * NH + m] = val;
+      } else {
+        if (col < KP) pb[m * KP + col] = val;
+        if (col == KIN) pb[NH * KP + NO * NH + m] = val;  // ones column: db0
+      }
+    }
+    if (kFold && hh == 0) {  // the SH columns 32..47 (hi + lo lanes) and the padding column
+#pragma unroll
+      for (int k = 0; k < 16; ++k) pb[m * KP + 32 + k] = have ? SHACC[k * TM + m] + SHACC[k * TM + 64 + m] : 0.0f;
+      pb[m * KP + KIN] = 0.0f;
     }
   }
   if (tid < NO * NH) {
@@ -1008,6 +1171,11 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
 
 constexpr size_t kBwdSmemRegs = 2 * kWBytes + kXtBytes + kR1Bytes + sizeof(float) * (2 * TM * 4 + NO * NH + NH + 4) + 24;
 constexpr size_t kBwdSmemBulk = kBwdSmemRegs + kRowsBytes;
+constexpr size_t kBwdSmemCompact = kBwdSmemRegs + TM * KC * 4;
+// SHACC, BETA, SHT after the compact layout, from the next 16-byte boundary (BETA is read as float4)
+constexpr size_t kBwdSmemFold = (kBwdSmemCompact + 15) / 16 * 16 + sizeof(float) * (TM * 16 + 2 * NH + 32);
+static_assert((TM * 16 * sizeof(float)) % 16 == 0, "BETA must stay 16-byte aligned after SHACC");
+static_assert(kBwdSmemFold <= 227 * 1024, "the folded adjoint's shared memory exceeds a CTA's");
 
 
 // Sum the per-block partials into dW0 (64,51), dW1 (3,64), db0 (64), db1 (3), in a fixed order
@@ -1129,8 +1297,13 @@ int launch_fwd(const HashArgs& a, const float* X, int64_t ldx, int64_t P, const 
   const int64_t tiles = (P + TM - 1) / TM;
   const bool compact = src.rays_d != nullptr;
   if (!kHashIn && (compact || ldx == KP) && (reinterpret_cast<uintptr_t>(X) & 15) == 0) {  // contiguous rows: two slots
-    auto kern2 = compact ? (custom_wait() ? k_mlp_fwd_rows2<true, true> : k_mlp_fwd_rows2<false, true>)
-                         : (custom_wait() ? k_mlp_fwd_rows2<true, false> : k_mlp_fwd_rows2<false, false>);
+    // compact rows whose tiles each lie inside one ray (samples per ray a multiple of the tile):
+    // the folded MLP
+    const bool fold = compact && src.S % TM == 0;
+    const bool cw = custom_wait();
+    auto kern2 = fold ? (cw ? k_mlp_fwd_rows2<true, true, true> : k_mlp_fwd_rows2<false, true, true>)
+                 : compact ? (cw ? k_mlp_fwd_rows2<true, true, false> : k_mlp_fwd_rows2<false, true, false>)
+                           : (cw ? k_mlp_fwd_rows2<true, false, false> : k_mlp_fwd_rows2<false, false, false>);
     cudaError_t e = cudaFuncSetAttribute(kern2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kFwd2Smem);
     if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "mlp forward: %s", cudaGetErrorString(e));
     const int64_t pairs = (tiles + 1) / 2;
@@ -1164,11 +1337,14 @@ int mlp_backward_launch(const float* x, int64_t ldx, int64_t n_points, const flo
   if (n_points > 0) {
     const int xvec = (ldx % 4 == 0) && ((reinterpret_cast<uintptr_t>(x) & 15) == 0);
     const bool bulk = xvec && (compact || ldx == KP);
-    const size_t smem = bulk ? kBwdSmemBulk : kBwdSmemRegs;
+    // compact rows whose tiles each lie inside one ray: the folded MLP (as in the forward)
+    const bool fold = compact && src.S % TM == 0;
+    const size_t smem = fold ? kBwdSmemFold : compact ? kBwdSmemCompact : bulk ? kBwdSmemBulk : kBwdSmemRegs;
     const bool cw = custom_wait();
-    auto kern = compact ? (cw ? k_mlp_bwd_tc<true, true, true> : k_mlp_bwd_tc<true, false, true>)
-                        : bulk ? (cw ? k_mlp_bwd_tc<true, true, false> : k_mlp_bwd_tc<true, false, false>)
-                               : (cw ? k_mlp_bwd_tc<false, true, false> : k_mlp_bwd_tc<false, false, false>);
+    auto kern = fold ? (cw ? k_mlp_bwd_tc<true, true, true, true> : k_mlp_bwd_tc<true, false, true, true>)
+                : compact ? (cw ? k_mlp_bwd_tc<true, true, true, false> : k_mlp_bwd_tc<true, false, true, false>)
+                : bulk ? (cw ? k_mlp_bwd_tc<true, true, false, false> : k_mlp_bwd_tc<true, false, false, false>)
+                       : (cw ? k_mlp_bwd_tc<false, true, false, false> : k_mlp_bwd_tc<false, false, false, false>);
     cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return set_error(VX_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
     kern<<<nb, 256, smem, st>>>(x, ldx, xvec, n_points, w, d_colors, colors, d_hash, d_normal, partials, t_guard, src);
