@@ -43,7 +43,10 @@ def _worker(rank, world, port, q):
         ex.reduce_grads([grid, var])
         ex.union_bitmap(bitmap)
         flag = amplify_after_reduce(var, 5.0)
-        q.put((rank, grads_before, grid.grad.clone(), var.grad.clone(), bool(flag), bitmap.clone()))
+        # numpy copies travel by value: a tensor would travel as a shared-memory handle that the
+        # parent can only open while this process is still alive
+        q.put((rank, grads_before.numpy(), grid.grad.numpy().copy(), var.grad.numpy().copy(), bool(flag),
+               bitmap.numpy().copy()))
     finally:
         dist.destroy_process_group()
 
@@ -61,6 +64,7 @@ def test_gradient_mean_bitmap_union_and_global_sign_amplification():
     for p in procs:
         p.join(timeout=30)
         assert p.exitcode == 0
+    res = [(r, *(torch.from_numpy(a) for a in (gb, g, v)), f, torch.from_numpy(bm)) for r, gb, g, v, f, bm in res]
     mean = (res[0][1] + res[1][1]) / 2
     for _, _, g, v, flag, bm in res:
         assert torch.allclose(g, mean, atol=1e-7)
@@ -129,7 +133,7 @@ def _half_batch_worker(rank, world, port, q):
         with torch.no_grad():
             sc.grid.grad.add_(ge.reshape(sc.grid.shape))
             sc.grid.grad.add_(gc.reshape(sc.grid.shape))
-        q.put((rank, [p.grad.clone() for p in sc.params()], bool(flag), verts.shape[0], ex.collectives))
+        q.put((rank, [p.grad.numpy().copy() for p in sc.params()], bool(flag), verts.shape[0], ex.collectives))
     finally:
         dist.destroy_process_group()
 
@@ -149,6 +153,7 @@ def test_two_half_batches_through_the_exchange_equal_the_full_batch():
     for p in procs:
         p.join(timeout=30)
         assert p.exitcode == 0
+    res = [(r, [torch.from_numpy(g) for g in gs], f, n, c) for r, gs, f, n, c in res]
     sc = _scene(O)
     o, d, t, t_rand, us = _batch()
     ref = sc.train_step(o, d, t, amplify_k=5.0, t_rand=t_rand, us=us, **RENDER)
