@@ -290,12 +290,12 @@ def _cpu_baseline(args, n_rays, steps):
                       f"(oracle: the reference's torch ops restated, float32 on CPU)"}, med
 
 
-def _oracle_scene_of(m, device, grad=True):
+def _oracle_scene_of(m, device, grad=True, dtype=torch.float32):
     """The oracle's scene holding copies of a fused model's parameters and occupancy mask."""
     from oracle import reference_path as O
 
     l0, l1 = m.radiance_mlp.net[0], m.radiance_mlp.net[2]
-    ps = [t.detach().to(device).clone().requires_grad_(grad) for t in (
+    ps = [t.detach().to(device, dtype).clone().requires_grad_(grad) for t in (
         m.sdf_grid.grid, m.variance_net.variance, m.radiance_hash.encoder.embeddings, l0.weight, l0.bias, l1.weight,
         l1.bias)]
     return O.OracleScene(*ps, occupancy=m.occupancy_grid.occupancy_mask.detach().to(device).clone())
@@ -325,6 +325,12 @@ def parity_leg(m, batch, dev, n_rays=CPU_SAMPLE_RAYS):
     sc = _oracle_scene_of(m, "cpu")
     oc, dc, tc = o.cpu(), d.cpu(), t.cpu()
     ref = sc.train_step(oc, dc, tc, band_voxels=3.0, amplify_k=5.0, step=0, s_warmup_steps=0, z_vals=z.cpu())
+    # the same step in float64: a gradient's bound is the float32 oracle's own distance from it
+    # (at least 1e-4); the variance gradient sums many cancelling terms, so float32 rounding of
+    # the colours alone moves it by more than 1e-4 of its size
+    sc64 = _oracle_scene_of(m, "cpu", dtype=torch.float64)
+    ref64 = sc64.train_step(oc.double(), dc.double(), tc.double(), band_voxels=3.0, amplify_k=5.0, step=0,
+                            s_warmup_steps=0, z_vals=z.cpu().double())
     near, far = O.near_far_from_sphere(oc, dc)
     zr, _, _ = O.sample_multistep_sdf(oc, dc, near, far, sc.sdf_fn, N_SAMPLES, N_IMPORTANCE, STEPS_UP, True, sc.occ_fn,
                                       t_rand=t_rand.cpu(), us=[u[k].cpu() for k in range(STEPS_UP)])
@@ -340,16 +346,20 @@ def parity_leg(m, batch, dev, n_rays=CPU_SAMPLE_RAYS):
           "embeddings": m.radiance_hash.encoder.embeddings, "w0": l0.weight, "b0": l0.bias, "w1": l1.weight,
           "b1": l1.bias}
     grads = {k: rel(p.grad, ref["grads"][k]) for k, p in gp.items()}
+    grads64 = {k: rel(p.grad, ref64["grads"][k]) for k, p in gp.items()}
+    bounds = {k: max(1e-4, 2.0 * rel(ref["grads"][k], ref64["grads"][k])) for k in gp}
     losses = {k: rel(out[k], ref[k]) for k in ("loss_rgb", "loss_eik", "loss_curv")}
     amp = bool(tr.amp_flag.item())
-    res = {"rays": n_rays, "loss_rel_err": losses, "grad_rel_err": grads,
+    res = {"rays": n_rays, "loss_rel_err": losses, "grad_rel_err": grads, "grad_rel_err_vs_float64": grads64,
+           "grad_bound": bounds,
            "n_active": [int(out["n_active"]), int(ref["n_active"])], "amplified": [amp, bool(ref["amplified"])],
            "sampler_rays_outside_1e-5": outside,
-           "tolerance": {"loss": 1e-5, "grad": 1e-4, "n_active": "equal", "amplified": "equal"},
+           "tolerance": {"loss": 1e-5, "grad": "grad_bound: max(1e-4, 2 x the float32 oracle's distance from "
+                                                 "the float64 oracle)", "n_active": "equal", "amplified": "equal"},
            "how": "one training step without the optimizers on a slice of a timed batch, parameters after the "
-                  "timed steps; the oracle (float32, host cores) steps on the fused sampler's samples; "
-                  "sampler_rays_outside_1e-5 compares the two samplers end to end on the same uniforms"}
-    res["within_tolerance"] = (max(losses.values()) <= 1e-5 and max(grads.values()) <= 1e-4
+                  "timed steps; the oracle (float32 and float64, host cores) steps on the fused sampler's "
+                  "samples; sampler_rays_outside_1e-5 compares the two samplers end to end on the same uniforms"}
+    res["within_tolerance"] = (max(losses.values()) <= 1e-5 and all(grads[k] <= bounds[k] for k in grads)
                                and res["n_active"][0] == res["n_active"][1] and amp == bool(ref["amplified"]))
     for p in gp.values():
         p.grad = None
