@@ -939,6 +939,18 @@ def serving_summary(args, duration):
     views = [(o.pin_memory(), d.pin_memory()) for o, d in views]
     qpool = [(torch.rand(1 << 22, 3, generator=torch.Generator().manual_seed(k)) * 2 - 1).pin_memory()
              for k in range(4)]
+    # warm-up before the measured window, as a deployed server is warmed: the largest and smallest
+    # request of each kind once per scene, so that the allocator's pools and the staging ring exist
+    # before the first timed arrival (first-use growth stalled the engine thread for up to a second)
+    warm = []
+    for i in range(n_scenes):
+        for n in (480000, 4096):
+            warm.append(eng.submit(Request(f"scene{i}", "render", (views[0][0][:n], views[0][1][:n]))))
+        for n in (1 << 22, 1 << 16):
+            warm.append(eng.submit(Request(f"scene{i}", "query", (qpool[0][:n],))))
+    for r in warm:
+        r.wait(600)
+    torch.cuda.synchronize()
     duration = float(duration)
     rate = 200.0
     t = 0.0
@@ -992,7 +1004,12 @@ def serving_summary(args, duration):
             "offered": {"rays_per_s": sum(r.n for r in rend) / duration, "points_per_s": sum(r.n for r in qry) / duration},
             "query_points_per_s": sum(r.n for r in qry) / wall, "wall_s": wall,
             "latency_all": latency_stats(reqs), "latency_render": latency_stats(rend),
-            "latency_query": latency_stats(qry), "clocks": clk.summary()}
+            "latency_query": latency_stats(qry),
+            # p50 over the first, middle and last third of the arrivals: a stall shows as a backlog
+            # that the later thirds inherit
+            "latency_p50_ms_by_third": [latency_stats(reqs[k * len(reqs) // 3:(k + 1) * len(reqs) // 3]).get("p50_ms")
+                                        for k in range(3)],
+            "clocks": clk.summary()}
     del eng, store, views, qpool
     torch.cuda.empty_cache()
     return line
