@@ -266,6 +266,33 @@ def test_cat_z_vals_matches_oracle(nr, n, ni):
     assert bool(torch.isnan(zg[0]).any()) == (n > 2 and ni > 2) and (n < 3 or not bool(torch.isnan(zg[0, :-1]).any()))
 
 
+@pytest.mark.parametrize("n", [40, 300])
+def test_up_sample_with_occupancy_grid(n):
+    """up_sample with an occupancy grid (rendering/sampler.py:243-292 with the occupancy factor
+    0.9 occ + 0.1 of rendering/occupancy_grid.py:122-147 on each interval's midpoint) against the
+    oracle, on a random 32^3 mask; 300 samples a ray takes more than eight 32-interval chunks."""
+    from voxneus_b200.models import OccupancyGrid
+    from voxneus_b200.rendering import up_sample
+
+    torch.manual_seed(6 + n)
+    nr = 50
+    o = torch.randn(nr, 3)
+    o = 3.0 * o / o.norm(dim=-1, keepdim=True)
+    d = -o / o.norm(dim=-1, keepdim=True) + 0.1 * torch.randn(nr, 3)
+    d = d / d.norm(dim=-1, keepdim=True)
+    z = torch.sort(torch.rand(nr, n) * 4 + 1, dim=-1)[0]
+    sdf = torch.randn(nr, n) * 0.3
+    u = torch.rand(nr, 16)
+    occ = OccupancyGrid(32).to(DEV)
+    mask = torch.rand(32, 32, 32) < 0.5
+    with torch.no_grad():
+        occ.occupancy_mask.copy_(to(mask))
+    lo, hi = torch.tensor((-1.0,) * 3), torch.tensor((1.0,) * 3)
+    ref = O.up_sample(o, d, z, sdf, 16, 128.0, det=False, u=u, occ_fn=lambda p: O.is_occupied(mask, p, lo, hi))
+    out = up_sample(to(o), to(d), to(z), to(sdf), 16, 128.0, det=False, occupancy_grid=occ, u=to(u))
+    assert_close(out, ref, VAL_TOL, "up_sample with occupancy")
+
+
 # ------------------------------------------------------------------ render forward / backward
 
 

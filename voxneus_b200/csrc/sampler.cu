@@ -298,8 +298,9 @@ __global__ void __launch_bounds__(128) k_up_sample(const float* __restrict__ ray
   extern __shared__ float smem[];
   const int lane = threadIdx.x & 31;
   const int warp = threadIdx.x >> 5;
-  float* base = smem + warp * (4 * n + 2);
-  WarpArrays A{base, base + n, nullptr, nullptr, base + 2 * n, base + 3 * n, nullptr, nullptr};
+  float* base = smem + warp * (5 * n + 2);
+  // z, f, z2 (the intervals' occupancy factors), cdf, w
+  WarpArrays A{base, base + n, base + 4 * n + 2, nullptr, base + 2 * n, base + 3 * n, nullptr, nullptr};
   const int64_t wpb = blockDim.x >> 5;
   for (int64_t r = blockIdx.x * wpb + warp; r < n_rays; r += (int64_t)gridDim.x * wpb) {
     const float ox = rays_o[3 * r], oy = rays_o[3 * r + 1], oz = rays_o[3 * r + 2];
@@ -475,7 +476,7 @@ int vx_up_sample(const float* rays_o, const float* rays_d, const float* z, const
   VX_REQUIRE(!occupancy || (occ_res > 0 && occ_min && occ_max), "occupancy mask needs its resolution and bounds");
   Occ oc = make_occ(occupancy, occ_res, occ_min, occ_max);
   const int threads = 128;
-  const size_t smem = (size_t)(threads / 32) * (4 * n + 2) * sizeof(float);
+  const size_t smem = (size_t)(threads / 32) * (5 * n + 2) * sizeof(float);
   VX_REQUIRE(smem <= 200 * 1024, "too many samples per ray for one block");
   if (smem > 48 * 1024) cudaFuncSetAttribute(k_up_sample, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   k_up_sample<<<grid_for(n_rays * 32, threads, 8), threads, smem, (cudaStream_t)stream>>>(
