@@ -40,13 +40,13 @@ def _rays(n, seed, host=False):
     return o.to(DEV), d.to(DEV), t.to(DEV)
 
 
-def _run(cuda_graph, steps, warmup_s, host=False):
+def _run(cuda_graph, steps, warmup_s, host=False, grid_adam="torch"):
     from voxneus_b200.rendering import RaySampler
     from voxneus_b200.training import FusedTrainer
 
     m = _model()
     tr = FusedTrainer(m, RaySampler(16, 16, perturb=True), band_voxels=3.0, s_warmup_steps=warmup_s,
-                      total_steps=10, occupancy_update_interval=3, cuda_graph=cuda_graph)
+                      total_steps=10, occupancy_update_interval=3, cuda_graph=cuda_graph, grid_adam=grid_adam)
     torch.manual_seed(11)  # the sampler's and occupancy refresh's draws (default CUDA generator)
     hist = []
     for i in range(steps):
@@ -57,13 +57,16 @@ def _run(cuda_graph, steps, warmup_s, host=False):
     return m, tr, hist
 
 
-def test_graph_step_is_bitwise_the_eager_step():
+@pytest.mark.parametrize("grid_adam", ["torch", "cuda"])
+def test_graph_step_is_bitwise_the_eager_step(grid_adam):
+    """grid_adam: "torch", the plain-PyTorch mode's formula (the default), or "cuda", the reference
+    extension's (masked_adam_upd; in the graph its step size is read from device memory)."""
     from voxneus_b200 import ops
 
     ops.set_deterministic(True)
     try:
-        me, te, he = _run(False, 8, 5)
-        mg, tg, hg = _run(True, 8, 5)
+        me, te, he = _run(False, 8, 5, grid_adam=grid_adam)
+        mg, tg, hg = _run(True, 8, 5, grid_adam=grid_adam)
     finally:
         ops.set_deterministic(False)
     assert tg.graph() is not None and tg.graph().amplify  # captured, and recaptured with amplification
