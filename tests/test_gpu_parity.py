@@ -397,6 +397,49 @@ def test_volume_render_api_and_alpha():
     assert_close(t, tr, VAL_TOL, "T")
 
 
+@pytest.mark.parametrize("ratio", [0.0, 0.35, 1.0])
+def test_iter_cos_annealing(ratio):
+    """NeuS's iter_cos annealing (rendering/neus_alpha.py:46-53: cos = -(relu(-cos/2 + 1/2)(1 - r) +
+    relu(-cos) r)) through compute_neus_alpha and volume_render_from_samples against the oracle:
+    values, and the gradients of colours, SDF, normals and s."""
+    from voxneus_b200.rendering import compute_neus_alpha, volume_render_from_samples
+
+    torch.manual_seed(9)
+    nr, ns = 29, 48
+    col = torch.rand(nr, ns, 3)
+    sdf = torch.randn(nr, ns, 1) * 0.05
+    nrm = torch.nn.functional.normalize(torch.randn(nr, ns, 3), dim=-1)
+    dirs = torch.nn.functional.normalize(torch.randn(nr, 3), dim=-1)
+    z = torch.sort(torch.rand(nr, ns) * 2 + 1, dim=-1)[0]
+    dists = torch.rand(nr, ns) * 0.05
+    s = torch.tensor(30.0)
+    leaves = [t.clone().requires_grad_(True) for t in (col, sdf, nrm, s)]
+    ref = O.volume_render(leaves[0], leaves[1], leaves[2], dirs.unsqueeze(1).expand(-1, ns, -1), z, dists, leaves[3],
+                          cos_anneal_ratio=ratio, use_iter_cos=True)
+    gl = [t.clone().requires_grad_(True) for t in (to(col), to(sdf), to(nrm), to(s))]
+    out = volume_render_from_samples(gl[0], gl[1], gl[2], to(dirs), to(z), to(dists), gl[3],
+                                     cos_anneal_ratio=ratio, use_iter_cos_annealing=True)
+    for k in ("rgb", "depth", "normal", "opacity", "weights", "alpha"):
+        assert_close(out[k], ref[k].detach(), VAL_TOL, k)
+    cot = {k: torch.randn_like(ref[k]) for k in ("rgb", "depth", "normal", "opacity")}
+    sum(((ref[k] * cot[k]).sum() for k in cot)).backward()
+    sum(((out[k] * to(cot[k])).sum() for k in cot)).backward()
+    for a, b, nm in zip(gl, leaves, ("colors", "sdf", "normals", "s")):
+        assert_close(a.grad, b.grad, GRAD_TOL, nm + " grad")
+    # the standalone alpha and its adjoint
+    al = [t.clone().requires_grad_(True) for t in (sdf, nrm, s)]
+    a_ref = O.neus_alpha(al[0], al[1], dirs.unsqueeze(1).expand(-1, ns, -1), dists, al[2], ratio, True)
+    ag = [t.clone().requires_grad_(True) for t in (to(sdf), to(nrm), to(s))]
+    a_out = compute_neus_alpha(ag[0], ag[1], to(dirs).unsqueeze(1), to(dists), ag[2], cos_anneal_ratio=ratio,
+                               use_iter_cos_annealing=True)
+    assert_close(a_out, a_ref.detach(), VAL_TOL, "alpha")
+    ca = torch.randn_like(a_ref)
+    (a_ref * ca).sum().backward()
+    (a_out * to(ca)).sum().backward()
+    for a, b, nm in zip(ag, al, ("sdf", "normals", "s")):
+        assert_close(a.grad, b.grad, GRAD_TOL, "alpha " + nm + " grad")
+
+
 # ------------------------------------------------------------------ regularizers, V_R, upsample, hash
 
 
