@@ -30,9 +30,10 @@ namespace vx {
 constexpr int KIN = 51;  // input features
 constexpr int KP = 52;   // row width of the input rows (column 51 is padding)
 // Compact rows of the fused appearance path: [hash 32 | normal 3 | pad], 144 bytes. The 16 SH(d)
-// features (columns 32..47 of a full row) depend on the ray only; the MLP kernels recompute them
-// from the ray's direction while they stage a tile, the same function on the same operands as the
-// row writer, so both layouts give the same bits.
+// features (columns 32..47 of a full row) depend on the ray only. When a ray's samples fill whole
+// 128-row tiles the folded MLP (fold_col, fold_bias below) adds them as a per-ray hidden bias;
+// otherwise the MLP kernels rebuild them from the ray's direction while they stage a tile, the same
+// function on the same operands as the row writer, so that both layouts give the same bits.
 constexpr int KC = 36;
 constexpr int NH = 64;   // hidden units
 constexpr int NO = 3;    // colours
@@ -706,9 +707,9 @@ __global__ void __launch_bounds__(256, 1) k_mlp_bwd_tc(const float* __restrict__
   uint32_t* s_taddr = reinterpret_cast<uint32_t*>(bar + 2);
   // kFold: the SH columns of dW0, [16][128]: one column per TMEM lane of DZ^T (hidden unit hi
   // parts in lanes 0..63, lo parts in 64..127; lanes consecutive, so a warp's accesses are
-  // conflict-free); the tile's hidden bias (read as float4: 16-byte aligned)
-  // and the SH(d) of the last two tiles. The dynamic shared memory starts 1024-byte aligned, so aligning the address aligns
-  // the offset.
+  // conflict-free); the hidden bias of the last two tiles (read as float4: 16-byte aligned) and
+  // their SH(d). The dynamic shared memory starts 1024-byte aligned, so aligning the address
+  // aligns the offset.
   float* SHACC = reinterpret_cast<float*>((reinterpret_cast<uintptr_t>(bar) + 24 + 15) & ~uintptr_t(15));
   float* BETA = SHACC + TM * 16;  // [2][64]: tiles by parity
   float* SHT = BETA + 2 * NH;     // [2][16]
