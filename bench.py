@@ -566,7 +566,7 @@ def run_fused(args):
     m, up_ms = make_scene(args.res, dev)
     tr = FusedTrainer(m, RaySampler(N_SAMPLES, N_IMPORTANCE, perturb=True), band_voxels=3.0, exchange=exchange,
                       cuda_graph=not args.eager)
-    graph_mode = tr.cuda_graph and exchange is None
+    graph_mode = tr.cuda_graph  # data-parallel ranks: two graphs, the exchange eager between them
     pool = synthetic.RayPool(seed=100 + rank)
     nb = 8
     batches = []

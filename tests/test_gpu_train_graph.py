@@ -40,13 +40,14 @@ def _rays(n, seed, host=False):
     return o.to(DEV), d.to(DEV), t.to(DEV)
 
 
-def _run(cuda_graph, steps, warmup_s, host=False, grid_adam="torch"):
+def _run(cuda_graph, steps, warmup_s, host=False, grid_adam="torch", exchange=None):
     from voxneus_b200.rendering import RaySampler
     from voxneus_b200.training import FusedTrainer
 
     m = _model()
     tr = FusedTrainer(m, RaySampler(16, 16, perturb=True), band_voxels=3.0, s_warmup_steps=warmup_s,
-                      total_steps=10, occupancy_update_interval=3, cuda_graph=cuda_graph, grid_adam=grid_adam)
+                      total_steps=10, occupancy_update_interval=3, cuda_graph=cuda_graph, grid_adam=grid_adam,
+                      exchange=exchange)
     torch.manual_seed(11)  # the sampler's and occupancy refresh's draws (default CUDA generator)
     hist = []
     for i in range(steps):
@@ -165,3 +166,45 @@ def test_graph_mode_recaptures_on_a_new_batch_shape():
     assert all(torch.equal(a, b) for a, b in zip(le, lg))
     for pa, pb in zip(me.parameters(), mg.parameters()):
         assert torch.equal(pa, pb)
+
+
+def test_data_parallel_graph_step_is_bitwise_the_eager_step():
+    """With a gradient exchange (here a one-rank NCCL group on this GPU) the step runs as two
+    graphs, render + backward and regularizer + optimizers, with the exchange's collectives run
+    eagerly between them (no collective inside a graph); it gives the eager data-parallel step's
+    bits: parameters, Adam state and outputs, across the switch to the amplified variant."""
+    import socket
+
+    import torch.distributed as dist
+
+    from voxneus_b200 import ops
+    from voxneus_b200.dataparallel import GradExchange
+
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        port = sk.getsockname()[1]
+    dist.init_process_group("nccl", init_method=f"tcp://127.0.0.1:{port}", rank=0, world_size=1, device_id=DEV)
+    try:
+        ops.set_deterministic(True)
+        try:
+            me, te, he = _run(False, 8, 5, exchange=GradExchange())
+            mg, tg, hg = _run(True, 8, 5, exchange=GradExchange())
+        finally:
+            ops.set_deterministic(False)
+        assert tg.graph() is not None and tg.graph().graph2 is not None and tg.graph().amplify
+        for i, (a, b) in enumerate(zip(he, hg)):
+            for k in a:
+                assert torch.equal(a[k], b[k]), (i, k)
+        for (n, pa), pb in zip(me.named_parameters(), mg.parameters()):
+            assert torch.equal(pa, pb), n
+        for name in ("sdf_optimizer", "net_optimizer"):
+            oe, og = te.optimizers[name], tg.optimizers[name]
+            for pa, pb in zip(me.parameters(), mg.parameters()):
+                if pa in oe.state:
+                    sa, sb = oe.state[pa], og.state[pb]
+                    assert sa["step"] == sb["step"]
+                    assert torch.equal(sa["exp_avg"], sb["exp_avg"]) and torch.equal(sa["exp_avg_sq"], sb["exp_avg_sq"])
+        del tg, mg
+    finally:
+        torch.cuda.synchronize()
+        dist.destroy_process_group()

@@ -87,8 +87,9 @@ class GradExchange:
 
 
 def amplify_after_reduce(variance: torch.nn.Parameter, k: float) -> torch.Tensor:
-    """grad <- k * grad where the (reduced) grad is negative; returns the device flag."""
+    """grad <- k * grad where the (reduced) grad is negative, in place (a captured optimizer
+    launch holds the gradient's address); returns the device flag."""
     g = variance.grad
     neg = g < 0
-    variance.grad = torch.where(neg, g * k, g)
+    g.copy_(torch.where(neg, g * k, g))
     return neg

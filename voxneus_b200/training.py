@@ -204,8 +204,8 @@ class FusedTrainer:
         m = self.model
         if [int(r) for r in m.sdf_grid.res] != self.res:
             raise RuntimeError("grid resolution changed; build a new FusedTrainer after scale_volume_grid")
-        graphable = (self.cuda_graph and self.exchange is None and self.optimize and randoms is None
-                     and z_vals is None and torch.is_grad_enabled())
+        graphable = (self.cuda_graph and self.optimize and randoms is None and z_vals is None
+                     and torch.is_grad_enabled())
         self._tc_watch.check()
         if graphable and self._eager_steps >= GRAPH_WARMUP_STEPS:
             out = self._graph_step(rays_o, rays_d, target, step)
@@ -226,32 +226,48 @@ class FusedTrainer:
         if self.occupancy_update_interval > 0 and step % self.occupancy_update_interval == 0:
             self.model.update_occupancy_grid(subsample_ratio=0.25, generator=self.occ_generator)
 
-    def _render_backward_regularize(self, rays_o, rays_d, target, amp_k: float, randoms=None, z_vals=None):
-        """Render, loss, backward, gradient exchange, V_R and the regularizer stencil."""
+    def _render_backward(self, rays_o, rays_d, target, amp_k: float, randoms=None, z_vals=None):
+        """Render, loss and backward (the V_R bitmap marked on the way); returns (loss, rgb)."""
         m = self.model
         self.bitmap.zero_()
         self.counts.zero_()
-        ex = self.exchange
         with ops.tc_guard(self.tc_status, self.tc_wait_polls):
             out = m.render(rays_o, rays_d, self.sampler, None, None, up_sample_steps=self.up_sample_steps,
                            sphere_radius=1.0, randoms=randoms, vr_bitmap=self.bitmap, extras=False,
-                           amplify_k=0.0 if ex is not None else amp_k, amp_flag=self.amp_flag, z_vals=z_vals)
+                           amplify_k=0.0 if self.exchange is not None else amp_k, amp_flag=self.amp_flag,
+                           z_vals=z_vals)
             # the loss kernel writes dL/drgb beside the loss: the backward starts from it directly
             # (the same values as loss.backward(), without the seed fill and the scale by 1)
             loss, d_rgb = ops.huber_loss(out["rgb"], target, self.huber_delta)
             out["rgb"].backward(d_rgb)
-        if ex is not None:
-            flag = ex.exchange(list(m.parameters()), self.bitmap, m.variance_net.variance, amp_k)
-            if flag is not None:
-                self.amp_flag.copy_(flag.reshape(1).int())
+        return loss.detach(), out["rgb"].detach()
+
+    def _exchange(self, amp_k: float) -> None:
+        """Data-parallel ranks: the gradient exchange (reduce, bitmap union, amplification on the
+        reduced sign), in place: the gradient and flag tensors keep their addresses."""
+        m = self.model
+        flag = self.exchange.exchange(list(m.parameters()), self.bitmap, m.variance_net.variance, amp_k)
+        if flag is not None:
+            self.amp_flag.copy_(flag.reshape(1).int())
+
+    def _regularize(self, loss, rgb) -> Dict[str, torch.Tensor]:
+        """V_R (counts and filters) and the regularizer stencil into the grid gradient."""
+        m = self.model
         grid = m.sdf_grid.grid
         lo, hi = m.sdf_grid.bounds()
         ops.vr_count(self.bitmap, grid.detach(), self.res, lo, hi, self.relax_radius, self.band, self.counts,
                      self.filtered)
         ops.reg_stencil(grid.detach(), self.filtered, self.res, lo, hi, self.relax_radius, self.band, self.counts,
                         self.w_eik, self.w_curv, grid.grad, self.reg_losses, self.n_active)
-        return {"loss_rgb": loss.detach(), "loss_eik": self.reg_losses[0], "loss_curv": self.reg_losses[1],
-                "n_active": self.n_active, "rgb": out["rgb"].detach(), "tc_status": self.tc_status}
+        return {"loss_rgb": loss, "loss_eik": self.reg_losses[0], "loss_curv": self.reg_losses[1],
+                "n_active": self.n_active, "rgb": rgb, "tc_status": self.tc_status}
+
+    def _render_backward_regularize(self, rays_o, rays_d, target, amp_k: float, randoms=None, z_vals=None):
+        """Render, loss, backward, gradient exchange, V_R and the regularizer stencil."""
+        loss, rgb = self._render_backward(rays_o, rays_d, target, amp_k, randoms, z_vals)
+        if self.exchange is not None:
+            self._exchange(amp_k)
+        return self._regularize(loss, rgb)
 
     def _eager_step(self, rays_o, rays_d, target, step: int, randoms, z_vals=None) -> Dict[str, torch.Tensor]:
         m = self.model
@@ -340,12 +356,28 @@ class _StepGraph:
         from . import _lib
 
         self.graph = torch.cuda.CUDAGraph(keep_graph=True)
+        self.graph2 = None
+        self.amp_k = amp_k
         l0 = _lib.launch_count()
-        with torch.cuda.graph(self.graph):
-            self.outputs = tr._render_backward_regularize(self.o, self.d, self.t, amp_k)
-            self._optimizer_launches(m)
+        if tr.exchange is None:
+            with torch.cuda.graph(self.graph):
+                self.outputs = tr._render_backward_regularize(self.o, self.d, self.t, amp_k)
+                self._optimizer_launches(m)
+        else:
+            # data-parallel ranks: two graphs, the collectives between them run eagerly (no NCCL
+            # call inside a graph): render + backward, then V_R + regularizer + optimizers
+            with torch.cuda.graph(self.graph):
+                loss, rgb = tr._render_backward(self.o, self.d, self.t, amp_k)
+            self.graph.instantiate()
+            tr._exchange(amp_k)  # the gradients the capture allocated, as every replay leaves them
+            self.graph2 = torch.cuda.CUDAGraph(keep_graph=True)
+            with torch.cuda.graph(self.graph2):
+                self.outputs = tr._regularize(loss, rgb)
+                self._optimizer_launches(m)
+            self.graph2.instantiate()
         self.launches = _lib.launch_count() - l0
-        self.graph.instantiate()
+        if self.graph2 is None:
+            self.graph.instantiate()
 
     def _optimizer_launches(self, m) -> None:
         grid = m.sdf_grid.grid
@@ -421,3 +453,6 @@ class _StepGraph:
         ev.record()
         self.slot_events[s] = ev
         self.graph.replay()
+        if self.graph2 is not None:  # data-parallel: the exchange between the two graphs
+            self.tr._exchange(self.amp_k)
+            self.graph2.replay()
