@@ -737,8 +737,11 @@ def run_fused(args):
             "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene, rays and targets)",
             "config": config(args, world), "e2e": e2e, "gpu_launches": int(launches),
-            "launch": "one CUDA graph replay per step (render .. optimizer; occupancy refresh and input copies "
-                      "eager)" if graph_mode else "eager (every kernel launched from the host)",
+            "launch": ("eager (every kernel launched from the host)" if not graph_mode else
+                       "one CUDA graph replay per step (render .. optimizer; occupancy refresh and input copies "
+                       "eager)" if exchange is None else
+                       "two CUDA graph replays per step (render + backward; V_R + regularizer + optimizers) with the "
+                       "gradient exchange's collectives issued eagerly between them"),
             "roofline": roofline, "roofline_hbm": roofline_hbm,
             "kernels_ms_per_step": {k: round(v, 4) for k, v in sorted(per_kernel.items(), key=lambda x: -x[1])},
             "mlp_tensor": mlp_tensor(per_kernel, args.rays * (N_SAMPLES + N_IMPORTANCE)),
