@@ -18,10 +18,14 @@
 //                  steps; Z = columns [0, 64) + [64, 128)
 //   dX  = DZ W0    the same with A = DZ_hi / DZ_lo, B = W0^T [hi; lo], K = 64 in 8 steps
 //   dW0 = [DZh;DZl]^T X   A = DZ^T [hi; lo], B = X^T [hi; lo] (N = 128), K = 128 samples in 16 steps
-// The forward writes the colours (and, for the adjoint, the 52-float input rows); the adjoint
-// recomputes Z with the identical MMA sequence, writes dL/d(hash) and dL/d(normal), accumulates
-// dW0 (and db0 through a ones column) in TMEM across its tiles and dW1/db1 in registers, and
-// writes per-block partials that k_mlp_wgrad_reduce sums in a fixed order (deterministic).
+// The forward writes the colours (and, for the adjoint, the input rows: 52 floats, or the compact
+// 36-float rows of the fused appearance path); the adjoint recomputes Z with the identical MMA
+// sequence, writes dL/d(hash) and dL/d(normal), accumulates dW0 (and db0 through a ones column) in
+// TMEM across its tiles and dW1 in TMEM / db1 in registers, and writes per-block partials that
+// k_mlp_wgrad_reduce sums in a fixed order (deterministic). The folded variant (compact rows whose
+// tiles each lie inside one ray) contracts K = 40 features [hash | normal | one] in 5 steps, with
+// SH(d) as a per-ray bias of the hidden layer and the SH columns of dW0 taken from each tile's
+// column sum of dL/dz.
 #include "hashgrid.cuh"
 #include "tc.cuh"
 
