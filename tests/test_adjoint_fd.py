@@ -14,7 +14,6 @@ gradients (Eq.11, Eq.14). Checks:
      kink and are counted, not compared).
 """
 
-import math
 
 import pytest
 import torch

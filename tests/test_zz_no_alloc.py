@@ -11,7 +11,6 @@ before any launch. It is named to be collected last and passes alone in a fresh 
 as after the others.
 """
 
-import ctypes
 
 import pytest
 import torch

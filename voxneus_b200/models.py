@@ -3,14 +3,13 @@
 Parameter and buffer names match the reference state_dict (sdf_grid.grid,
 variance_net.variance, radiance_hash.encoder.embeddings, radiance_mlp.net.{0,2}.*,
 occupancy_grid.*), so reference checkpoints load unchanged. Geometry, sampling,
-compositing and the hash encoding run in the library's kernels; the 2-layer MLP is a dense
-contraction and stays on torch's cuBLAS GEMMs.
+compositing, the hash encoding and the 2-layer radiance MLP (on the tcgen05 tensor cores) run in
+the library's kernels, each with its hand-written adjoint.
 """
 
 from __future__ import annotations
 
-import math
-from typing import Dict, List, Optional, Tuple, Union
+from typing import Dict, List, Optional, Tuple
 
 import torch
 import torch.nn as nn
